@@ -1,0 +1,131 @@
+/*
+ * qcs_b200.h -- extensions of the B200 simulator beyond the RQS-SVG API.
+ *
+ * None of these functions exists in the reference library; each one says
+ * which reference behaviour it builds on. They follow the same conventions
+ * as qcs.h: return 1 on success, 0 on failure with the message passed to the
+ * exception callback. Include qcs.h first.
+ */
+#pragma once
+#include "qcs.h"
+
+#ifdef __cplusplus
+extern "C"
+{
+#endif
+
+/*
+ * Execution modes for gate calls (qcs_simulator_set_fusion).
+ *   QCS_FUSION_PLAIN   one kernel launch per gate call, issued when the call
+ *                      is made -- the reference's execution model
+ *                      (src/qcs.cu:2679-2703).
+ *   QCS_FUSION_GREEDY  gate calls are queued; when a result is needed (a
+ *                      measurement, a state read, an event) the queue is cut
+ *                      into cache-blocked passes by the greedy planner, and
+ *                      each pass applies many gates in one read and one write
+ *                      of the state. Every gate is still applied with its own
+ *                      FP64 formula, in an order that respects dependencies.
+ *   QCS_FUSION_LEARNED like GREEDY, with the pass boundaries chosen by the
+ *                      dynamic-programming planner under the learned cost
+ *                      model (falls back to GREEDY when no model is loaded).
+ * The default is GREEDY unless the environment variable QCS_FUSION is set to
+ * 0, 1 or 2.
+ */
+#define QCS_FUSION_PLAIN 0
+#define QCS_FUSION_GREEDY 1
+#define QCS_FUSION_LEARNED 2
+
+int qcs_simulator_set_fusion(qcs_simulator *sim, int mode);
+int qcs_simulator_get_fusion(const qcs_simulator *sim, int *mode);
+
+/*
+ * Pin the measurement random-number generator. The engine is
+ * std::mt19937_64 seeded with a 32-bit value, as in the reference
+ * (src/qcs.cu:1845-1852), so the same seed gives the same sequence of
+ * uniforms as the reference's engine. Without this call the seed comes from
+ * std::random_device, exactly like the reference.
+ */
+int qcs_simulator_set_seed(qcs_simulator *sim, uint32_t seed);
+
+/* Complete all queued and in-flight work of the simulator. */
+int qcs_simulator_synchronize(qcs_simulator *sim);
+
+/*
+ * Copy the state vector, in logical qubit order, into a host array of
+ * 2 * 2^n doubles (re, im interleaved) -- the same bytes save_statevector
+ * writes to its file (src/qcs.cu:2494-2543). count is the number of
+ * amplitudes the buffer holds and must be at least 2^n.
+ */
+int qcs_simulator_get_statevector(qcs_simulator *sim, double *amplitudes, uint64_t count);
+
+/*
+ * Load a state vector given in logical qubit order (2 * 2^n doubles). This is
+ * the reachable form of the reference's unreachable loader
+ * (src/qcs.cu:2121-2159). Clears the measured-qubit bookkeeping.
+ */
+int qcs_simulator_set_statevector(qcs_simulator *sim, const double *amplitudes, uint64_t count);
+
+/*
+ * <Z_q> for every logical qubit q = 0 .. n-1, normalised by the state's norm
+ * (states are not renormalised after measurement, src/qcs.cu:2654-2674).
+ * expectations must hold n doubles; norm (may be NULL) receives sum |a|^2.
+ * One read pass over the state, FP64 accumulation.
+ */
+int qcs_simulator_expectation_z(qcs_simulator *sim, double *expectations, double *norm);
+
+/*
+ * Draw num_shots bitstrings of all n qubits from the current state without
+ * changing it. Shot s measures logical qubits 0, 1, ..., n-1 in that order
+ * with the chain rule of measure_qubit (src/qcs.cu:2545-2677): for qubit j,
+ * r = u * (P0 + P1) with u from the simulator's engine and outcome = P0 < r.
+ * The uniforms are drawn from the same engine in the same order as
+ * num_shots repetitions of "run circuit, measure qubits 0..n-1" would draw
+ * them, so the outcomes equal the reference's bin/qcs sample loop
+ * (src/qcs_main.cpp:153-193) for a circuit that ends with that measurement.
+ * bitstrings[s] has bit q set when logical qubit q was measured as 1.
+ * Requires n <= 64.
+ */
+int qcs_simulator_sample(qcs_simulator *sim, uint32_t num_shots, uint64_t *bitstrings);
+
+/*
+ * Counters since creation (or the last reset_stats): kernels launched by the
+ * library, gates received, passes executed by the fused path, and the
+ * algorithmic bytes of the gates (2 * bytes_per_amplitude * amplitudes each
+ * gate can change).
+ */
+typedef struct qcs_b200_stats
+{
+    uint64_t kernel_launches;
+    uint64_t gates_received;
+    uint64_t gates_applied;
+    uint64_t fused_passes;
+    uint64_t plain_gate_kernels;
+    double algorithmic_bytes;
+} qcs_b200_stats;
+
+int qcs_simulator_get_stats(const qcs_simulator *sim, qcs_b200_stats *stats);
+int qcs_simulator_reset_stats(qcs_simulator *sim);
+
+/*
+ * Kernel timing recorder. When enabled, every gate kernel the library
+ * launches is bracketed by CUDA events on the simulator's stream; the sums
+ * below are per kernel class since the last read. Reading synchronizes the
+ * stream and clears the records. bytes = algorithmic bytes of the launches
+ * (a fused pass reads and writes the whole state once).
+ */
+typedef struct qcs_b200_kernel_times
+{
+    uint64_t fused_launches;
+    double fused_ms;
+    double fused_bytes;
+    uint64_t plain_launches;
+    double plain_ms;
+    double plain_bytes;
+} qcs_b200_kernel_times;
+
+int qcs_simulator_set_kernel_timing(qcs_simulator *sim, int enable);
+int qcs_simulator_get_kernel_times(qcs_simulator *sim, qcs_b200_kernel_times *times);
+
+#ifdef __cplusplus
+}
+#endif

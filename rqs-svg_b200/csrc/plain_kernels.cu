@@ -1,0 +1,583 @@
+// Plain-path kernels: one launch per gate, state preparation, measurement
+// reductions, collapse and <Z> sums.
+//
+// Layout: the register is one contiguous array of double2 (complex128,
+// 16-byte aligned); physical qubit q is bit q of the index. A gate on
+// targets T with controls C visits "groups": the 2^(n - |T u C|) indices
+// whose T and C bits are zero, enumerated by inserting zero bits at the
+// sorted operand positions (the role of thread_num_to_state_index_q*,
+// reference src/qcs.cu:156-376), then ORs in the control values and each
+// active target offset.
+//
+// Consecutive threads take consecutive groups, so every warp reads and writes
+// contiguous 16-byte amplitudes wherever the operand bits are >= 5; loads use
+// the streaming cache hint (each amplitude is touched once per pass over a
+// register far larger than L2).
+
+#include "qcs_internal.h"
+
+#include <cuda_runtime.h>
+
+namespace qcsb
+{
+namespace
+{
+
+constexpr int kThreads = 256;
+constexpr int kSMs = 148;
+constexpr int kMaxOps = kMaxQubits;
+
+__device__ __forceinline__ double2 cfma(double2 m, double2 v, double2 acc)
+{
+    acc.x = fma(m.x, v.x, acc.x);
+    acc.x = fma(-m.y, v.y, acc.x);
+    acc.y = fma(m.x, v.y, acc.y);
+    acc.y = fma(m.y, v.x, acc.y);
+    return acc;
+}
+
+__device__ __forceinline__ double2 cmul(double2 m, double2 v)
+{
+    double2 r;
+    r.x = fma(m.x, v.x, -m.y * v.y);
+    r.y = fma(m.x, v.y, m.y * v.x);
+    return r;
+}
+
+// Insert a zero bit below each mask boundary: masks[i] = (1 << pos_i) - 1
+// for operand positions sorted ascending.
+template <int MAXOPS>
+__device__ __forceinline__ uint64_t insert_zero_bits(uint64_t g, const uint64_t *masks, int nops)
+{
+#pragma unroll
+    for (int i = 0; i < MAXOPS; ++i)
+    {
+        if (i >= nops)
+            break;
+        const uint64_t lo = g & masks[i];
+        g = lo | ((g ^ lo) << 1);
+    }
+    return g;
+}
+
+template <int NA, bool DIAG>
+struct PlainParams
+{
+    double2 *state;
+    uint64_t ngroups;
+    uint64_t cval;
+    int nops;
+    uint64_t masks[kMaxOps];
+    uint64_t off[NA];
+    double2 m[DIAG ? NA : NA * NA];
+};
+
+template <int NA, bool DIAG, int U>
+__global__ void __launch_bounds__(kThreads) gate_plain_kernel(const __grid_constant__ PlainParams<NA, DIAG> p)
+{
+    const uint64_t step = (uint64_t)gridDim.x * kThreads * U;
+    for (uint64_t g0 = (uint64_t)blockIdx.x * kThreads * U + threadIdx.x; g0 < p.ngroups; g0 += step)
+    {
+        uint64_t base[U];
+        double2 v[U][NA];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const uint64_t g = g0 + (uint64_t)u * kThreads;
+            base[u] = insert_zero_bits<kMaxOps>(g, p.masks, p.nops) | p.cval;
+            if (g < p.ngroups)
+            {
+#pragma unroll
+                for (int a = 0; a < NA; ++a)
+                    v[u][a] = __ldcs(p.state + (base[u] | p.off[a]));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const uint64_t g = g0 + (uint64_t)u * kThreads;
+            if (g >= p.ngroups)
+                continue;
+            if (DIAG)
+            {
+#pragma unroll
+                for (int a = 0; a < NA; ++a)
+                    __stcs(p.state + (base[u] | p.off[a]), cmul(p.m[a], v[u][a]));
+            }
+            else
+            {
+#pragma unroll
+                for (int a = 0; a < NA; ++a)
+                {
+                    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int b = 0; b < NA; ++b)
+                        acc = cfma(p.m[a * NA + b], v[u][b], acc);
+                    __stcs(p.state + (base[u] | p.off[a]), acc);
+                }
+            }
+        }
+    }
+}
+
+// Sorted operand positions (targets and controls) as insertion masks.
+int fill_masks(const GateOp &op, uint64_t *masks)
+{
+    uint64_t bits = op.cmask;
+    for (int i = 0; i < op.nt; ++i)
+        bits |= 1ull << op.tq[i];
+    int nops = 0;
+    while (bits)
+    {
+        const int pos = __builtin_ctzll(bits);
+        masks[nops++] = (1ull << pos) - 1;
+        bits &= bits - 1;
+    }
+    return nops;
+}
+
+unsigned grid_for(uint64_t work_items, int per_block)
+{
+    uint64_t blocks = (work_items + per_block - 1) / per_block;
+    const uint64_t cap = (uint64_t)kSMs * 16;
+    if (blocks > cap)
+        blocks = cap;
+    if (blocks == 0)
+        blocks = 1;
+    return static_cast<unsigned>(blocks);
+}
+
+template <int NA, bool DIAG>
+int launch_plain_na(double2 *state, int n, const GateOp &op, cudaStream_t stream)
+{
+    constexpr int U = NA == 1 ? 4 : (NA == 2 ? 2 : 1);
+    PlainParams<NA, DIAG> p;
+    std::memset(&p, 0, sizeof(p));
+    p.state = state;
+    p.nops = fill_masks(op, p.masks);
+    p.ngroups = 1ull << (n - p.nops);
+    p.cval = op.cval;
+    for (int a = 0; a < NA; ++a)
+    {
+        uint64_t off = 0;
+        for (int i = 0; i < op.nt; ++i)
+            if ((op.act[a] >> i) & 1)
+                off |= 1ull << op.tq[i];
+        p.off[a] = off;
+    }
+    const int nm = DIAG ? NA : NA * NA;
+    for (int k = 0; k < nm; ++k)
+        p.m[k] = make_double2(op.mat[k].re, op.mat[k].im);
+    const unsigned grid = grid_for(p.ngroups, kThreads * U);
+    gate_plain_kernel<NA, DIAG, U><<<grid, kThreads, 0, stream>>>(p);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+template <bool DIAG>
+int launch_plain_dispatch(double2 *state, int n, const GateOp &op, cudaStream_t stream)
+{
+    switch (op.na)
+    {
+    case 1: return launch_plain_na<1, DIAG>(state, n, op, stream);
+    case 2: return launch_plain_na<2, DIAG>(state, n, op, stream);
+    case 3: return launch_plain_na<3, DIAG>(state, n, op, stream);
+    case 4: return launch_plain_na<4, DIAG>(state, n, op, stream);
+    case 5: return launch_plain_na<5, DIAG>(state, n, op, stream);
+    case 6: return launch_plain_na<6, DIAG>(state, n, op, stream);
+    case 7: return launch_plain_na<7, DIAG>(state, n, op, stream);
+    case 8: return launch_plain_na<8, DIAG>(state, n, op, stream);
+    case 16: return launch_plain_na<16, DIAG>(state, n, op, stream);
+    default: break;
+    }
+    // 9..15 active sub-indices: pad with inactive sub-indices (identity
+    // rows/columns), which exist because na < 2^nt.
+    GateOp padded = op;
+    const int d = 1 << op.nt;
+    const int na = op.na;
+    bool used[kMaxSub] = {};
+    for (int a = 0; a < na; ++a)
+        used[op.act[a]] = true;
+    int k = na;
+    for (int s = 0; s < d && k < 16; ++s)
+        if (!used[s])
+            padded.act[k++] = static_cast<uint8_t>(s);
+    if (k != 16)
+        throw std::runtime_error("internal: cannot pad gate operation");
+    padded.na = 16;
+    if (DIAG)
+    {
+        for (int a = na; a < 16; ++a)
+            padded.mat[a] = cplx{1.0, 0.0};
+    }
+    else
+    {
+        for (int a = 0; a < 16; ++a)
+            for (int b = 0; b < 16; ++b)
+            {
+                cplx v{0.0, 0.0};
+                if (a < na && b < na)
+                    v = op.mat[a * na + b];
+                else if (a == b)
+                    v = cplx{1.0, 0.0};
+                padded.mat[a * 16 + b] = v;
+            }
+    }
+    return launch_plain_na<16, DIAG>(state, n, padded, stream);
+}
+
+// ------------------------------------------------------------ preparation
+
+__global__ void fill_kernel(double2 *state, uint64_t count, double2 value)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (uint64_t)gridDim.x * kThreads)
+        __stcs(state + i, value);
+}
+
+__global__ void sequential_kernel(double2 *state, uint64_t count)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (uint64_t)gridDim.x * kThreads)
+        __stcs(state + i, make_double2(static_cast<double>(i), 0.0));
+}
+
+__global__ void set_one_kernel(double2 *state, uint64_t index, double2 value) { state[index] = value; }
+
+// ------------------------------------------------------------ reductions
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct ProbParams
+{
+    const double2 *state;
+    uint64_t ngroups;
+    uint64_t cval;
+    uint64_t tbit;
+    int nops;
+    uint64_t masks[kMaxOps];
+    double2 *partials;
+};
+
+// Per-block (sum |a0|^2, sum |a1|^2) over the groups; fixed reduction order,
+// so repeated calls give identical sums.
+__global__ void __launch_bounds__(kThreads) measure_probs_kernel(const __grid_constant__ ProbParams p)
+{
+    double s0 = 0.0, s1 = 0.0;
+    for (uint64_t g = (uint64_t)blockIdx.x * kThreads + threadIdx.x; g < p.ngroups; g += (uint64_t)gridDim.x * kThreads)
+    {
+        const uint64_t i0 = insert_zero_bits<kMaxOps>(g, p.masks, p.nops) | p.cval;
+        const double2 a0 = __ldcs(p.state + i0);
+        const double2 a1 = __ldcs(p.state + (i0 | p.tbit));
+        s0 = fma(a0.x, a0.x, fma(a0.y, a0.y, s0));
+        s1 = fma(a1.x, a1.x, fma(a1.y, a1.y, s1));
+    }
+    __shared__ double sh[2][kThreads / 32];
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    if (l == 0)
+    {
+        sh[0][w] = s0;
+        sh[1][w] = s1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t0 = 0.0, t1 = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k)
+        {
+            t0 += sh[0][k];
+            t1 += sh[1][k];
+        }
+        p.partials[blockIdx.x] = make_double2(t0, t1);
+    }
+}
+
+// Sums count double2 partials in a fixed order into *out (one block).
+__global__ void __launch_bounds__(kThreads) sum_partials2_kernel(const double2 *partials, int count, double2 *out)
+{
+    double s0 = 0.0, s1 = 0.0;
+    for (int i = threadIdx.x; i < count; i += kThreads)
+    {
+        s0 += partials[i].x;
+        s1 += partials[i].y;
+    }
+    __shared__ double sh[2][kThreads / 32];
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    if (l == 0)
+    {
+        sh[0][w] = s0;
+        sh[1][w] = s1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t0 = 0.0, t1 = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k)
+        {
+            t0 += sh[0][k];
+            t1 += sh[1][k];
+        }
+        *out = make_double2(t0, t1);
+    }
+}
+
+__global__ void collapse_kernel(double2 *state, uint64_t ngroups, uint64_t lowmask, uint64_t zero_bit)
+{
+    for (uint64_t g = (uint64_t)blockIdx.x * kThreads + threadIdx.x; g < ngroups; g += (uint64_t)gridDim.x * kThreads)
+    {
+        const uint64_t lo = g & lowmask;
+        const uint64_t i = lo | ((g ^ lo) << 1) | zero_bit;
+        __stcs(state + i, make_double2(0.0, 0.0));
+    }
+}
+
+// <Z> sums. Thread k of the grid (G = gridDim * 256 = 2^gbits threads)
+// visits indices i = it * G + k. Bits of i below gbits are fixed per thread;
+// bits at or above gbits are the bits of `it`. Per block the kernel writes
+// n + 1 partial sums: [0] the block's total, [1 + q] the part with bit q set.
+constexpr int kZThreads = 256;
+constexpr int kZMinBits = 12;                 // registers below this use one thread
+constexpr int kZMaxHi = kMaxQubits - kZMinBits; // "it" bits per thread
+
+__global__ void zsums_small_kernel(const double2 *state, int n, double *sums)
+{
+    double s[kMaxQubits + 1];
+    for (int j = 0; j <= n; ++j)
+        s[j] = 0.0;
+    for (uint64_t i = 0; i < (1ull << n); ++i)
+    {
+        const double2 a = state[i];
+        const double pr = fma(a.x, a.x, a.y * a.y);
+        s[0] += pr;
+        for (int q = 0; q < n; ++q)
+            if ((i >> q) & 1)
+                s[1 + q] += pr;
+    }
+    for (int j = 0; j <= n; ++j)
+        sums[j] = s[j];
+}
+
+__global__ void __launch_bounds__(kZThreads) zsums_kernel(const double2 *state, int n, int gbits, double *partials)
+{
+    const uint64_t gt = (uint64_t)blockIdx.x * kZThreads + threadIdx.x;
+    const uint64_t G = 1ull << gbits;
+    const uint64_t iters = 1ull << (n - gbits);
+    double total = 0.0;
+    double hi[kZMaxHi];
+    const int nhi = n - gbits;
+#pragma unroll
+    for (int q = 0; q < kZMaxHi; ++q)
+        hi[q] = 0.0;
+    for (uint64_t it = 0; it < iters; ++it)
+    {
+        const double2 a = __ldcs(state + it * G + gt);
+        const double pr = fma(a.x, a.x, a.y * a.y);
+        total += pr;
+#pragma unroll
+        for (int q = 0; q < kZMaxHi; ++q)
+            if (q < nhi && ((it >> q) & 1))
+                hi[q] += pr;
+    }
+    __shared__ double sh[kZThreads / 32];
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    auto block_sum = [&](double v) -> double {
+        v = warp_sum(v);
+        __syncthreads();
+        if (l == 0)
+            sh[w] = v;
+        __syncthreads();
+        double t = 0.0;
+        if (threadIdx.x == 0)
+            for (int k = 0; k < kZThreads / 32; ++k)
+                t += sh[k];
+        return t;
+    };
+    double *out = partials + (size_t)blockIdx.x * (n + 1);
+    const double btotal = block_sum(total);
+    if (threadIdx.x == 0)
+        out[0] = btotal;
+    // Low bits: q < gbits. Thread bits (q < 8) mask the per-thread totals;
+    // block bits (8 <= q < gbits) are uniform in the block.
+    const int tbits = gbits < 8 ? gbits : 8;
+    for (int q = 0; q < tbits; ++q)
+    {
+        const double v = block_sum(((threadIdx.x >> q) & 1) ? total : 0.0);
+        if (threadIdx.x == 0)
+            out[1 + q] = v;
+    }
+    if (threadIdx.x == 0)
+        for (int q = tbits; q < gbits; ++q)
+            out[1 + q] = ((gt >> q) & 1) ? btotal : 0.0;
+    for (int q = 0; q < nhi; ++q)
+    {
+        const double v = block_sum(hi[q]);
+        if (threadIdx.x == 0)
+            out[1 + gbits + q] = v;
+    }
+}
+
+__global__ void zsums_final_kernel(const double *partials, int nblocks, int nsums, double *sums)
+{
+    for (int j = threadIdx.x; j < nsums; j += blockDim.x)
+    {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b)
+            s += partials[(size_t)b * nsums + j];
+        sums[j] = s;
+    }
+}
+
+// ------------------------------------------------------------ gather
+
+struct PermParams
+{
+    int n;
+    int l2p[kMaxQubits];
+};
+
+__device__ __forceinline__ uint64_t logical_to_physical(uint64_t l, const PermParams &pp)
+{
+    uint64_t ph = 0;
+    for (int j = 0; j < pp.n; ++j)
+        ph |= ((l >> j) & 1ull) << pp.l2p[j];
+    return ph;
+}
+
+__global__ void gather_logical_kernel(const double2 *state, PermParams pp, uint64_t begin, uint64_t count, double2 *out)
+{
+    for (uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (uint64_t)gridDim.x * kThreads)
+        out[k] = state[logical_to_physical(begin + k, pp)];
+}
+
+__global__ void scatter_logical_kernel(double2 *state, PermParams pp, uint64_t begin, uint64_t count, const double2 *in)
+{
+    for (uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (uint64_t)gridDim.x * kThreads)
+        state[logical_to_physical(begin + k, pp)] = in[k];
+}
+
+PermParams make_perm(int n, const int *l2p)
+{
+    PermParams pp;
+    pp.n = n;
+    for (int j = 0; j < n; ++j)
+        pp.l2p[j] = l2p[j];
+    return pp;
+}
+
+} // namespace
+
+int launch_gate_plain(double2 *state, int n, const GateOp &op, cudaStream_t stream)
+{
+    if (op.na == 0)
+        return 0;
+    return op.diag ? launch_plain_dispatch<true>(state, n, op, stream)
+                   : launch_plain_dispatch<false>(state, n, op, stream);
+}
+
+int launch_init_zero(double2 *state, int n, cudaStream_t stream)
+{
+    QCSB_CUDA(cudaMemsetAsync(state, 0, sizeof(double2) << n, stream));
+    set_one_kernel<<<1, 1, 0, stream>>>(state, 0, make_double2(1.0, 0.0));
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_init_flat(double2 *state, int n, cudaStream_t stream)
+{
+    const uint64_t count = 1ull << n;
+    fill_kernel<<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, count, make_double2(1.0, 0.0));
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_init_sequential(double2 *state, int n, cudaStream_t stream)
+{
+    const uint64_t count = 1ull << n;
+    sequential_kernel<<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, count);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_set_amplitude(double2 *state, uint64_t index, double re, double im, cudaStream_t stream)
+{
+    set_one_kernel<<<1, 1, 0, stream>>>(state, index, make_double2(re, im));
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_measure_probs(const double2 *state, int n, int t, uint64_t cmask, uint64_t cval,
+                         double2 *partials, double2 *result, cudaStream_t stream)
+{
+    ProbParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.state = state;
+    GateOp op;
+    op.nt = 1;
+    op.tq[0] = t;
+    op.cmask = cmask;
+    p.nops = fill_masks(op, p.masks);
+    p.ngroups = 1ull << (n - p.nops);
+    p.cval = cval;
+    p.tbit = 1ull << t;
+    p.partials = partials;
+    // A fixed grid (independent of n) keeps the partial count constant.
+    measure_probs_kernel<<<kReduceBlocks, kThreads, 0, stream>>>(p);
+    QCSB_CUDA(cudaGetLastError());
+    sum_partials2_kernel<<<1, kThreads, 0, stream>>>(partials, kReduceBlocks, result);
+    QCSB_CUDA(cudaGetLastError());
+    return 2;
+}
+
+int launch_collapse(double2 *state, int n, int t, int keep_value, cudaStream_t stream)
+{
+    const uint64_t ngroups = 1ull << (n - 1);
+    const uint64_t zero_bit = keep_value ? 0ull : (1ull << t);
+    collapse_kernel<<<grid_for(ngroups, kThreads * 4), kThreads, 0, stream>>>(state, ngroups, (1ull << t) - 1, zero_bit);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_zsums(const double2 *state, int n, double *partials, double *sums, cudaStream_t stream)
+{
+    const int nsums = n + 1;
+    if (n < kZMinBits)
+    {
+        zsums_small_kernel<<<1, 1, 0, stream>>>(state, n, sums);
+        QCSB_CUDA(cudaGetLastError());
+        return 1;
+    }
+    // 2^gbits threads in total: at most 512 blocks of 256 threads.
+    const int gbits = n < 17 ? n : 17;
+    const int blocks = 1 << (gbits - 8);
+    zsums_kernel<<<blocks, kZThreads, 0, stream>>>(state, n, gbits, partials);
+    QCSB_CUDA(cudaGetLastError());
+    zsums_final_kernel<<<1, 64, 0, stream>>>(partials, blocks, nsums, sums);
+    QCSB_CUDA(cudaGetLastError());
+    return 2;
+}
+
+int launch_gather_logical(const double2 *state, int n, const int *l2p, uint64_t begin,
+                          uint64_t count, double2 *out, cudaStream_t stream)
+{
+    gather_logical_kernel<<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, make_perm(n, l2p), begin, count, out);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_scatter_logical(double2 *state, int n, const int *l2p, uint64_t begin,
+                           uint64_t count, const double2 *in, cudaStream_t stream)
+{
+    scatter_logical_kernel<<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, make_perm(n, l2p), begin, count, in);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+} // namespace qcsb

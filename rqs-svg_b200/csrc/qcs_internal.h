@@ -1,0 +1,127 @@
+// Internal declarations shared by the host core and the sm_100a kernels.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace qcsb
+{
+
+// Largest register the library accepts. 2^34 complex128 amplitudes = 256 GiB,
+// above any single B200; the allocator rejects what does not fit first.
+constexpr int kMaxQubits = 40;
+// Most targets one gate operation may carry (API gates use <= 4).
+constexpr int kMaxTargets = 4;
+constexpr int kMaxSub = 1 << kMaxTargets;
+
+std::string strformat(const char *fmt, ...);
+
+#define QCSB_CUDA(call)                                                                 \
+    do                                                                                  \
+    {                                                                                   \
+        cudaError_t qcsb_err_ = (call);                                                 \
+        if (qcsb_err_ != cudaSuccess)                                                   \
+            throw std::runtime_error(::qcsb::strformat("%s failed: %s (%s:%d)", #call,  \
+                                                       cudaGetErrorString(qcsb_err_),   \
+                                                       __FILE__, __LINE__));            \
+    } while (0)
+
+struct cplx
+{
+    double re, im;
+};
+
+// A gate on physical qubits, reduced to the sub-indices it changes.
+//
+// Sub-index s of a target group has bit i equal to the value of physical
+// qubit tq[i] (reference ordering: target i is bit i, src/qcs.cu:255-259).
+// act[0..na) lists the sub-indices whose amplitude can change; every other
+// sub-index has an identity row and column in the gate's matrix, so only the
+// na x na block mat (row-major, output x input) is applied (or its diagonal
+// when diag is set). Controls: the gate acts where (index & cmask) == cval.
+struct GateOp
+{
+    int nt = 0;
+    int tq[kMaxTargets] = {0, 0, 0, 0};
+    uint64_t cmask = 0;
+    uint64_t cval = 0;
+    bool diag = false;
+    int na = 0;
+    uint8_t act[kMaxSub] = {};
+    cplx mat[kMaxSub * kMaxSub] = {};   // na*na (dense) or na (diag) entries used
+    // Number of amplitudes this gate can change in a 2^n register: the
+    // algorithmic unit of work (2 * bytes_per_amp * changed amps per gate).
+    double changed_amps(int n) const;
+};
+
+// Dense 2^nt x 2^nt unitary of an API gate (row = output sub-index).
+struct GateMatrix
+{
+    int nt = 0;
+    cplx m[kMaxSub * kMaxSub] = {};
+};
+
+// Builds the matrix of a named gate of the reference API. Throws on unknown
+// names or a wrong parameter count.
+GateMatrix gate_matrix(const char *name, const double *params, int nparams);
+int gate_arity(const char *name);
+
+// Reduce a dense matrix on targets tq to a GateOp (active set + diag flag).
+GateOp make_gate_op(const GateMatrix &g, const int *tq, uint64_t cmask, uint64_t cval);
+
+// ---------------------------------------------------------------- kernels
+// Every launch helper below enqueues on `stream` and returns the number of
+// kernels launched (for the launch counters).
+
+// Plain path: one kernel applying one GateOp to the whole register.
+int launch_gate_plain(double2 *state, int n, const GateOp &op, cudaStream_t stream);
+
+// |0..0>, flat (all 1), sequential (a[i] = i), and "entangled" (a[0] = 1,
+// leaving the rest as is) state preparation.
+int launch_init_zero(double2 *state, int n, cudaStream_t stream);
+int launch_init_flat(double2 *state, int n, cudaStream_t stream);
+int launch_init_sequential(double2 *state, int n, cudaStream_t stream);
+int launch_set_amplitude(double2 *state, uint64_t index, double re, double im, cudaStream_t stream);
+
+// Squared-norm sums (P0, P1) of target qubit t over the subspace where
+// (index & cmask) == cval. partials must hold kReduceBlocks double2;
+// result receives one double2 on the device.
+constexpr int kReduceBlocks = 592;   // 4 x 148 SMs
+int launch_measure_probs(const double2 *state, int n, int t, uint64_t cmask, uint64_t cval,
+                         double2 *partials, double2 *result, cudaStream_t stream);
+
+// Zero every amplitude whose bit t differs from keep_value.
+int launch_collapse(double2 *state, int n, int t, int keep_value, cudaStream_t stream);
+
+// sums[0] = sum |a|^2, sums[1 + q] = sum over amplitudes with bit q set of
+// |a|^2 (physical qubits q = 0..n-1). partials must hold
+// kReduceBlocks * (n + 1) doubles; sums receives n + 1 doubles.
+int launch_zsums(const double2 *state, int n, double *partials, double *sums, cudaStream_t stream);
+
+// Gather the register into logical order: out[l] = state[phys(l)], where
+// phys(l) deposits logical bit j of l at physical bit l2p[j]; for indices
+// [begin, begin + count). l2p lives in device-readable memory (kernel arg).
+int launch_gather_logical(const double2 *state, int n, const int *l2p, uint64_t begin,
+                          uint64_t count, double2 *out, cudaStream_t stream);
+int launch_scatter_logical(double2 *state, int n, const int *l2p, uint64_t begin,
+                           uint64_t count, const double2 *in, cudaStream_t stream);
+
+// Shot sampler (chain rule over physical qubits in the order given by
+// order[0..n)). See sampler.cu for the data layout.
+struct SamplerWorkspace
+{
+    double *tree = nullptr;      // 2^(s+1) doubles
+    double2 *unused = nullptr;
+    size_t tree_bytes = 0;
+};
+int launch_sampler(const double2 *state, int n, const int *order, uint32_t num_shots,
+                   const double *uniforms, uint64_t *out_bits, double *tree, int split,
+                   cudaStream_t stream);
+size_t sampler_tree_bytes(int n, int *split_out);
+
+} // namespace qcsb

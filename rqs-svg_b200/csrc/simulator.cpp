@@ -1,0 +1,687 @@
+// Host orchestration of the simulator.
+//
+// Semantics follow the reference's simulator_core (src/qcs.cu:1685-2899) at
+// one process: logical<->physical qubit mapping, measured qubits acting as
+// implicit controls of later gates (and cancelling gates whose explicit
+// control contradicts them), cached re-measurement without a random draw,
+// measurement by (P0, P1) reduction + host mt19937_64 draw + zeroing of the
+// other branch without renormalisation, and the state preparations.
+//
+// Execution differs: gate calls become GateOps on physical qubits. In plain
+// mode each is launched at once (one kernel per gate, like the reference);
+// otherwise they are queued and executed by the fused executor when a result
+// is needed.
+
+#include "simulator.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
+
+#include <curand.h>
+
+namespace qcsb
+{
+namespace
+{
+
+constexpr uint64_t kStagingAmps = 1ull << 22;   // 64 MiB per staging buffer
+constexpr size_t kScratchReserve = 256ull << 20;
+
+bool contains(const std::vector<int> &v, int x) { return std::find(v.begin(), v.end(), x) != v.end(); }
+
+int env_fusion_mode()
+{
+    const char *e = std::getenv("QCS_FUSION");
+    if (e == nullptr || e[0] == '\0')
+        return QCS_FUSION_GREEDY;
+    const int m = std::atoi(e);
+    if (m < QCS_FUSION_PLAIN || m > QCS_FUSION_LEARNED)
+        return QCS_FUSION_GREEDY;
+    return m;
+}
+
+} // namespace
+
+Simulator::Simulator()
+{
+    // reference setup(), src/qcs.cu:1789-1858, at a single process: the
+    // device is the current one, the seed comes from std::random_device.
+    QCSB_CUDA(cudaGetDevice(&device_));
+    QCSB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    std::random_device rd;
+    set_seed(rd());
+    fusion_mode_ = env_fusion_mode();
+}
+
+Simulator::~Simulator()
+{
+    if (!disposed_)
+    {
+        try
+        {
+            dispose();
+        }
+        catch (...)
+        {
+        }
+    }
+}
+
+void Simulator::set_seed(uint32_t seed)
+{
+    seed_ = seed;
+    engine_ = std::mt19937_64(seed);
+}
+
+void Simulator::set_fusion(int mode)
+{
+    if (mode < QCS_FUSION_PLAIN || mode > QCS_FUSION_LEARNED)
+        throw std::runtime_error(strformat("fusion mode %d is not one of 0 (plain), 1 (greedy), 2 (learned)", mode));
+    if (allocated())
+        flush();
+    fusion_mode_ = mode;
+}
+
+void Simulator::require_allocated(const char *what) const
+{
+    if (disposed_)
+        throw std::runtime_error(strformat("%s: the simulator has been disposed", what));
+    if (state_ == nullptr)
+        throw std::runtime_error(strformat("%s: allocate_memory must be called first", what));
+}
+
+void Simulator::check_qubit(int q, const char *role) const
+{
+    if (q < 0 || q >= n_)
+        throw std::runtime_error(strformat("%s qubit %d is out of range [0, %d)", role, q, n_));
+}
+
+void Simulator::allocate_memory()
+{
+    // reference allocate_memory, src/qcs.cu:1887-1998
+    if (disposed_)
+        throw std::runtime_error("allocate_memory: the simulator has been disposed");
+    const int n = num_qubits_cfg;
+    if (state_ != nullptr)
+        throw std::runtime_error(strformat("num_qubits is already set %d > 0", n_));
+    if (n <= 0)
+        throw std::runtime_error("allocate_memory: set_num_qubits must be called with a positive count first");
+    size_t free_b = 0, total_b = 0;
+    QCSB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t usable = free_b > kScratchReserve ? free_b - kScratchReserve : 0;
+    int max_n = 0;
+    while (max_n < 62 && (sizeof(double2) << (max_n + 1)) <= usable)
+        ++max_n;
+    if (max_n > kMaxQubits)
+        max_n = kMaxQubits;
+    if (n > max_n)
+        throw std::runtime_error(strformat("num_qubits(%d) > max_num_qubits_local_device(%d) + log_num_procs(0)", n, max_n));
+    QCSB_CUDA(cudaMalloc(&state_, sizeof(double2) << n));
+    n_ = n;
+    perm_p2l_.assign(n, 0);
+    perm_l2p_.assign(n, 0);
+    reinitialize_mapping();
+    QCSB_CUDA(cudaMalloc(&red_partials_, sizeof(double2) * kReduceBlocks));
+    QCSB_CUDA(cudaMalloc(&red_result_, sizeof(double2)));
+    QCSB_CUDA(cudaMalloc(&zsum_partials_, sizeof(double) * 512 * (kMaxQubits + 1)));
+    QCSB_CUDA(cudaMalloc(&zsum_result_, sizeof(double) * (kMaxQubits + 1)));
+    host_pinned_bytes_ = 1 << 16;
+    QCSB_CUDA(cudaMallocHost(&host_pinned_, host_pinned_bytes_));
+    fused_ = new FusedExecutor(stream_);
+    set_zero_state();
+}
+
+void Simulator::dispose()
+{
+    // reference dispose, src/qcs.cu:2836-2845 (MPI_Finalize has no
+    // counterpart in a single process)
+    if (disposed_)
+        throw std::runtime_error("dispose: the simulator has already been disposed");
+    pending_.clear();
+    disposed_ = true;
+    if (stream_)
+        cudaStreamSynchronize(stream_);
+    delete fused_;
+    fused_ = nullptr;
+    cudaFree(state_);
+    cudaFree(red_partials_);
+    cudaFree(red_result_);
+    cudaFree(zsum_partials_);
+    cudaFree(zsum_result_);
+    cudaFree(staging_dev_);
+    if (host_pinned_)
+        cudaFreeHost(host_pinned_);
+    if (staging_host_)
+        cudaFreeHost(staging_host_);
+    state_ = nullptr;
+    red_partials_ = red_result_ = staging_dev_ = staging_host_ = nullptr;
+    zsum_partials_ = zsum_result_ = nullptr;
+    host_pinned_ = nullptr;
+    for (cudaEvent_t e : events_)
+        cudaEventDestroy(e);
+    events_.clear();
+    if (stream_)
+        cudaStreamDestroy(stream_);
+    stream_ = nullptr;
+    n_ = 0;
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess)
+        throw std::runtime_error(strformat("dispose: %s", cudaGetErrorString(err)));
+}
+
+void Simulator::set_mapping(const std::vector<int> &perm_p2l)
+{
+    // reference qcs_simulator_set_mapping_cxx, src/qcs.cu:3045-3062
+    if (num_qubits_cfg <= 0)
+        throw std::runtime_error("set_num_qubits must be called before set_mapping");
+    if ((int)perm_p2l.size() != num_qubits_cfg)
+        throw std::runtime_error(strformat("mapping size %d does not match num_qubits %d", (int)perm_p2l.size(), num_qubits_cfg));
+    std::vector<bool> used(num_qubits_cfg, false);
+    for (int l : perm_p2l)
+    {
+        if (l < 0 || l >= num_qubits_cfg)
+            throw std::runtime_error(strformat("mapping value %d is out of range [0, %d)", l, num_qubits_cfg));
+        if (used[l])
+            throw std::runtime_error(strformat("mapping value %d appears multiple times", l));
+        used[l] = true;
+    }
+    initial_perm_p2l_ = perm_p2l;
+}
+
+void Simulator::reinitialize_mapping()
+{
+    // reference reinitialize_mapping, src/qcs.cu:1860-1885
+    if (n_ == 0)
+        return;
+    if (initial_perm_p2l_.empty())
+    {
+        for (int q = 0; q < n_; ++q)
+            perm_p2l_[q] = perm_l2p_[q] = q;
+        return;
+    }
+    if ((int)initial_perm_p2l_.size() != n_)
+        throw std::runtime_error(strformat("mapping size %d does not match num_qubits %d", (int)initial_perm_p2l_.size(), n_));
+    flush();
+    perm_p2l_ = initial_perm_p2l_;
+    for (int p = 0; p < n_; ++p)
+        perm_l2p_[perm_p2l_[p]] = p;
+}
+
+bool Simulator::identity_mapping() const
+{
+    for (int q = 0; q < n_; ++q)
+        if (perm_l2p_[q] != q)
+            return false;
+    return true;
+}
+
+void Simulator::apply_gate(const char *name, const double *params, int nparams,
+                           const std::vector<int> &targets, const std::vector<int> &negctrls,
+                           const std::vector<int> &ctrls)
+{
+    require_allocated("gate");
+    ++stats.gates_received;
+    const int arity = gate_arity(name);
+    if ((int)targets.size() != arity)
+        throw std::runtime_error(strformat("gate %s takes %d target qubits, got %d", name, arity, (int)targets.size()));
+    uint64_t seen = 0;
+    auto claim = [&](int q, const char *role) {
+        check_qubit(q, role);
+        if ((seen >> q) & 1)
+            throw std::runtime_error(strformat("gate %s: qubit %d appears more than once among targets and controls", name, q));
+        seen |= 1ull << q;
+    };
+    for (int q : targets)
+        claim(q, "target");
+    for (int q : negctrls)
+        claim(q, "negative control");
+    for (int q : ctrls)
+        claim(q, "control");
+    const GateMatrix gm = gate_matrix(name, params, nparams);
+
+    // Measured qubits that are not targets become controls on their measured
+    // value; a contradicting explicit control cancels the gate
+    // (reference prepare_control_qubit_num_list, src/qcs.cu:2161-2204).
+    std::vector<int> ctrl_lists[2] = {negctrls, ctrls};
+    std::vector<int> keep[2];
+    const std::vector<int> *measured[2] = {&measured0_, &measured1_};
+    bool condition = true;
+    for (int v = 0; v < 2; ++v)
+        for (int q : *measured[v])
+        {
+            if (contains(targets, q))
+                continue;   // a gate on a measured qubit makes it unmeasured
+            keep[v].push_back(q);
+            const bool same = contains(ctrl_lists[v], q);
+            const bool other = contains(ctrl_lists[1 - v], q);
+            if (!same && !other)
+                ctrl_lists[v].push_back(q);
+            else if (other)
+                condition = false;
+        }
+    if (!condition)
+        return;   // measured lists are left as they were (src/qcs.cu:2689-2691)
+
+    uint64_t cmask = 0, cval = 0;
+    for (int v = 0; v < 2; ++v)
+        for (int q : ctrl_lists[v])
+        {
+            const int p = perm_l2p_[q];
+            cmask |= 1ull << p;
+            if (v)
+                cval |= 1ull << p;
+        }
+    int tq[kMaxTargets] = {0, 0, 0, 0};
+    for (int i = 0; i < arity; ++i)
+        tq[i] = perm_l2p_[targets[i]];
+    const GateOp op = make_gate_op(gm, tq, cmask, cval);
+
+    measured0_ = keep[0];
+    measured1_ = keep[1];
+
+    if (op.na == 0)
+        return;   // identity on every amplitude
+    ++stats.gates_applied;
+    stats.algorithmic_bytes += 2.0 * sizeof(double2) * op.changed_amps(n_);
+    if (fusion_mode_ == QCS_FUSION_PLAIN)
+    {
+        if (timer.enabled)
+            timer.begin(stream_, KernelTimer::kPlain, 2.0 * sizeof(double2) * op.changed_amps(n_));
+        const int k = launch_gate_plain(state_, n_, op, stream_);
+        if (timer.enabled)
+            timer.end(stream_);
+        stats.kernel_launches += k;
+        stats.plain_gate_kernels += k;
+    }
+    else
+    {
+        pending_.push_back(op);
+    }
+}
+
+void Simulator::flush()
+{
+    if (pending_.empty() || state_ == nullptr)
+        return;
+    const int k = fused_->run(state_, n_, pending_, fusion_mode_, stats, timer);
+    stats.kernel_launches += k;
+    pending_.clear();
+}
+
+void Simulator::synchronize()
+{
+    require_allocated("synchronize");
+    flush();
+    QCSB_CUDA(cudaStreamSynchronize(stream_));
+}
+
+int Simulator::measure(int q)
+{
+    // reference measure_qubit, src/qcs.cu:2545-2677
+    require_allocated("measure");
+    check_qubit(q, "measured");
+    if (contains(measured0_, q))
+        return 0;
+    if (contains(measured1_, q))
+        return 1;
+    flush();
+    uint64_t cmask = 0, cval = 0;
+    for (int m : measured0_)
+        cmask |= 1ull << perm_l2p_[m];
+    for (int m : measured1_)
+    {
+        cmask |= 1ull << perm_l2p_[m];
+        cval |= 1ull << perm_l2p_[m];
+    }
+    const int t = perm_l2p_[q];
+    stats.kernel_launches += launch_measure_probs(state_, n_, t, cmask, cval, red_partials_, red_result_, stream_);
+    double2 *h = static_cast<double2 *>(host_pinned_);
+    QCSB_CUDA(cudaMemcpyAsync(h, red_result_, sizeof(double2), cudaMemcpyDeviceToHost, stream_));
+    QCSB_CUDA(cudaStreamSynchronize(stream_));
+    const double p0 = h->x, p1 = h->y;
+    const double sum = p0 + p1;
+    std::uniform_real_distribution<double> dist(0, sum);
+    const double r = dist(engine_);
+    const int result = p0 < r;
+    (result ? measured1_ : measured0_).push_back(q);
+    stats.kernel_launches += launch_collapse(state_, n_, t, result, stream_);
+    return result;
+}
+
+void Simulator::reset_qubit(int q)
+{
+    // reference qcs_simulator_reset_cxx, src/qcs.cu:3077-3081
+    if (measure(q))
+        apply_gate("x", nullptr, 0, {q}, {}, {});
+}
+
+void Simulator::clear_measurement_state()
+{
+    measured0_.clear();
+    measured1_.clear();
+}
+
+void Simulator::set_zero_state()
+{
+    require_allocated("set_zero_state");
+    discard_pending();
+    clear_measurement_state();
+    stats.kernel_launches += launch_init_zero(state_, n_, stream_);
+}
+
+void Simulator::set_flat_state()
+{
+    require_allocated("set_flat_state");
+    discard_pending();
+    clear_measurement_state();
+    stats.kernel_launches += launch_init_flat(state_, n_, stream_);
+}
+
+void Simulator::set_sequential_state()
+{
+    require_allocated("set_sequential_state");
+    discard_pending();
+    clear_measurement_state();
+    stats.kernel_launches += launch_init_sequential(state_, n_, stream_);
+}
+
+void Simulator::set_entangled_state()
+{
+    // reference initialize_entangled at one process, src/qcs.cu:2081-2095:
+    // amplitude 0 becomes 1, every other amplitude keeps its value.
+    require_allocated("set_entangled_state");
+    flush();
+    clear_measurement_state();
+    stats.kernel_launches += launch_set_amplitude(state_, 0, 1.0, 0.0, stream_);
+}
+
+void Simulator::set_random_state()
+{
+    // reference initialize_use_curand, src/qcs.cu:2097-2119: unnormalised
+    // N(0, 1) real and imaginary parts from cuRAND's default generator seeded
+    // with the simulator seed. The measured lists are kept, as there.
+    require_allocated("set_random_state");
+    discard_pending();
+    curandGenerator_t gen;
+    if (curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS)
+        throw std::runtime_error("curandCreateGenerator failed");
+    curandStatus_t st = curandSetStream(gen, stream_);
+    if (st == CURAND_STATUS_SUCCESS)
+        st = curandSetPseudoRandomGeneratorSeed(gen, seed_);
+    if (st == CURAND_STATUS_SUCCESS)
+        st = curandGenerateNormalDouble(gen, reinterpret_cast<double *>(state_), 2ull << n_, 0.0, 1.0);
+    curandDestroyGenerator(gen);
+    if (st != CURAND_STATUS_SUCCESS)
+        throw std::runtime_error(strformat("cuRAND failed with status %d", (int)st));
+    ++stats.kernel_launches;
+}
+
+void Simulator::ensure_staging()
+{
+    if (staging_dev_ != nullptr)
+        return;
+    staging_count_ = std::min<uint64_t>(kStagingAmps, 1ull << n_);
+    QCSB_CUDA(cudaMalloc(&staging_dev_, sizeof(double2) * staging_count_));
+    QCSB_CUDA(cudaMallocHost(&staging_host_, sizeof(double2) * staging_count_));
+}
+
+// Move the whole register between device (physical order) and host (logical
+// order) through the pinned staging buffer, one chunk at a time.
+void Simulator::logical_transfer(double *host, uint64_t count, bool to_host)
+{
+    (void)count;
+    ensure_staging();
+    const uint64_t total = 1ull << n_;
+    const bool ident = identity_mapping();
+    for (uint64_t begin = 0; begin < total; begin += staging_count_)
+    {
+        const uint64_t cnt = std::min<uint64_t>(staging_count_, total - begin);
+        const size_t bytes = sizeof(double2) * cnt;
+        if (to_host)
+        {
+            const double2 *src = state_ + begin;
+            if (!ident)
+            {
+                stats.kernel_launches += launch_gather_logical(state_, n_, perm_l2p_.data(), begin, cnt, staging_dev_, stream_);
+                src = staging_dev_;
+            }
+            QCSB_CUDA(cudaMemcpyAsync(staging_host_, src, bytes, cudaMemcpyDeviceToHost, stream_));
+            QCSB_CUDA(cudaStreamSynchronize(stream_));
+            std::memcpy(host + 2 * begin, staging_host_, bytes);
+        }
+        else
+        {
+            std::memcpy(staging_host_, host + 2 * begin, bytes);
+            double2 *dst = ident ? state_ + begin : staging_dev_;
+            QCSB_CUDA(cudaMemcpyAsync(dst, staging_host_, bytes, cudaMemcpyHostToDevice, stream_));
+            if (!ident)
+                stats.kernel_launches += launch_scatter_logical(state_, n_, perm_l2p_.data(), begin, cnt, staging_dev_, stream_);
+            QCSB_CUDA(cudaStreamSynchronize(stream_));
+        }
+    }
+}
+
+void Simulator::save_statevector(const char *path)
+{
+    // reference save_statevector, src/qcs.cu:2494-2543: raw complex128 in
+    // logical index order. Written sequentially, one chunk at a time.
+    require_allocated("save_statevector");
+    if (path == nullptr)
+        throw std::runtime_error("save_statevector: output path must not be NULL");
+    flush();
+    FILE *fp = std::fopen(path, "wb");
+    if (fp == nullptr)
+        throw std::runtime_error("open failed");
+    ensure_staging();
+    const uint64_t total = 1ull << n_;
+    const bool ident = identity_mapping();
+    for (uint64_t begin = 0; begin < total; begin += staging_count_)
+    {
+        const uint64_t cnt = std::min<uint64_t>(staging_count_, total - begin);
+        const double2 *src = state_ + begin;
+        if (!ident)
+        {
+            stats.kernel_launches += launch_gather_logical(state_, n_, perm_l2p_.data(), begin, cnt, staging_dev_, stream_);
+            src = staging_dev_;
+        }
+        QCSB_CUDA(cudaMemcpyAsync(staging_host_, src, sizeof(double2) * cnt, cudaMemcpyDeviceToHost, stream_));
+        QCSB_CUDA(cudaStreamSynchronize(stream_));
+        if (std::fwrite(staging_host_, sizeof(double2), cnt, fp) != cnt)
+        {
+            std::fclose(fp);
+            throw std::runtime_error("fwrite failed");
+        }
+    }
+    std::fflush(fp);
+    std::fclose(fp);
+}
+
+void Simulator::get_statevector(double *out, uint64_t count)
+{
+    require_allocated("get_statevector");
+    if (out == nullptr)
+        throw std::runtime_error("get_statevector: output pointer must not be NULL");
+    if (count < (1ull << n_))
+        throw std::runtime_error(strformat("get_statevector: buffer holds %llu amplitudes, the register has %llu",
+                                           (unsigned long long)count, (unsigned long long)(1ull << n_)));
+    flush();
+    logical_transfer(out, count, true);
+}
+
+void Simulator::set_statevector(const double *in, uint64_t count)
+{
+    require_allocated("set_statevector");
+    if (in == nullptr)
+        throw std::runtime_error("set_statevector: input pointer must not be NULL");
+    if (count != (1ull << n_))
+        throw std::runtime_error(strformat("set_statevector: got %llu amplitudes, the register has %llu",
+                                           (unsigned long long)count, (unsigned long long)(1ull << n_)));
+    discard_pending();
+    clear_measurement_state();
+    logical_transfer(const_cast<double *>(in), count, false);
+}
+
+void Simulator::expectation_z(double *out, double *norm)
+{
+    require_allocated("expectation_z");
+    if (out == nullptr)
+        throw std::runtime_error("expectation_z: output pointer must not be NULL");
+    flush();
+    stats.kernel_launches += launch_zsums(state_, n_, zsum_partials_, zsum_result_, stream_);
+    double *h = static_cast<double *>(host_pinned_);
+    QCSB_CUDA(cudaMemcpyAsync(h, zsum_result_, sizeof(double) * (n_ + 1), cudaMemcpyDeviceToHost, stream_));
+    QCSB_CUDA(cudaStreamSynchronize(stream_));
+    const double total = h[0];
+    for (int q = 0; q < n_; ++q)
+    {
+        const double p1 = h[1 + perm_l2p_[q]];
+        out[q] = total > 0.0 ? (total - 2.0 * p1) / total : 0.0;
+    }
+    if (norm)
+        *norm = total;
+}
+
+void Simulator::sample(uint32_t num_shots, uint64_t *out)
+{
+    require_allocated("sample");
+    if (n_ > 64)
+        throw std::runtime_error("sample: more than 64 qubits do not fit a 64-bit outcome");
+    if (num_shots > 0 && out == nullptr)
+        throw std::runtime_error("sample: output pointer must not be NULL");
+    flush();
+    int split = 0;
+    const size_t tree_bytes = sampler_tree_bytes(n_, &split);
+    const size_t nu = (size_t)num_shots * n_;
+    const size_t need_host = std::max(sizeof(double) * nu, sizeof(uint64_t) * (size_t)num_shots);
+    if (need_host > host_pinned_bytes_)
+    {
+        QCSB_CUDA(cudaStreamSynchronize(stream_));
+        QCSB_CUDA(cudaFreeHost(host_pinned_));
+        host_pinned_ = nullptr;
+        host_pinned_bytes_ = need_host;
+        QCSB_CUDA(cudaMallocHost(&host_pinned_, host_pinned_bytes_));
+    }
+    double *u = static_cast<double *>(host_pinned_);
+    // same draws, in the same order, as num_shots rounds of measuring
+    // qubits 0..n-1 (src/qcs.cu:2615-2617)
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    for (size_t k = 0; k < nu; ++k)
+        u[k] = dist(engine_);
+    double *tree = nullptr, *u_dev = nullptr;
+    uint64_t *bits_dev = nullptr;
+    QCSB_CUDA(cudaMallocAsync(&tree, tree_bytes, stream_));
+    QCSB_CUDA(cudaMallocAsync(&u_dev, sizeof(double) * std::max<size_t>(nu, 1), stream_));
+    QCSB_CUDA(cudaMallocAsync(&bits_dev, sizeof(uint64_t) * std::max<uint32_t>(num_shots, 1), stream_));
+    QCSB_CUDA(cudaMemcpyAsync(u_dev, u, sizeof(double) * nu, cudaMemcpyHostToDevice, stream_));
+    stats.kernel_launches += launch_sampler(state_, n_, perm_l2p_.data(), num_shots, u_dev, bits_dev, tree, split, stream_);
+    QCSB_CUDA(cudaStreamSynchronize(stream_));   // the pinned buffer is reused below
+    QCSB_CUDA(cudaMemcpyAsync(host_pinned_, bits_dev, sizeof(uint64_t) * num_shots, cudaMemcpyDeviceToHost, stream_));
+    QCSB_CUDA(cudaFreeAsync(tree, stream_));
+    QCSB_CUDA(cudaFreeAsync(u_dev, stream_));
+    QCSB_CUDA(cudaFreeAsync(bits_dev, stream_));
+    QCSB_CUDA(cudaStreamSynchronize(stream_));
+    std::memcpy(out, host_pinned_, sizeof(uint64_t) * num_shots);
+}
+
+KernelTimer::~KernelTimer()
+{
+    clear();
+    for (cudaEvent_t e : pool_)
+        cudaEventDestroy(e);
+}
+
+cudaEvent_t KernelTimer::take()
+{
+    if (!pool_.empty())
+    {
+        cudaEvent_t e = pool_.back();
+        pool_.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    QCSB_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void KernelTimer::begin(cudaStream_t stream, int cls, double bytes)
+{
+    Rec r{cls, bytes, take(), take()};
+    QCSB_CUDA(cudaEventRecord(r.a, stream));
+    recs_.push_back(r);
+}
+
+void KernelTimer::end(cudaStream_t stream) { QCSB_CUDA(cudaEventRecord(recs_.back().b, stream)); }
+
+void KernelTimer::collect(qcs_b200_kernel_times &out)
+{
+    out = qcs_b200_kernel_times{};
+    for (const Rec &r : recs_)
+    {
+        QCSB_CUDA(cudaEventSynchronize(r.b));
+        float ms = 0.0f;
+        QCSB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        if (r.cls == kFused)
+        {
+            ++out.fused_launches;
+            out.fused_ms += ms;
+            out.fused_bytes += r.bytes;
+        }
+        else
+        {
+            ++out.plain_launches;
+            out.plain_ms += ms;
+            out.plain_bytes += r.bytes;
+        }
+    }
+    clear();
+}
+
+void KernelTimer::clear()
+{
+    for (const Rec &r : recs_)
+    {
+        pool_.push_back(r.a);
+        pool_.push_back(r.b);
+    }
+    recs_.clear();
+}
+
+int Simulator::event_create()
+{
+    if (disposed_)
+        throw std::runtime_error("event_create: the simulator has been disposed");
+    cudaEvent_t e;
+    QCSB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDefault));
+    events_.push_back(e);
+    return (int)events_.size() - 1;
+}
+
+void Simulator::event_record(int event_num)
+{
+    if (disposed_)
+        throw std::runtime_error("event_record: the simulator has been disposed");
+    if (event_num < 0 || event_num >= (int)events_.size())
+        throw std::runtime_error(strformat("event %d does not exist", event_num));
+    flush();
+    QCSB_CUDA(cudaEventRecordWithFlags(events_[event_num], stream_, cudaEventDefault));
+}
+
+double Simulator::event_elapsed(int start, int stop)
+{
+    // reference event_get_elapsed_time, src/qcs.cu:2862-2897: seconds
+    if (disposed_)
+        throw std::runtime_error("event_get_elapsed_time: the simulator has been disposed");
+    for (int e : {start, stop})
+        if (e < 0 || e >= (int)events_.size())
+            throw std::runtime_error(strformat("event %d does not exist", e));
+    QCSB_CUDA(cudaEventSynchronize(events_[start]));
+    QCSB_CUDA(cudaEventSynchronize(events_[stop]));
+    float ms = 0.0f;
+    QCSB_CUDA(cudaEventElapsedTime(&ms, events_[start], events_[stop]));
+    return ms * 1e-3;
+}
+
+} // namespace qcsb

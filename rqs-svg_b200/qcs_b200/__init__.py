@@ -1,0 +1,341 @@
+"""ctypes binding of the qcs C API (include/qcs.h, include/qcs_b200.h).
+
+The same binding drives any library that exports the reference's C ABI:
+the B200 library (rqs-svg_b200/lib/libqcs.so), and -- in the tests only --
+the CPU oracle and the reference build. Calls mirror the C functions one to
+one (reference src/qcs.cu:3383-3759); a 0 return raises QCSError carrying the
+message the library passed to its exception callback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent.parent
+REPO_DIR = PKG_DIR.parent
+LIB_PATH = PKG_DIR / "lib" / "libqcs.so"
+CLI_PATH = PKG_DIR / "bin" / "qcs"
+
+bit_num_t = ctypes.c_int16
+bit_t = ctypes.c_uint8
+event_num_t = ctypes.c_int16
+_P = ctypes.c_void_p
+_BN = ctypes.POINTER(bit_num_t)
+
+# name -> (number of double parameters, number of targets)
+GATES = {
+    "global_phase": (1, 0),
+    "h": (0, 1), "x": (0, 1), "y": (0, 1), "z": (0, 1), "s": (0, 1), "sdg": (0, 1),
+    "t": (0, 1), "tdg": (0, 1), "sx": (0, 1), "sxdg": (0, 1), "id": (0, 1),
+    "rx": (1, 1), "ry": (1, 1), "rz": (1, 1), "u1": (1, 1), "p": (1, 1),
+    "u2": (2, 1), "r": (2, 1), "u3": (3, 1), "u": (3, 1), "u4": (4, 1),
+    "swap": (0, 2), "iswap": (0, 2), "dcx": (0, 2), "ecr": (0, 2),
+    "rxx": (1, 2), "ryy": (1, 2), "rzz": (1, 2), "rzx": (1, 2),
+    "xx_plus_yy": (2, 2), "xx_minus_yy": (2, 2),
+    "rccx": (0, 3), "rcccx": (0, 4),
+}
+
+FUSION_PLAIN, FUSION_GREEDY, FUSION_LEARNED = 0, 1, 2
+
+
+class QCSError(RuntimeError):
+    pass
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("kernel_launches", ctypes.c_uint64),
+        ("gates_received", ctypes.c_uint64),
+        ("gates_applied", ctypes.c_uint64),
+        ("fused_passes", ctypes.c_uint64),
+        ("plain_gate_kernels", ctypes.c_uint64),
+        ("algorithmic_bytes", ctypes.c_double),
+    ]
+
+
+class KernelTimes(ctypes.Structure):
+    _fields_ = [
+        ("fused_launches", ctypes.c_uint64),
+        ("fused_ms", ctypes.c_double),
+        ("fused_bytes", ctypes.c_double),
+        ("plain_launches", ctypes.c_uint64),
+        ("plain_ms", ctypes.c_double),
+        ("plain_bytes", ctypes.c_double),
+    ]
+
+
+_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_char_p, ctypes.c_size_t)
+
+
+class Library:
+    """One loaded implementation of the qcs C API."""
+
+    def __init__(self, path: str | os.PathLike = LIB_PATH, mode: int = ctypes.RTLD_LOCAL):
+        self.path = str(path)
+        if not os.path.exists(self.path):
+            raise QCSError(f"{self.path} is missing: build it with `make -C rqs-svg_b200`")
+        self.lib = ctypes.CDLL(self.path, mode=mode)
+        self.last_error = ""
+
+        def _on_error(msg, length):
+            self.last_error = ctypes.string_at(msg, length).decode(errors="replace")
+
+        self._cb = _CALLBACK(_on_error)
+        self.lib.qcs_set_exception_callback.argtypes = [_CALLBACK]
+        self.lib.qcs_set_exception_callback(self._cb)
+        self._declare()
+
+    def has(self, name: str) -> bool:
+        return hasattr(self.lib, name)
+
+    def _declare(self):
+        L = self.lib
+        sig = {
+            "qcs_simulator_create": [ctypes.POINTER(_P)],
+            "qcs_simulator_destroy": [_P],
+            "qcs_simulator_allocate_memory": [_P],
+            "qcs_simulator_dispose": [_P],
+            "qcs_simulator_get_num_procs": [_P, ctypes.POINTER(bit_t)],
+            "qcs_simulator_get_proc_num": [_P, ctypes.POINTER(bit_t)],
+            "qcs_simulator_get_num_qubits": [_P, ctypes.POINTER(bit_t)],
+            "qcs_simulator_get_num_clbits": [_P, ctypes.POINTER(bit_t)],
+            "qcs_simulator_set_num_qubits": [_P, bit_num_t],
+            "qcs_simulator_set_mapping": [_P, _BN, bit_num_t],
+            "qcs_simulator_set_num_clbits": [_P, bit_num_t],
+            "qcs_simulator_get_clbits": [_P, ctypes.POINTER(bit_t)],
+            "qcs_simulator_get_clbits_string": [_P, ctypes.c_char_p],
+            "qcs_simulator_reset": [_P, bit_num_t],
+            "qcs_simulator_set_zero_state": [_P],
+            "qcs_simulator_set_sequential_state": [_P],
+            "qcs_simulator_set_flat_state": [_P],
+            "qcs_simulator_set_entangled_state": [_P],
+            "qcs_simulator_set_random_state": [_P],
+            "qcs_simulator_reset_clbits": [_P],
+            "qcs_simulator_reset_measurement_state": [_P],
+            "qcs_simulator_reinitialize_mapping": [_P],
+            "qcs_simulator_gate_global_phase": [_P, ctypes.c_double, _BN, bit_num_t, _BN, bit_num_t],
+            "qcs_simulator_measure": [_P, bit_num_t, ctypes.POINTER(bit_t)],
+            "qcs_simulator_measure_to_clbit": [_P, bit_num_t, bit_num_t, ctypes.POINTER(bit_t)],
+            "qcs_simulator_read": [_P, bit_num_t, ctypes.POINTER(bit_t)],
+            "qcs_simulator_save_statevector": [_P, ctypes.c_char_p],
+            "qcs_simulator_event_create": [_P, ctypes.POINTER(bit_t)],
+            "qcs_simulator_event_record": [_P, ctypes.c_int],
+            "qcs_simulator_event_get_elapsed_time": [_P, event_num_t, event_num_t, ctypes.POINTER(ctypes.c_double)],
+            # extensions (absent from the reference build)
+            "qcs_simulator_set_fusion": [_P, ctypes.c_int],
+            "qcs_simulator_get_fusion": [_P, ctypes.POINTER(ctypes.c_int)],
+            "qcs_simulator_set_seed": [_P, ctypes.c_uint32],
+            "qcs_simulator_synchronize": [_P],
+            "qcs_simulator_get_statevector": [_P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
+            "qcs_simulator_set_statevector": [_P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
+            "qcs_simulator_expectation_z": [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+            "qcs_simulator_sample": [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)],
+            "qcs_simulator_get_stats": [_P, ctypes.POINTER(Stats)],
+            "qcs_simulator_reset_stats": [_P],
+            "qcs_simulator_set_kernel_timing": [_P, ctypes.c_int],
+            "qcs_simulator_get_kernel_times": [_P, ctypes.POINTER(KernelTimes)],
+        }
+        for name, (np_, nt) in GATES.items():
+            if name == "global_phase":
+                continue
+            sig[f"qcs_simulator_gate_{name}"] = [_P] + [ctypes.c_double] * np_ + [_BN, bit_num_t, _BN, bit_num_t, _BN, bit_num_t]
+        for name, args in sig.items():
+            if hasattr(L, name):
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = ctypes.c_int
+
+    def call(self, name: str, *args) -> None:
+        self.last_error = ""
+        ok = getattr(self.lib, name)(*args)
+        if ok != 1:
+            raise QCSError(f"{name} failed: {self.last_error}")
+
+
+def _arr(values):
+    values = list(values)
+    if not values:
+        return None, 0
+    return (bit_num_t * len(values))(*values), len(values)
+
+
+class Simulator:
+    """A qcs_simulator handle: create, configure, allocate, run, destroy."""
+
+    def __init__(self, lib: Library, num_qubits: int, num_clbits: int = 0, mapping=None,
+                 seed: int | None = None, fusion: int | None = None, allocate: bool = True):
+        self.lib = lib
+        self.n = num_qubits
+        self.h = _P()
+        lib.call("qcs_simulator_create", ctypes.byref(self.h))
+        lib.call("qcs_simulator_set_num_qubits", self.h, num_qubits)
+        if num_clbits:
+            lib.call("qcs_simulator_set_num_clbits", self.h, num_clbits)
+        if mapping is not None:
+            arr, cnt = _arr(mapping)
+            lib.call("qcs_simulator_set_mapping", self.h, arr, cnt)
+        if seed is not None:
+            lib.call("qcs_simulator_set_seed", self.h, seed)
+        if fusion is not None and lib.has("qcs_simulator_set_fusion"):
+            lib.call("qcs_simulator_set_fusion", self.h, fusion)
+        if allocate:
+            lib.call("qcs_simulator_allocate_memory", self.h)
+
+    # -- lifecycle
+    def close(self):
+        if self.h:
+            self.lib.call("qcs_simulator_destroy", self.h)
+            self.h = _P()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- gates
+    def gate(self, name: str, params=(), targets=(), negctrls=(), ctrls=()):
+        t, nt = _arr(targets)
+        ng, nng = _arr(negctrls)
+        c, nc = _arr(ctrls)
+        if name == "global_phase":
+            self.lib.call("qcs_simulator_gate_global_phase", self.h, float(params[0]), ng, nng, c, nc)
+        else:
+            self.lib.call(f"qcs_simulator_gate_{name}", self.h, *[float(p) for p in params], t, nt, ng, nng, c, nc)
+
+    def run(self, circuit):
+        """Replay a circuit: a list of (op, params, targets, negctrls, ctrls);
+        op "measure" takes targets=(qubit,) and params=(clbit,)."""
+        for op, params, targets, negctrls, ctrls in circuit:
+            if op == "measure":
+                self.measure_to_clbit(targets[0], int(params[0]))
+            else:
+                self.gate(op, params, targets, negctrls, ctrls)
+
+    # -- measurement and classical bits
+    def measure(self, q: int) -> int:
+        r = bit_t()
+        self.lib.call("qcs_simulator_measure", self.h, q, ctypes.byref(r))
+        return r.value
+
+    def measure_to_clbit(self, q: int, c: int) -> int:
+        r = bit_t()
+        self.lib.call("qcs_simulator_measure_to_clbit", self.h, q, c, ctypes.byref(r))
+        return r.value
+
+    def read(self, c: int) -> int:
+        r = bit_t()
+        self.lib.call("qcs_simulator_read", self.h, c, ctypes.byref(r))
+        return r.value
+
+    def reset(self, q: int):
+        self.lib.call("qcs_simulator_reset", self.h, q)
+
+    def clbits_string(self) -> str:
+        n = bit_t()
+        self.lib.call("qcs_simulator_get_num_clbits", self.h, ctypes.byref(n))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        self.lib.call("qcs_simulator_get_clbits_string", self.h, buf)
+        return buf.value.decode()
+
+    # -- state preparation and bookkeeping
+    def set_state(self, kind: str):
+        self.lib.call(f"qcs_simulator_set_{kind}_state", self.h)
+
+    def reset_clbits(self):
+        self.lib.call("qcs_simulator_reset_clbits", self.h)
+
+    def reset_measurement_state(self):
+        self.lib.call("qcs_simulator_reset_measurement_state", self.h)
+
+    def reinitialize_mapping(self):
+        self.lib.call("qcs_simulator_reinitialize_mapping", self.h)
+
+    # -- output
+    def save_statevector(self, path: str):
+        self.lib.call("qcs_simulator_save_statevector", self.h, str(path).encode())
+
+    def statevector(self) -> np.ndarray:
+        """State in logical order as complex128 (through save_statevector
+        when the library has no get_statevector, as for the reference)."""
+        size = 1 << self.n
+        if self.lib.has("qcs_simulator_get_statevector"):
+            out = np.empty(2 * size, dtype=np.float64)
+            self.lib.call("qcs_simulator_get_statevector", self.h,
+                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), size)
+            return out.view(np.complex128)
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "sv.bin")
+            self.save_statevector(p)
+            return np.fromfile(p, dtype=np.complex128)
+
+    def set_statevector(self, amps: np.ndarray):
+        a = np.ascontiguousarray(amps, dtype=np.complex128).view(np.float64)
+        self.lib.call("qcs_simulator_set_statevector", self.h,
+                      a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size // 2)
+
+    def expectation_z(self):
+        out = np.empty(self.n, dtype=np.float64)
+        norm = ctypes.c_double()
+        self.lib.call("qcs_simulator_expectation_z", self.h,
+                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(norm))
+        return out, norm.value
+
+    def sample(self, shots: int) -> np.ndarray:
+        out = np.zeros(shots, dtype=np.uint64)
+        self.lib.call("qcs_simulator_sample", self.h, shots,
+                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+        return out
+
+    def synchronize(self):
+        self.lib.call("qcs_simulator_synchronize", self.h)
+
+    def set_fusion(self, mode: int):
+        self.lib.call("qcs_simulator_set_fusion", self.h, mode)
+
+    def set_seed(self, seed: int):
+        self.lib.call("qcs_simulator_set_seed", self.h, seed)
+
+    # -- events
+    def event_create(self) -> int:
+        r = bit_t()
+        self.lib.call("qcs_simulator_event_create", self.h, ctypes.byref(r))
+        return r.value
+
+    def event_record(self, e: int):
+        self.lib.call("qcs_simulator_event_record", self.h, e)
+
+    def elapsed(self, a: int, b: int) -> float:
+        r = ctypes.c_double()
+        self.lib.call("qcs_simulator_event_get_elapsed_time", self.h, a, b, ctypes.byref(r))
+        return r.value
+
+    def stats(self) -> dict:
+        s = Stats()
+        self.lib.call("qcs_simulator_get_stats", self.h, ctypes.byref(s))
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def reset_stats(self):
+        self.lib.call("qcs_simulator_reset_stats", self.h)
+
+    def set_kernel_timing(self, enable: bool):
+        self.lib.call("qcs_simulator_set_kernel_timing", self.h, 1 if enable else 0)
+
+    def kernel_times(self) -> dict:
+        t = KernelTimes()
+        self.lib.call("qcs_simulator_get_kernel_times", self.h, ctypes.byref(t))
+        return {f: getattr(t, f) for f, _ in KernelTimes._fields_}
+
+
+def fidelity(a: np.ndarray, b: np.ndarray) -> float:
+    """|<a|b>|^2 / (<a|a><b|b>)."""
+    na = np.vdot(a, a).real
+    nb = np.vdot(b, b).real
+    if na == 0 or nb == 0:
+        return 1.0 if na == nb else 0.0
+    return float(abs(np.vdot(a, b)) ** 2 / (na * nb))

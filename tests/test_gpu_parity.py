@@ -1,0 +1,295 @@
+"""Parity of the B200 library with the oracle and the reference fixtures.
+
+Every test drives the CUDA library through its C ABI (ctypes) in both
+execution modes: plain (one kernel per gate) and greedy (fused passes).
+Tolerances: complex128 amplitudes agree to 1e-12 absolute (states of norm
+<= 1, or scaled by the largest amplitude), fidelity >= 1 - 1e-12; shot
+outcomes and clbits are compared exactly (same seed, same uniforms).
+"""
+
+import filecmp
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import golden_cases
+import qcs_b200
+from qcs_b200 import GATES, FUSION_GREEDY, FUSION_PLAIN
+from qcs_b200 import circuits as C
+
+pytestmark = pytest.mark.gpu
+
+MODES = [FUSION_PLAIN, FUSION_GREEDY]
+TOL = 1e-12
+
+
+def _run(lib, n, circ, fusion=None, seed=1, mapping=None, start=None, num_clbits=0):
+    with qcs_b200.Simulator(lib, n, num_clbits or n, seed=seed, mapping=mapping, fusion=fusion) as sim:
+        if start is not None:
+            sim.set_statevector(start)
+        sim.run(circ)
+        return sim.statevector(), sim.clbits_string()
+
+
+def _random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("name", sorted(GATES))
+def test_every_gate_kind(gpu_lib, oracle_lib, name, mode):
+    for n in (3, 6, 9, 13):
+        circ = C.random_circuit(n, 30, seed=n * 131 + sum(map(ord, name)), max_controls=3, gates=[name])
+        start = _random_state(n, n)
+        got, _ = _run(gpu_lib, n, circ, fusion=mode, start=start)
+        ref, _ = _run(oracle_lib, n, circ, start=start)
+        assert np.max(np.abs(got - ref)) <= TOL, (name, n)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("n", [1, 2, 5, 8, 11, 12, 16])
+def test_mixed_random_circuits(gpu_lib, oracle_lib, n, mode):
+    circ = C.random_circuit(n, 200, seed=1000 + n, max_controls=3)
+    start = _random_state(n, 7)
+    got, _ = _run(gpu_lib, n, circ, fusion=mode, start=start)
+    ref, _ = _run(oracle_lib, n, circ, start=start)
+    assert np.max(np.abs(got - ref)) <= TOL
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_twenty_qubit_layered_and_qft(gpu_lib, oracle_lib, mode):
+    for circ in (C.layered_u3_cz(20, 6, seed=3), C.qft(20, seed=4)[0], C.layered_u3_cz_cx_toffoli(20, 4, seed=5)):
+        got, _ = _run(gpu_lib, 20, circ, fusion=mode)
+        ref, _ = _run(oracle_lib, 20, circ)
+        assert np.max(np.abs(got - ref)) <= TOL
+        assert qcs_b200.fidelity(got, ref) >= 1 - 1e-12
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_measurements_match_oracle(gpu_lib, oracle_lib, mode):
+    for n, seed in [(5, 1), (8, 2), (12, 3), (14, 4)]:
+        circ = [("h", (), (q,), (), ()) for q in range(n)]
+        circ += C.random_circuit(n, 80, seed=seed, max_controls=2, measure_prob=0.1)
+        circ += [("measure", (q,), (q,), (), ()) for q in range(n)]
+        for rng_seed in (7, 8):
+            got, gbits = _run(gpu_lib, n, circ, fusion=mode, seed=rng_seed)
+            ref, rbits = _run(oracle_lib, n, circ, seed=rng_seed)
+            assert gbits == rbits
+            assert np.max(np.abs(got - ref)) <= TOL
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_mapping_and_saved_file(gpu_lib, oracle_lib, mode):
+    n = 9
+    mapping = [4, 8, 0, 2, 7, 1, 3, 6, 5]
+    circ = C.random_circuit(n, 120, seed=55, max_controls=2)
+    with tempfile.TemporaryDirectory() as d:
+        files = []
+        for lib, fus in ((gpu_lib, mode), (oracle_lib, None)):
+            with qcs_b200.Simulator(lib, n, mapping=mapping, seed=3, fusion=fus) as sim:
+                sim.run(circ)
+                p = os.path.join(d, f"{len(files)}.bin")
+                sim.save_statevector(p)
+                files.append(p)
+        a = np.fromfile(files[0], dtype=np.complex128)
+        b = np.fromfile(files[1], dtype=np.complex128)
+        assert a.size == b.size == 1 << n
+        assert np.max(np.abs(a - b)) <= TOL
+
+
+def test_saved_file_bytes_equal_state(gpu_lib):
+    n = 23   # several staging chunks
+    with qcs_b200.Simulator(gpu_lib, n) as sim:
+        sim.run(C.layered_u3_cz(n, 2, seed=9))
+        sv = sim.statevector()
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "s.bin")
+            sim.save_statevector(p)
+            assert np.array_equal(np.fromfile(p, dtype=np.complex128), sv)
+
+
+@pytest.mark.parametrize("prep", ["zero", "flat", "sequential", "random"])
+def test_state_preparations(gpu_lib, oracle_lib, prep):
+    n = 10
+    circ = C.random_circuit(n, 40, seed=66, max_controls=1)
+    out = []
+    for lib in (gpu_lib, oracle_lib):
+        with qcs_b200.Simulator(lib, n, seed=4242) as sim:
+            sim.set_state(prep)
+            sim.run(circ)
+            out.append(sim.statevector())
+    scale = max(1.0, float(np.max(np.abs(out[1]))))
+    assert np.max(np.abs(out[0] - out[1])) <= TOL * scale
+
+
+def test_entangled_keeps_other_amplitudes(gpu_lib, oracle_lib):
+    out = []
+    for lib in (gpu_lib, oracle_lib):
+        with qcs_b200.Simulator(lib, 6, seed=1) as sim:
+            sim.run(C.random_circuit(6, 30, seed=3))
+            sim.set_state("entangled")
+            out.append(sim.statevector())
+    assert out[0][0] == 1.0
+    assert np.max(np.abs(out[0] - out[1])) <= TOL
+
+
+def test_expectation_z_matches_oracle(gpu_lib, oracle_lib):
+    for n in (4, 12, 15):
+        circ = C.layered_u3_cz(n, 3, seed=n)
+        res = []
+        for lib in (gpu_lib, oracle_lib):
+            with qcs_b200.Simulator(lib, n, mapping=list(reversed(range(n)))) as sim:
+                sim.run(circ)
+                res.append(sim.expectation_z())
+        assert np.max(np.abs(res[0][0] - res[1][0])) <= 1e-12
+        assert abs(res[0][1] - res[1][1]) <= 1e-12
+
+
+@pytest.mark.parametrize("n", [3, 10, 21, 24])
+def test_sampler_matches_sequential_measurement(gpu_lib, oracle_lib, n):
+    circ = C.layered_u3_cz(n, 3, seed=n + 1)
+    shots = 256 if n <= 10 else 64
+    with qcs_b200.Simulator(gpu_lib, n, seed=31337) as sim:
+        sim.run(circ)
+        got = [int(v) for v in sim.sample(shots)]
+    if n <= 10:
+        with qcs_b200.Simulator(oracle_lib, n, seed=31337) as sim:
+            sim.run(circ)
+            ref = [int(v) for v in sim.sample(shots)]
+    else:
+        # same rule through the library's own measure() path
+        ref = []
+        with qcs_b200.Simulator(gpu_lib, n, seed=31337) as sim:
+            sim.run(circ)
+            sv0 = sim.statevector()
+            for _ in range(shots):
+                ref.append(sum(sim.measure(q) << q for q in range(n)))
+                sim.set_statevector(sv0)
+    assert got == ref
+
+
+def test_sampler_does_not_change_state(gpu_lib):
+    with qcs_b200.Simulator(gpu_lib, 12, seed=5) as sim:
+        sim.run(C.layered_u3_cz(12, 3, seed=1))
+        before = sim.statevector()
+        sim.sample(100)
+        assert np.array_equal(before, sim.statevector())
+
+
+def test_plain_and_fused_agree_at_24_qubits(gpu_lib):
+    n = 24
+    circ = C.layered_u3_cz_cx_toffoli(n, 4, seed=11) + C.qft(n, seed=12)[0]
+    a, _ = _run(gpu_lib, n, circ, fusion=FUSION_PLAIN)
+    b, _ = _run(gpu_lib, n, circ, fusion=FUSION_GREEDY)
+    assert np.max(np.abs(a - b)) <= TOL
+    assert abs(np.vdot(a, a).real - 1.0) <= 1e-12
+
+
+def test_inverse_circuit_returns_to_zero_at_28_qubits(gpu_lib):
+    # size-independent property: U followed by U^dagger is the identity
+    n = 28
+    fwd = C.random_circuit(n, 120, seed=21, max_controls=2,
+                           gates=["h", "x", "u3", "rx", "ry", "rz", "p", "swap", "rzz", "rxx"])
+    inv = []
+    for op, params, t, neg, pos in reversed(fwd):
+        if op == "u3":
+            th, ph, la = params
+            inv.append(("u3", (-th, -la, -ph), t, neg, pos))
+        elif op in ("rx", "ry", "rz", "p", "rzz", "rxx"):
+            inv.append((op, (-params[0],), t, neg, pos))
+        else:
+            inv.append((op, params, t, neg, pos))
+    with qcs_b200.Simulator(gpu_lib, n) as sim:
+        sim.run(fwd + inv)
+        z, norm = sim.expectation_z()
+        assert abs(norm - 1.0) <= 1e-11
+        assert np.all(np.abs(z - 1.0) <= 1e-11)
+
+
+# ------------------------------------------------------------ reference fixtures
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("case", golden_cases.cases(), ids=lambda c: c["name"])
+def test_matches_reference_golden(gpu_lib, case, mode):
+    g = np.load(golden_cases_path())
+    key = case["name"]
+    with qcs_b200.Simulator(gpu_lib, case["n"], case["num_clbits"], mapping=case["mapping"],
+                            seed=golden_cases.SEED, fusion=mode) as sim:
+        shots, state = golden_cases.run_case(sim, case)
+    ref = g[f"{key}/state"]
+    assert list(g[f"{key}/shots"]) == shots
+    scale = max(1.0, float(np.max(np.abs(ref))))
+    assert np.max(np.abs(state - ref)) <= TOL * scale
+
+
+def golden_cases_path():
+    from pathlib import Path
+
+    p = Path(__file__).resolve().parent / "golden" / "reference_golden.npz"
+    if not p.exists():
+        pytest.fail(f"{p} is missing")
+    return p
+
+
+# ------------------------------------------------------------ C ABI behaviour
+
+
+def test_error_convention(gpu_lib):
+    lib = gpu_lib
+    with qcs_b200.Simulator(lib, 4) as sim:
+        with pytest.raises(qcs_b200.QCSError, match="target"):
+            sim.gate("swap", (), (0,))
+        with pytest.raises(qcs_b200.QCSError, match="out of range"):
+            sim.gate("h", (), (4,))
+        with pytest.raises(qcs_b200.QCSError, match="more than once"):
+            sim.gate("x", (), (1,), (1,), ())
+        with pytest.raises(qcs_b200.QCSError, match="clbit"):
+            sim.measure_to_clbit(0, 9)
+        with pytest.raises(qcs_b200.QCSError, match="already"):
+            lib.call("qcs_simulator_allocate_memory", sim.h)
+        # NULL result pointer
+        assert lib.lib.qcs_simulator_measure(sim.h, 0, None) == 0
+        assert "NULL" in lib.last_error
+        # the simulator still works after errors
+        sim.gate("h", (), (0,))
+        assert abs(abs(sim.statevector()[1]) - 2 ** -0.5) < 1e-15
+
+
+def test_over_capacity_allocation_fails_cleanly(gpu_lib):
+    sim = qcs_b200.Simulator(gpu_lib, 40, allocate=False)
+    with pytest.raises(qcs_b200.QCSError, match="num_qubits"):
+        gpu_lib.call("qcs_simulator_allocate_memory", sim.h)
+    sim.close()
+
+
+def test_events_measure_elapsed_seconds(gpu_lib):
+    with qcs_b200.Simulator(gpu_lib, 20) as sim:
+        a, b = sim.event_create(), sim.event_create()
+        sim.event_record(a)
+        sim.run(C.layered_u3_cz(20, 2, seed=1))
+        sim.event_record(b)
+        t = sim.elapsed(a, b)
+        assert 0.0 < t < 10.0
+
+
+def test_dispose_then_use_is_an_error(gpu_lib):
+    sim = qcs_b200.Simulator(gpu_lib, 3)
+    gpu_lib.call("qcs_simulator_dispose", sim.h)
+    with pytest.raises(qcs_b200.QCSError, match="disposed"):
+        sim.gate("h", (), (0,))
+    sim.close()
+
+
+def test_stats_count_launches(gpu_lib):
+    with qcs_b200.Simulator(gpu_lib, 16, fusion=FUSION_GREEDY) as sim:
+        sim.reset_stats()
+        sim.run(C.layered_u3_cz(16, 4, seed=2))
+        sim.synchronize()
+        st = sim.stats()
+        assert st["gates_received"] == 16 * 4 + 8 + 7 + 8 + 7
+        assert st["fused_passes"] >= 1 and st["kernel_launches"] >= st["fused_passes"]
