@@ -14,7 +14,8 @@
 // back. A non-diagonal gate must have its targets in S. Diagonal gates and
 // controls may sit on any qubit, local or not: every amplitude knows its full
 // index (local bits from its position, the rest from the chunk), so they are
-// evaluated per amplitude (or once per chunk).
+// evaluated per amplitude (or once per chunk). The host orders the pass's
+// gates into as few stages as their dependencies allow.
 //
 // Every gate is applied with its own FP64 matrix, in an order that respects
 // all dependencies, so the result equals the gate-by-gate result up to the
@@ -30,9 +31,11 @@ namespace qcsb
 namespace
 {
 
-constexpr int kFusedMaxOps = 48;
-constexpr int kFusedMaxStages = 24;
+constexpr int kFusedMaxOps = 64;
+constexpr int kFusedMaxStages = 40;
 constexpr int kLowBits = 3;      // qubits 0..2 are always local: 128-byte runs
+constexpr int kStageBits = 4;    // amplitudes per thread in a stage: 2^4
+constexpr int kDefaultLocal = 11;
 constexpr int kMaxLocal = 12;
 constexpr size_t kPlanWindow = 4096;   // ops scanned past the first pending one
 
@@ -40,26 +43,30 @@ enum FKind : uint8_t
 {
     F_DENSE1 = 0,  // 2x2 on one stage bit
     F_SWAP1 = 1,   // X: exchange the pair
-    F_DENSE2 = 2,  // 4x4 on two stage bits
+    F_DENSE2 = 2,  // 4x4 on two stage bits (b0 < b1)
     F_SWAP2 = 3,   // exchange sub-indices 01 and 10
-    F_DIAG = 4,    // diagonal on up to 4 targets anywhere
+    F_PHASE = 4,   // multiply by m[0] where the condition bits match
+    F_DIAG = 5,    // diagonal on one or two targets anywhere
 };
 
+// One gate of a pass. Conditions: (local index & lcmask) == lcval and
+// (physical chunk bits & gcmask) == gcval. For F_PHASE the condition includes
+// the target bits of the single changed sub-index.
 struct FOp
 {
     uint8_t kind;
     uint8_t nt;
-    uint8_t b0, b1;        // stage-bit positions (dense kinds)
-    int8_t loc[4];         // local bit of target i, -1 when outside Q (diag)
-    uint8_t phys[4];       // physical qubit of target i
-    uint32_t lcmask, lcval; // controls on local bits
-    uint64_t gcmask, gcval; // controls on non-local physical bits
+    uint8_t b0, b1;         // stage-bit positions (dense kinds)
+    int8_t loc[2];          // F_DIAG: local bit of target i, -1 when outside Q
+    uint8_t phys[2];        // F_DIAG: physical qubit of target i
+    uint32_t lcmask, lcval;
+    uint64_t gcmask, gcval;
     double2 m[16];
 };
 
 struct FStage
 {
-    uint8_t sbits[4];      // local bit positions of the stage, ascending
+    uint8_t sbits[kStageBits];   // local bit positions of the stage, ascending
     uint16_t op_begin, op_end;
 };
 
@@ -103,58 +110,63 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <int SB, int B>
-__device__ __forceinline__ void apply_dense1(double2 (&a)[1 << SB], const FOp &op, const uint32_t (&jr)[1 << SB])
+constexpr int R = 1 << kStageBits;
+
+template <int B>
+__device__ __forceinline__ void apply_dense1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     const double2 m00 = op.m[0], m01 = op.m[1], m10 = op.m[2], m11 = op.m[3];
+    const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
-    for (int r = 0; r < (1 << SB); ++r)
+    for (int r = 0; r < R; ++r)
     {
         if (r & (1 << B))
-            continue;
-        if ((jr[r] & op.lcmask) != op.lcval)
             continue;
         const int r1 = r | (1 << B);
         const double2 x0 = a[r], x1 = a[r1];
-        a[r] = cmad2(m00, x0, m01, x1);
-        a[r1] = cmad2(m10, x0, m11, x1);
+        const double2 y0 = cmad2(m00, x0, m01, x1);
+        const double2 y1 = cmad2(m10, x0, m11, x1);
+        const bool ok = (jr[r] & cm) == cv;
+        a[r] = ok ? y0 : x0;
+        a[r1] = ok ? y1 : x1;
     }
 }
 
-template <int SB, int B>
-__device__ __forceinline__ void apply_swap1(double2 (&a)[1 << SB], const FOp &op, const uint32_t (&jr)[1 << SB])
+template <int B>
+__device__ __forceinline__ void apply_swap1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
+    const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
-    for (int r = 0; r < (1 << SB); ++r)
+    for (int r = 0; r < R; ++r)
     {
         if (r & (1 << B))
             continue;
-        if ((jr[r] & op.lcmask) != op.lcval)
-            continue;
         const int r1 = r | (1 << B);
-        const double2 t = a[r];
-        a[r] = a[r1];
-        a[r1] = t;
+        const double2 x0 = a[r], x1 = a[r1];
+        const bool ok = (jr[r] & cm) == cv;
+        a[r] = ok ? x1 : x0;
+        a[r1] = ok ? x0 : x1;
     }
 }
 
-template <int SB, int B0, int B1>
-__device__ __forceinline__ void apply_dense2(double2 (&a)[1 << SB], const FOp &op, const uint32_t (&jr)[1 << SB])
+template <int B0, int B1>
+__device__ __forceinline__ void apply_dense2(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
+    const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
-    for (int r = 0; r < (1 << SB); ++r)
+    for (int r = 0; r < R; ++r)
     {
         if (r & ((1 << B0) | (1 << B1)))
             continue;
-        if ((jr[r] & op.lcmask) != op.lcval)
+        if ((jr[r] & cm) != cv)
             continue;
         const int i1 = r | (1 << B0), i2 = r | (1 << B1), i3 = r | (1 << B0) | (1 << B1);
         const double2 x0 = a[r], x1 = a[i1], x2 = a[i2], x3 = a[i3];
         const double2 *m = op.m;
-        double2 y0 = cmad2(m[0], x0, m[1], x1), t0 = cmad2(m[2], x2, m[3], x3);
-        double2 y1 = cmad2(m[4], x0, m[5], x1), t1 = cmad2(m[6], x2, m[7], x3);
-        double2 y2 = cmad2(m[8], x0, m[9], x1), t2 = cmad2(m[10], x2, m[11], x3);
-        double2 y3 = cmad2(m[12], x0, m[13], x1), t3 = cmad2(m[14], x2, m[15], x3);
+        const double2 y0 = cmad2(m[0], x0, m[1], x1), t0 = cmad2(m[2], x2, m[3], x3);
+        const double2 y1 = cmad2(m[4], x0, m[5], x1), t1 = cmad2(m[6], x2, m[7], x3);
+        const double2 y2 = cmad2(m[8], x0, m[9], x1), t2 = cmad2(m[10], x2, m[11], x3);
+        const double2 y3 = cmad2(m[12], x0, m[13], x1), t3 = cmad2(m[14], x2, m[15], x3);
         a[r] = make_double2(y0.x + t0.x, y0.y + t0.y);
         a[i1] = make_double2(y1.x + t1.x, y1.y + t1.y);
         a[i2] = make_double2(y2.x + t2.x, y2.y + t2.y);
@@ -162,109 +174,128 @@ __device__ __forceinline__ void apply_dense2(double2 (&a)[1 << SB], const FOp &o
     }
 }
 
-template <int SB, int B0, int B1>
-__device__ __forceinline__ void apply_swap2(double2 (&a)[1 << SB], const FOp &op, const uint32_t (&jr)[1 << SB])
+template <int B0, int B1>
+__device__ __forceinline__ void apply_swap2(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
+    const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
-    for (int r = 0; r < (1 << SB); ++r)
+    for (int r = 0; r < R; ++r)
     {
         if (r & ((1 << B0) | (1 << B1)))
             continue;
-        if ((jr[r] & op.lcmask) != op.lcval)
-            continue;
         const int i1 = r | (1 << B0), i2 = r | (1 << B1);
-        const double2 t = a[i1];
-        a[i1] = a[i2];
-        a[i2] = t;
+        const double2 x1 = a[i1], x2 = a[i2];
+        const bool ok = (jr[r] & cm) == cv;
+        a[i1] = ok ? x2 : x1;
+        a[i2] = ok ? x1 : x2;
     }
 }
 
-template <int SB>
-__device__ __forceinline__ void apply_diag(double2 (&a)[1 << SB], const FOp &op, const uint32_t (&jr)[1 << SB], uint64_t cbase)
+__device__ __forceinline__ void apply_phase(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
-    uint32_t s_chunk = 0;
-    for (int i = 0; i < op.nt; ++i)
-        if (op.loc[i] < 0)
-            s_chunk |= static_cast<uint32_t>((cbase >> op.phys[i]) & 1ull) << i;
+    const double2 e = op.m[0];
+    const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
-    for (int r = 0; r < (1 << SB); ++r)
+    for (int r = 0; r < R; ++r)
+    {
+        const double2 y = cmul(e, a[r]);
+        a[r] = ((jr[r] & cm) == cv) ? y : a[r];
+    }
+}
+
+__device__ __forceinline__ void apply_diag(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R], uint64_t cbase)
+{
+    // up to two targets: entries in registers, selected per amplitude
+    const double2 d0 = op.m[0], d1 = op.m[1], d2 = op.m[2], d3 = op.m[3];
+    const uint32_t cm = op.lcmask, cv = op.lcval;
+    const int l0 = op.loc[0], l1 = op.nt > 1 ? op.loc[1] : -1;
+    const uint32_t c0 = l0 < 0 ? static_cast<uint32_t>((cbase >> op.phys[0]) & 1ull) : 0u;
+    const uint32_t c1 = (op.nt > 1 && l1 < 0) ? static_cast<uint32_t>((cbase >> op.phys[1]) & 1ull) : 0u;
+    const uint32_t sh0 = l0 < 0 ? 0u : static_cast<uint32_t>(l0);
+    const uint32_t sh1 = l1 < 0 ? 0u : static_cast<uint32_t>(l1);
+    const uint32_t use0 = l0 < 0 ? 0u : 1u, use1 = l1 < 0 ? 0u : 1u;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
     {
         const uint32_t j = jr[r];
-        if ((j & op.lcmask) != op.lcval)
-            continue;
-        uint32_t s = s_chunk;
-        for (int i = 0; i < op.nt; ++i)
-            if (op.loc[i] >= 0)
-                s |= ((j >> op.loc[i]) & 1u) << i;
-        a[r] = cmul(op.m[s], a[r]);
+        const uint32_t s0 = use0 ? ((j >> sh0) & 1u) : c0;
+        const uint32_t s1 = use1 ? ((j >> sh1) & 1u) : c1;
+        const double2 lo = s0 ? d1 : d0;
+        const double2 hi = s0 ? d3 : d2;
+        const double2 d = s1 ? hi : lo;
+        const double2 y = cmul(d, a[r]);
+        a[r] = ((j & cm) == cv) ? y : a[r];
     }
 }
 
-template <int SB>
-__device__ __forceinline__ void dispatch_dense1(double2 (&a)[1 << SB], const FOp &op, const uint32_t (&jr)[1 << SB], bool swap)
+__device__ __forceinline__ void dispatch_dense1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     switch (op.b0)
     {
-    case 0: swap ? apply_swap1<SB, 0>(a, op, jr) : apply_dense1<SB, 0>(a, op, jr); break;
-    case 1: swap ? apply_swap1<SB, 1>(a, op, jr) : apply_dense1<SB, 1>(a, op, jr); break;
-    case 2: swap ? apply_swap1<SB, 2>(a, op, jr) : apply_dense1<SB, 2>(a, op, jr); break;
-    default:
-        if constexpr (SB > 3)
-            swap ? apply_swap1<SB, 3>(a, op, jr) : apply_dense1<SB, 3>(a, op, jr);
-        break;
+    case 0: apply_dense1<0>(a, op, jr); break;
+    case 1: apply_dense1<1>(a, op, jr); break;
+    case 2: apply_dense1<2>(a, op, jr); break;
+    default: apply_dense1<3>(a, op, jr); break;
     }
 }
 
-template <int SB, int B0>
-__device__ __forceinline__ void dispatch_dense2_b1(double2 (&a)[1 << SB], const FOp &op, const uint32_t (&jr)[1 << SB], bool swap)
-{
-    switch (op.b1)
-    {
-    case 0: if constexpr (B0 != 0) { swap ? apply_swap2<SB, B0, 0>(a, op, jr) : apply_dense2<SB, B0, 0>(a, op, jr); } break;
-    case 1: if constexpr (B0 != 1) { swap ? apply_swap2<SB, B0, 1>(a, op, jr) : apply_dense2<SB, B0, 1>(a, op, jr); } break;
-    case 2: if constexpr (B0 != 2) { swap ? apply_swap2<SB, B0, 2>(a, op, jr) : apply_dense2<SB, B0, 2>(a, op, jr); } break;
-    default:
-        if constexpr (SB > 3 && B0 != 3)
-            swap ? apply_swap2<SB, B0, 3>(a, op, jr) : apply_dense2<SB, B0, 3>(a, op, jr);
-        break;
-    }
-}
-
-template <int SB>
-__device__ __forceinline__ void dispatch_dense2(double2 (&a)[1 << SB], const FOp &op, const uint32_t (&jr)[1 << SB], bool swap)
+__device__ __forceinline__ void dispatch_swap1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     switch (op.b0)
     {
-    case 0: dispatch_dense2_b1<SB, 0>(a, op, jr, swap); break;
-    case 1: dispatch_dense2_b1<SB, 1>(a, op, jr, swap); break;
-    case 2: dispatch_dense2_b1<SB, 2>(a, op, jr, swap); break;
-    default:
-        if constexpr (SB > 3)
-            dispatch_dense2_b1<SB, 3>(a, op, jr, swap);
-        break;
+    case 0: apply_swap1<0>(a, op, jr); break;
+    case 1: apply_swap1<1>(a, op, jr); break;
+    case 2: apply_swap1<2>(a, op, jr); break;
+    default: apply_swap1<3>(a, op, jr); break;
     }
 }
 
-// One CTA per chunk at a time; blockDim.x == 2^(k - SB).
-template <int SB>
-__global__ void __launch_bounds__(256) fused_pass_kernel(const __grid_constant__ FPassParams p)
+// (b0, b1) with b0 < b1 encoded as b0 * 4 + b1
+__device__ __forceinline__ void dispatch_dense2(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+{
+    switch (op.b0 * 4 + op.b1)
+    {
+    case 1: apply_dense2<0, 1>(a, op, jr); break;
+    case 2: apply_dense2<0, 2>(a, op, jr); break;
+    case 3: apply_dense2<0, 3>(a, op, jr); break;
+    case 6: apply_dense2<1, 2>(a, op, jr); break;
+    case 7: apply_dense2<1, 3>(a, op, jr); break;
+    default: apply_dense2<2, 3>(a, op, jr); break;
+    }
+}
+
+__device__ __forceinline__ void dispatch_swap2(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+{
+    switch (op.b0 * 4 + op.b1)
+    {
+    case 1: apply_swap2<0, 1>(a, op, jr); break;
+    case 2: apply_swap2<0, 2>(a, op, jr); break;
+    case 3: apply_swap2<0, 3>(a, op, jr); break;
+    case 6: apply_swap2<1, 2>(a, op, jr); break;
+    case 7: apply_swap2<1, 3>(a, op, jr); break;
+    default: apply_swap2<2, 3>(a, op, jr); break;
+    }
+}
+
+// One CTA per chunk at a time; blockDim.x == 2^(k - kStageBits) <= 128, so
+// that three CTAs (12 warps, 3 x 64 KB of double-buffered chunks) share an SM.
+__global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constant__ FPassParams p)
 {
     extern __shared__ double2 smem[];
     const int k = p.k;
-    const int T = 1 << (k - SB);
+    const int T = 1 << (k - kStageBits);
     const int tid = threadIdx.x;
-    constexpr int R = 1 << SB;
-    double2 *buf[2] = {smem, smem + (1 << k)};
+    const int chunk_elems = 1 << k;
 
     // global offset of this thread's element tid + m*T, m < R
     uint64_t dep_tid = 0;
-    for (int i = 0; i < k - SB; ++i)
+    for (int i = 0; i < k - kStageBits; ++i)
         if ((tid >> i) & 1)
             dep_tid |= p.qbit[i];
-    uint64_t hb[SB];
+    uint64_t hb[kStageBits];
 #pragma unroll
-    for (int b = 0; b < SB; ++b)
-        hb[b] = p.qbit[k - SB + b];
+    for (int b = 0; b < kStageBits; ++b)
+        hb[b] = p.qbit[k - kStageBits + b];
 
     auto chunk_base = [&](uint64_t c) -> uint64_t {
         uint64_t g = c;
@@ -275,33 +306,34 @@ __global__ void __launch_bounds__(256) fused_pass_kernel(const __grid_constant__
         }
         return g;
     };
+    auto elem_offset = [&](int m) -> uint64_t {
+        uint64_t off = dep_tid;
+#pragma unroll
+        for (int b = 0; b < kStageBits; ++b)
+            if ((m >> b) & 1)
+                off |= hb[b];
+        return off;
+    };
     auto issue_load = [&](uint64_t c, double2 *dst) {
-        const uint64_t cb = chunk_base(c) | dep_tid;
+        const uint64_t cb = chunk_base(c);
 #pragma unroll
         for (int m = 0; m < R; ++m)
-        {
-            uint64_t off = cb;
-#pragma unroll
-            for (int b = 0; b < SB; ++b)
-                if ((m >> b) & 1)
-                    off |= hb[b];
-            const int e = tid + m * T;
-            cp_async16(dst + swz(e), p.state + off);
-        }
+            cp_async16(dst + swz(tid + m * T), p.state + (cb | elem_offset(m)));
         cp_async_commit();
     };
 
     uint64_t c = blockIdx.x;
     if (c >= p.chunks)
         return;
-    issue_load(c, buf[0]);
+    issue_load(c, smem);
     int cur = 0;
     for (; c < p.chunks; c += gridDim.x)
     {
+        double2 *sb = smem + cur * chunk_elems;
         const uint64_t next = c + gridDim.x;
         if (next < p.chunks)
         {
-            issue_load(next, buf[cur ^ 1]);
+            issue_load(next, smem + (cur ^ 1) * chunk_elems);
             cp_async_wait<1>();
         }
         else
@@ -309,16 +341,14 @@ __global__ void __launch_bounds__(256) fused_pass_kernel(const __grid_constant__
             cp_async_wait<0>();
         }
         __syncthreads();
-        double2 *sb = buf[cur];
         const uint64_t cbase = chunk_base(c);
 
         for (int st = 0; st < p.nstages; ++st)
         {
             const FStage &S = p.stages[st];
-            // group base: insert zeros at the stage bits (ascending)
             uint32_t j0 = static_cast<uint32_t>(tid);
 #pragma unroll
-            for (int b = 0; b < SB; ++b)
+            for (int b = 0; b < kStageBits; ++b)
             {
                 const uint32_t lo = j0 & ((1u << S.sbits[b]) - 1u);
                 j0 = lo | ((j0 ^ lo) << 1);
@@ -330,7 +360,7 @@ __global__ void __launch_bounds__(256) fused_pass_kernel(const __grid_constant__
             {
                 uint32_t j = j0;
 #pragma unroll
-                for (int b = 0; b < SB; ++b)
+                for (int b = 0; b < kStageBits; ++b)
                     if ((r >> b) & 1)
                         j |= 1u << S.sbits[b];
                 jr[r] = j;
@@ -343,11 +373,12 @@ __global__ void __launch_bounds__(256) fused_pass_kernel(const __grid_constant__
                     continue;
                 switch (op.kind)
                 {
-                case F_DENSE1: dispatch_dense1<SB>(a, op, jr, false); break;
-                case F_SWAP1: dispatch_dense1<SB>(a, op, jr, true); break;
-                case F_DENSE2: dispatch_dense2<SB>(a, op, jr, false); break;
-                case F_SWAP2: dispatch_dense2<SB>(a, op, jr, true); break;
-                default: apply_diag<SB>(a, op, jr, cbase); break;
+                case F_DENSE1: dispatch_dense1(a, op, jr); break;
+                case F_SWAP1: dispatch_swap1(a, op, jr); break;
+                case F_DENSE2: dispatch_dense2(a, op, jr); break;
+                case F_SWAP2: dispatch_swap2(a, op, jr); break;
+                case F_PHASE: apply_phase(a, op, jr); break;
+                default: apply_diag(a, op, jr, cbase); break;
                 }
             }
 #pragma unroll
@@ -356,19 +387,10 @@ __global__ void __launch_bounds__(256) fused_pass_kernel(const __grid_constant__
             __syncthreads();
         }
 
-        // write back
-        const uint64_t cb = cbase | dep_tid;
+        const uint64_t cb = cbase;
 #pragma unroll
         for (int m = 0; m < R; ++m)
-        {
-            uint64_t off = cb;
-#pragma unroll
-            for (int b = 0; b < SB; ++b)
-                if ((m >> b) & 1)
-                    off |= hb[b];
-            const int e = tid + m * T;
-            __stcs(p.state + off, sb[swz(e)]);
-        }
+            __stcs(p.state + (cb | elem_offset(m)), sb[swz(tid + m * T)]);
         __syncthreads();
         cur ^= 1;
     }
@@ -391,7 +413,7 @@ OpClass classify(const GateOp &op)
         t |= 1ull << op.tq[i];
     if (op.diag)
     {
-        c.fusable = op.nt <= 4;
+        c.fusable = op.na == 1 || op.nt <= 2;
         c.dense = 0;
         c.diag = t | op.cmask;
     }
@@ -404,37 +426,31 @@ OpClass classify(const GateOp &op)
     return c;
 }
 
-bool is_x(const GateOp &op)
+// X and Y commute when X's dense qubits avoid all of Y's qubits and X's
+// diagonal qubits avoid Y's dense qubits (ops that are diagonal on every
+// shared qubit commute).
+bool commute(const OpClass &x, const OpClass &y)
 {
-    // 2x2 [[0,1],[1,0]] on both sub-indices
-    if (op.nt != 1 || op.na != 2 || op.diag)
+    return (x.dense & (y.dense | y.diag)) == 0 && (x.diag & y.dense) == 0;
+}
+
+bool is_perm(const GateOp &op, int size)
+{
+    // the na x na block is [[0,1],[1,0]]
+    if (op.diag || op.na != 2 || size != 2)
         return false;
     const cplx *m = op.mat;
     return m[0].re == 0 && m[0].im == 0 && m[1].re == 1 && m[1].im == 0 &&
            m[2].re == 1 && m[2].im == 0 && m[3].re == 0 && m[3].im == 0;
 }
 
-bool is_swap(const GateOp &op)
-{
-    if (op.nt != 2 || op.na != 2 || op.diag || op.act[0] != 1 || op.act[1] != 2)
-        return false;
-    const cplx *m = op.mat;
-    return m[0].re == 0 && m[0].im == 0 && m[1].re == 1 && m[1].im == 0 &&
-           m[2].re == 1 && m[2].im == 0 && m[3].re == 0 && m[3].im == 0;
-}
+bool is_x(const GateOp &op) { return op.nt == 1 && is_perm(op, 2); }
+bool is_swap(const GateOp &op) { return op.nt == 2 && op.act[0] == 1 && op.act[1] == 2 && is_perm(op, 2); }
 
-// Full 2^nt x 2^nt matrix (dense) or 2^nt diagonal (diag) of a GateOp.
-void expand(const GateOp &op, double2 *out)
+// Full 2^nt x 2^nt matrix of a dense GateOp (row-major).
+void expand_dense(const GateOp &op, double2 *out)
 {
     const int d = 1 << op.nt;
-    if (op.diag)
-    {
-        for (int s = 0; s < d; ++s)
-            out[s] = make_double2(1.0, 0.0);
-        for (int a = 0; a < op.na; ++a)
-            out[op.act[a]] = make_double2(op.mat[a].re, op.mat[a].im);
-        return;
-    }
     for (int r = 0; r < d; ++r)
         for (int c = 0; c < d; ++c)
             out[r * d + c] = make_double2(r == c ? 1.0 : 0.0, 0.0);
@@ -445,7 +461,7 @@ void expand(const GateOp &op, double2 *out)
 
 struct PlannedPass
 {
-    std::vector<int> ops;   // indices into the queue, in execution order
+    std::vector<int> ops;   // indices into the queue, in queue order
     uint64_t local = 0;     // physical qubits of Q
 };
 
@@ -459,9 +475,7 @@ struct Segment
 // Greedy pass construction. Ops are taken in queue order; an op joins the
 // current pass when its dense targets fit in Q (k qubits) and it commutes
 // with every op left behind so far (an op is left behind when it does not
-// fit). Commutation test: X and Y commute when X's dense qubits avoid all of
-// Y's qubits and X's diagonal qubits avoid Y's dense qubits (ops that are
-// diagonal on every shared qubit commute).
+// fit).
 std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int low)
 {
     const size_t N = q.size();
@@ -470,7 +484,7 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
         cls[i] = classify(q[i]);
     std::vector<bool> done(N, false);
     std::vector<Segment> out;
-    const uint64_t low_mask = (low >= 64) ? ~0ull : ((1ull << low) - 1);
+    const uint64_t low_mask = (1ull << low) - 1;
     const uint64_t all = (n >= 64) ? ~0ull : ((1ull << n) - 1);
     size_t first = 0;
     while (true)
@@ -523,7 +537,6 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
                     break;
             }
         }
-        // fill Q up to k qubits with the lowest unused ones
         for (int b = 0; b < n && __builtin_popcountll(local) < k; ++b)
             local |= 1ull << b;
         s.pass.local = local;
@@ -532,189 +545,210 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
     return out;
 }
 
-// Split a pass into stages of SB bits and fill the kernel parameters.
-// Returns false when the pass does not fit the parameter block limits.
-template <int SB>
+// Order a pass's ops into stages of at most kStageBits local dense bits:
+// repeatedly open a stage and add every op whose dependencies are met and
+// whose dense targets fit, in queue order, until none fits.
+void schedule_stages(const std::vector<GateOp> &q, const PlannedPass &pp, const int *loc_of,
+                     std::vector<std::vector<int>> &stage_ops, std::vector<uint32_t> &stage_bits)
+{
+    const size_t m = pp.ops.size();
+    std::vector<OpClass> cls(m);
+    std::vector<uint32_t> need(m, 0);
+    for (size_t i = 0; i < m; ++i)
+    {
+        cls[i] = classify(q[pp.ops[i]]);
+        uint64_t d = cls[i].dense;
+        while (d)
+        {
+            const int b = __builtin_ctzll(d);
+            need[i] |= 1u << loc_of[b];
+            d &= d - 1;
+        }
+    }
+    std::vector<bool> done(m, false);
+    size_t left = m;
+    while (left > 0)
+    {
+        uint32_t bits = 0;
+        std::vector<int> ops;
+        bool progress = true;
+        while (progress)
+        {
+            progress = false;
+            for (size_t i = 0; i < m; ++i)
+            {
+                if (done[i])
+                    continue;
+                bool ready = true;
+                for (size_t j = 0; j < i && ready; ++j)
+                    if (!done[j] && !commute(cls[j], cls[i]))
+                        ready = false;
+                if (!ready)
+                    continue;
+                const uint32_t nb = bits | need[i];
+                if (__builtin_popcount(nb) > kStageBits)
+                    continue;
+                bits = nb;
+                ops.push_back((int)i);
+                done[i] = true;
+                --left;
+                progress = true;
+            }
+        }
+        stage_ops.push_back(std::move(ops));
+        stage_bits.push_back(bits);
+    }
+}
+
+// Fill the kernel parameters of a pass. Returns false when the pass does not
+// fit the parameter block limits.
 bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm)
 {
     std::memset(&prm, 0, sizeof(prm));
     prm.n = n;
     prm.k = k;
     prm.chunks = 1ull << (n - k);
-    int qphys[kMaxLocal];
-    int nl = 0;
     int loc_of[kMaxQubits];
     for (int b = 0; b < kMaxQubits; ++b)
         loc_of[b] = -1;
+    int nl = 0;
     for (int b = 0; b < n; ++b)
         if ((pp.local >> b) & 1)
         {
             loc_of[b] = nl;
-            qphys[nl++] = b;
+            prm.qmasks[nl] = (1ull << b) - 1;
+            prm.qbit[nl] = 1ull << b;
+            ++nl;
         }
     if (nl != k)
         throw std::runtime_error("internal: pass locality size mismatch");
-    for (int i = 0; i < k; ++i)
-    {
-        prm.qmasks[i] = (1ull << qphys[i]) - 1;
-        prm.qbit[i] = 1ull << qphys[i];
-    }
-    uint64_t all_local_mask = pp.local;
-    int nst = 0;
-    int cur_bits[4];
-    int ncur = 0;
-    auto close_stage = [&](int begin, int end) -> bool {
-        if (nst >= kFusedMaxStages)
-            return false;
-        // pad with the lowest local bits not in the stage
-        int bits[4];
-        int nb = ncur;
-        for (int i = 0; i < ncur; ++i)
-            bits[i] = cur_bits[i];
-        for (int l = 0; l < k && nb < SB; ++l)
-        {
-            bool used = false;
-            for (int i = 0; i < nb; ++i)
-                used = used || bits[i] == l;
-            if (!used)
-                bits[nb++] = l;
-        }
-        std::sort(bits, bits + SB);
-        FStage &S = prm.stages[nst++];
-        for (int i = 0; i < SB; ++i)
-            S.sbits[i] = static_cast<uint8_t>(bits[i]);
-        for (int i = SB; i < 4; ++i)
-            S.sbits[i] = 0;
-        S.op_begin = static_cast<uint16_t>(begin);
-        S.op_end = static_cast<uint16_t>(end);
-        return true;
-    };
-    int stage_begin = 0;
-    ncur = 0;
-    int nops = 0;
-    std::vector<int> stage_of(pp.ops.size());
-    // first assign stages (by local bit positions), then encode ops with
-    // their stage-relative bit positions
-    std::vector<std::vector<int>> stage_bits;
-    std::vector<std::pair<int, int>> ranges;
-    for (size_t oi = 0; oi < pp.ops.size(); ++oi)
-    {
-        const GateOp &op = q[pp.ops[oi]];
-        const OpClass c = classify(op);
-        int need[2];
-        int nneed = 0;
-        for (int b = 0; b < n; ++b)
-            if ((c.dense >> b) & 1)
-                need[nneed++] = loc_of[b];
-        int add = 0;
-        for (int i = 0; i < nneed; ++i)
-        {
-            bool have = false;
-            for (int j = 0; j < ncur; ++j)
-                have = have || cur_bits[j] == need[i];
-            add += have ? 0 : 1;
-        }
-        if (ncur + add > SB)
-        {
-            stage_bits.push_back(std::vector<int>(cur_bits, cur_bits + ncur));
-            ranges.push_back({stage_begin, (int)oi});
-            stage_begin = (int)oi;
-            ncur = 0;
-        }
-        for (int i = 0; i < nneed; ++i)
-        {
-            bool have = false;
-            for (int j = 0; j < ncur; ++j)
-                have = have || cur_bits[j] == need[i];
-            if (!have)
-                cur_bits[ncur++] = need[i];
-        }
-        stage_of[oi] = (int)ranges.size();
-    }
-    stage_bits.push_back(std::vector<int>(cur_bits, cur_bits + ncur));
-    ranges.push_back({stage_begin, (int)pp.ops.size()});
-    if (ranges.size() > (size_t)kFusedMaxStages || pp.ops.size() > (size_t)kFusedMaxOps)
+    if (pp.ops.size() > (size_t)kFusedMaxOps)
         return false;
-    for (size_t si = 0; si < ranges.size(); ++si)
+
+    std::vector<std::vector<int>> stage_ops;
+    std::vector<uint32_t> stage_bits;
+    schedule_stages(q, pp, loc_of, stage_ops, stage_bits);
+    if (stage_ops.size() > (size_t)kFusedMaxStages)
+        return false;
+    prm.nstages = (int)stage_ops.size();
+    int nops = 0;
+    for (size_t si = 0; si < stage_ops.size(); ++si)
     {
-        ncur = (int)stage_bits[si].size();
-        for (int i = 0; i < ncur; ++i)
-            cur_bits[i] = stage_bits[si][i];
-        if (!close_stage(ranges[si].first, ranges[si].second))
-            return false;
-    }
-    prm.nstages = nst;
-    (void)all_local_mask;
-    for (size_t oi = 0; oi < pp.ops.size(); ++oi)
-    {
-        const GateOp &op = q[pp.ops[oi]];
-        FOp &f = prm.ops[nops++];
-        const FStage &S = prm.stages[stage_of[oi]];
-        auto stage_pos = [&](int local_bit) -> int {
-            for (int i = 0; i < SB; ++i)
-                if (S.sbits[i] == local_bit)
-                    return i;
-            throw std::runtime_error("internal: target not in stage");
-        };
-        f.nt = static_cast<uint8_t>(op.nt);
-        for (int i = 0; i < 4; ++i)
-        {
-            f.loc[i] = -1;
-            f.phys[i] = 0;
-        }
-        for (int i = 0; i < op.nt; ++i)
-        {
-            f.phys[i] = static_cast<uint8_t>(op.tq[i]);
-            f.loc[i] = static_cast<int8_t>(loc_of[op.tq[i]]);
-        }
-        uint32_t lcm = 0, lcv = 0;
-        uint64_t gcm = 0, gcv = 0;
-        for (int b = 0; b < n; ++b)
-            if ((op.cmask >> b) & 1)
+        // stage bits: the needed ones, padded with the lowest other local bits
+        uint32_t bits = stage_bits[si];
+        for (int l = 0; l < k && __builtin_popcount(bits) < kStageBits; ++l)
+            bits |= 1u << l;
+        FStage &S = prm.stages[si];
+        int pos_in_stage[kMaxLocal];
+        int nb = 0;
+        for (int l = 0; l < k; ++l)
+            if ((bits >> l) & 1)
             {
-                const bool v = (op.cval >> b) & 1;
-                if (loc_of[b] >= 0)
+                pos_in_stage[l] = nb;
+                S.sbits[nb++] = static_cast<uint8_t>(l);
+            }
+        S.op_begin = static_cast<uint16_t>(nops);
+        for (int oi : stage_ops[si])
+        {
+            const GateOp &op = q[pp.ops[oi]];
+            FOp &f = prm.ops[nops++];
+            std::memset(&f, 0, sizeof(f));
+            f.nt = static_cast<uint8_t>(op.nt);
+            uint64_t cm = op.cmask, cv = op.cval;
+            if (op.diag && op.na == 1)
+            {
+                // one changed sub-index: a phase on the amplitudes whose
+                // control and target bits all match
+                f.kind = F_PHASE;
+                for (int i = 0; i < op.nt; ++i)
                 {
-                    lcm |= 1u << loc_of[b];
-                    if (v)
-                        lcv |= 1u << loc_of[b];
+                    cm |= 1ull << op.tq[i];
+                    if ((op.act[0] >> i) & 1)
+                        cv |= 1ull << op.tq[i];
+                }
+                f.m[0] = make_double2(op.mat[0].re, op.mat[0].im);
+            }
+            else if (op.diag)
+            {
+                f.kind = F_DIAG;
+                for (int s = 0; s < 4; ++s)
+                    f.m[s] = make_double2(1.0, 0.0);
+                for (int a = 0; a < op.na; ++a)
+                    f.m[op.act[a]] = make_double2(op.mat[a].re, op.mat[a].im);
+                for (int i = 0; i < op.nt; ++i)
+                {
+                    f.phys[i] = static_cast<uint8_t>(op.tq[i]);
+                    f.loc[i] = static_cast<int8_t>(loc_of[op.tq[i]]);
+                }
+                if (op.nt < 2)
+                {
+                    // second target absent: entries 2, 3 repeat 0, 1
+                    f.m[2] = f.m[0];
+                    f.m[3] = f.m[1];
+                    f.loc[1] = -1;
+                    f.phys[1] = 0;
+                }
+            }
+            else if (op.nt == 1)
+            {
+                f.kind = is_x(op) ? F_SWAP1 : F_DENSE1;
+                f.b0 = static_cast<uint8_t>(pos_in_stage[loc_of[op.tq[0]]]);
+                expand_dense(op, f.m);
+            }
+            else
+            {
+                f.kind = is_swap(op) ? F_SWAP2 : F_DENSE2;
+                int p0 = pos_in_stage[loc_of[op.tq[0]]];
+                int p1 = pos_in_stage[loc_of[op.tq[1]]];
+                double2 full[16];
+                expand_dense(op, full);
+                if (p0 < p1)
+                {
+                    for (int i = 0; i < 16; ++i)
+                        f.m[i] = full[i];
                 }
                 else
                 {
-                    gcm |= 1ull << b;
-                    if (v)
-                        gcv |= 1ull << b;
+                    // exchange the roles of the two targets: sub-index bits swap
+                    auto sw = [](int s) { return ((s & 1) << 1) | ((s >> 1) & 1); };
+                    for (int r = 0; r < 4; ++r)
+                        for (int c = 0; c < 4; ++c)
+                            f.m[r * 4 + c] = full[sw(r) * 4 + sw(c)];
+                    std::swap(p0, p1);
                 }
+                f.b0 = static_cast<uint8_t>(p0);
+                f.b1 = static_cast<uint8_t>(p1);
             }
-        f.lcmask = lcm;
-        f.lcval = lcv;
-        f.gcmask = gcm;
-        f.gcval = gcv;
-        if (op.diag)
-        {
-            f.kind = F_DIAG;
-            expand(op, f.m);
+            uint32_t lcm = 0, lcv = 0;
+            uint64_t gcm = 0, gcv = 0;
+            for (int b = 0; b < n; ++b)
+                if ((cm >> b) & 1)
+                {
+                    const bool v = (cv >> b) & 1;
+                    if (loc_of[b] >= 0)
+                    {
+                        lcm |= 1u << loc_of[b];
+                        if (v)
+                            lcv |= 1u << loc_of[b];
+                    }
+                    else
+                    {
+                        gcm |= 1ull << b;
+                        if (v)
+                            gcv |= 1ull << b;
+                    }
+                }
+            f.lcmask = lcm;
+            f.lcval = lcv;
+            f.gcmask = gcm;
+            f.gcval = gcv;
         }
-        else if (op.nt == 1)
-        {
-            f.kind = is_x(op) ? F_SWAP1 : F_DENSE1;
-            f.b0 = static_cast<uint8_t>(stage_pos(loc_of[op.tq[0]]));
-            expand(op, f.m);
-        }
-        else
-        {
-            f.kind = is_swap(op) ? F_SWAP2 : F_DENSE2;
-            f.b0 = static_cast<uint8_t>(stage_pos(loc_of[op.tq[0]]));
-            f.b1 = static_cast<uint8_t>(stage_pos(loc_of[op.tq[1]]));
-            expand(op, f.m);
-        }
+        S.op_end = static_cast<uint16_t>(nops);
     }
     return true;
 }
 
-constexpr int kStageBits = 3;
-
-int launch_fused_pass(double2 *state, int n, int k, const FPassParams &prm, cudaStream_t stream)
+int launch_fused_pass(double2 *state, int k, const FPassParams &prm, cudaStream_t stream)
 {
     const int threads = 1 << (k - kStageBits);
     const size_t smem = 2 * sizeof(double2) * (size_t(1) << k);
@@ -723,18 +757,22 @@ int launch_fused_pass(double2 *state, int n, int k, const FPassParams &prm, cuda
     QCSB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64 || !configured[dev])
     {
-        QCSB_CUDA(cudaFuncSetAttribute(fused_pass_kernel<kStageBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        QCSB_CUDA(cudaFuncSetAttribute(fused_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        2 * 16 * (1 << kMaxLocal)));
         if (dev >= 0 && dev < 64)
             configured[dev] = true;
     }
+    int per_sm = 0;
+    QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_pass_kernel, threads, smem));
+    int sms = 148;
+    QCSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     uint64_t grid = prm.chunks;
-    const uint64_t cap = 148ull * 4;
+    const uint64_t cap = (uint64_t)sms * (per_sm > 0 ? per_sm : 1);
     if (grid > cap)
         grid = cap;
-    FPassParams p = prm;
+    FPassParams &p = const_cast<FPassParams &>(prm);
     p.state = state;
-    fused_pass_kernel<kStageBits><<<static_cast<unsigned>(grid), threads, smem, stream>>>(p);
+    fused_pass_kernel<<<static_cast<unsigned>(grid), threads, smem, stream>>>(p);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
@@ -742,14 +780,14 @@ int launch_fused_pass(double2 *state, int n, int k, const FPassParams &prm, cuda
 int choose_local_bits(int n)
 {
     const char *e = std::getenv("QCS_FUSED_LOCAL_BITS");
-    int k = 11;
+    int k = kDefaultLocal;
     if (e && e[0])
         k = std::atoi(e);
     if (k > kMaxLocal)
         k = kMaxLocal;
-    if (k > kStageBits + 8)   // at most 256 threads per CTA
-        k = kStageBits + 8;
-    if (k < kStageBits + 5)
+    if (k > kStageBits + 7)   // at most 128 threads per CTA (launch bounds)
+        k = kStageBits + 7;
+    if (k < kStageBits + 5)   // at least one warp
         k = kStageBits + 5;
     if (k > n)
         k = n;
@@ -758,12 +796,15 @@ int choose_local_bits(int n)
 
 } // namespace
 
+int fused_min_qubits() { return kStageBits + 5; }
+
 FusedExecutor::FusedExecutor(cudaStream_t stream) : stream_(stream) {}
 FusedExecutor::~FusedExecutor() {}
 
 int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, int mode, qcs_b200_stats &stats,
                        KernelTimer &timer)
 {
+    (void)mode;
     auto plain = [&](const GateOp &op) {
         if (timer.enabled)
             timer.begin(stream_, KernelTimer::kPlain, 2.0 * sizeof(double2) * op.changed_amps(n));
@@ -773,10 +814,9 @@ int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, in
         stats.plain_gate_kernels += k;
         return k;
     };
-    (void)mode;
     int launches = 0;
     // Small registers: a pass would not fill a warp; run gate by gate.
-    if (n < kStageBits + 5)
+    if (n < fused_min_qubits())
     {
         for (const GateOp &op : ops)
             launches += plain(op);
@@ -793,11 +833,11 @@ int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, in
             launches += plain(ops[s.plain_op]);
             continue;
         }
-        if (build_params<kStageBits>(ops, s.pass, n, k, *prm))
+        if (build_params(ops, s.pass, n, k, *prm))
         {
             if (timer.enabled)
                 timer.begin(stream_, KernelTimer::kFused, 2.0 * sizeof(double2) * std::ldexp(1.0, n));
-            launches += launch_fused_pass(state, n, k, *prm, stream_);
+            launches += launch_fused_pass(state, k, *prm, stream_);
             if (timer.enabled)
                 timer.end(stream_);
             ++stats.fused_passes;

@@ -18,6 +18,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 namespace qcsb
 {
 namespace
@@ -72,7 +74,19 @@ struct PlainParams
     double2 m[DIAG ? NA : NA * NA];
 };
 
-template <int NA, bool DIAG, int U>
+template <bool STREAM>
+__device__ __forceinline__ double2 ld_amp(const double2 *p) { return STREAM ? __ldcs(p) : *p; }
+template <bool STREAM>
+__device__ __forceinline__ void st_amp(double2 *p, double2 v)
+{
+    if (STREAM)
+        __stcs(p, v);
+    else
+        *p = v;
+}
+
+// STREAM selects evict-first cache hints; U groups per thread per iteration.
+template <int NA, bool DIAG, int U, bool STREAM>
 __global__ void __launch_bounds__(kThreads) gate_plain_kernel(const __grid_constant__ PlainParams<NA, DIAG> p)
 {
     const uint64_t step = (uint64_t)gridDim.x * kThreads * U;
@@ -89,7 +103,7 @@ __global__ void __launch_bounds__(kThreads) gate_plain_kernel(const __grid_const
             {
 #pragma unroll
                 for (int a = 0; a < NA; ++a)
-                    v[u][a] = __ldcs(p.state + (base[u] | p.off[a]));
+                    v[u][a] = ld_amp<STREAM>(p.state + (base[u] | p.off[a]));
             }
         }
 #pragma unroll
@@ -102,7 +116,7 @@ __global__ void __launch_bounds__(kThreads) gate_plain_kernel(const __grid_const
             {
 #pragma unroll
                 for (int a = 0; a < NA; ++a)
-                    __stcs(p.state + (base[u] | p.off[a]), cmul(p.m[a], v[u][a]));
+                    st_amp<STREAM>(p.state + (base[u] | p.off[a]), cmul(p.m[a], v[u][a]));
             }
             else
             {
@@ -113,7 +127,7 @@ __global__ void __launch_bounds__(kThreads) gate_plain_kernel(const __grid_const
 #pragma unroll
                     for (int b = 0; b < NA; ++b)
                         acc = cfma(p.m[a * NA + b], v[u][b], acc);
-                    __stcs(p.state + (base[u] | p.off[a]), acc);
+                    st_amp<STREAM>(p.state + (base[u] | p.off[a]), acc);
                 }
             }
         }
@@ -136,15 +150,29 @@ int fill_masks(const GateOp &op, uint64_t *masks)
     return nops;
 }
 
-unsigned grid_for(uint64_t work_items, int per_block)
+unsigned grid_for(uint64_t work_items, int per_block, uint64_t cap = (uint64_t)kSMs * 16)
 {
     uint64_t blocks = (work_items + per_block - 1) / per_block;
-    const uint64_t cap = (uint64_t)kSMs * 16;
     if (blocks > cap)
         blocks = cap;
     if (blocks == 0)
         blocks = 1;
     return static_cast<unsigned>(blocks);
+}
+
+// Launch shape of the plain gate kernel (tuning knob QCS_PLAIN_VARIANT):
+//   0  grid-stride over 148 x 16 blocks, U groups per thread, evict-first hints
+//   1  one thread per group over the whole grid, default cache policy
+//   2  one thread per group over the whole grid, evict-first hints
+//   3  grid-stride, U groups per thread, default cache policy
+int plain_variant()
+{
+    static int v = [] {
+        const char *e = std::getenv("QCS_PLAIN_VARIANT");
+        const int x = (e && e[0]) ? std::atoi(e) : 1;
+        return (x >= 0 && x <= 3) ? x : 1;
+    }();
+    return v;
 }
 
 template <int NA, bool DIAG>
@@ -168,8 +196,22 @@ int launch_plain_na(double2 *state, int n, const GateOp &op, cudaStream_t stream
     const int nm = DIAG ? NA : NA * NA;
     for (int k = 0; k < nm; ++k)
         p.m[k] = make_double2(op.mat[k].re, op.mat[k].im);
-    const unsigned grid = grid_for(p.ngroups, kThreads * U);
-    gate_plain_kernel<NA, DIAG, U><<<grid, kThreads, 0, stream>>>(p);
+    const uint64_t one_shot_cap = 1ull << 31;
+    switch (plain_variant())
+    {
+    case 0:
+        gate_plain_kernel<NA, DIAG, U, true><<<grid_for(p.ngroups, kThreads * U), kThreads, 0, stream>>>(p);
+        break;
+    case 2:
+        gate_plain_kernel<NA, DIAG, 1, true><<<grid_for(p.ngroups, kThreads, one_shot_cap), kThreads, 0, stream>>>(p);
+        break;
+    case 3:
+        gate_plain_kernel<NA, DIAG, U, false><<<grid_for(p.ngroups, kThreads * U), kThreads, 0, stream>>>(p);
+        break;
+    default:
+        gate_plain_kernel<NA, DIAG, 1, false><<<grid_for(p.ngroups, kThreads, one_shot_cap), kThreads, 0, stream>>>(p);
+        break;
+    }
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }

@@ -136,6 +136,20 @@ def hea_circuit(n: int, depth: int, seed: int):
     return c
 
 
+def to_gatelist(circuit, num_qubits: int, num_clbits: int) -> str:
+    """Text form read by examples/gatelist.c (the bin/qcs plug-in)."""
+    lines = [f"{num_qubits} {num_clbits}"]
+    for op, params, targets, neg, pos in circuit:
+        if op == "measure":
+            lines.append(f"measure {targets[0]} {int(params[0])}")
+            continue
+        parts = [op, str(len(params))] + [repr(float(p)) for p in params]
+        for group in (targets, neg, pos):
+            parts += [str(len(group))] + [str(q) for q in group]
+        lines.append(" ".join(parts))
+    return "\n".join(lines) + "\n"
+
+
 def algorithmic_bytes(circuit, n: int, bytes_per_amp: int = 16) -> float:
     """Sum over gates of 2 * bytes_per_amp * (amplitudes the gate can change):
     dense and permuting 1-qubit gates change 2^(n-c) amplitudes, one-sided
