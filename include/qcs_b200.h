@@ -126,6 +126,36 @@ typedef struct qcs_b200_kernel_times
 int qcs_simulator_set_kernel_timing(qcs_simulator *sim, int enable);
 int qcs_simulator_get_kernel_times(qcs_simulator *sim, qcs_b200_kernel_times *times);
 
+/*
+ * Allocation-free squared-norm sums of a complex128 state vector held in the
+ * caller's device memory. This entry point has no counterpart in the
+ * reference library.
+ *
+ * It is for callers that cannot let a library call cudaMalloc: code inside a
+ * framework whose caching allocator owns the device memory, real-time loops
+ * that cannot take an allocation's latency or failure, and paths that must
+ * not synchronise the device. The caller passes the input and the output;
+ * the reduction's scratch is a fixed array inside libqcs.so (168 KiB, held by
+ * every GPU that loads the library until the process exits).
+ *
+ *   state_device  2^num_qubits complex128 amplitudes (re, im doubles),
+ *                 16-byte aligned, in device memory
+ *   num_qubits    1 .. 40; larger registers are rejected (the scratch is
+ *                 sized for 40 qubits)
+ *   sums_device   num_qubits + 1 doubles in device memory:
+ *                 sums[0] = sum |a_i|^2, sums[1 + q] = sum over i with bit q
+ *                 set of |a_i|^2, so <Z_q> = (sums[0] - 2 sums[1+q]) / sums[0]
+ *   stream        cudaStream_t to run on (NULL: the default stream); the call
+ *                 returns once the work is queued
+ *
+ * The first call on each device looks up the scratch array's device address
+ * with that device current; make that first call before any stream capture.
+ * All calls share the scratch array, so calls that overlap on the GPU race:
+ * serialise them. Returns 1 on success, 0 with a message to the exception
+ * callback on failure.
+ */
+int qcs_b200_zsums_noalloc(const double *state_device, int num_qubits, double *sums_device, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -92,6 +92,8 @@ void gate(qcs_simulator *sim, const char *name, std::initializer_list<double> pa
 
 } // namespace
 
+void qcsb::report_error(const char *message) { report(message); }
+
 // ------------------------------------------------------------ C++ API
 
 qcs_simulator *qcs_simulator_create_cxx()

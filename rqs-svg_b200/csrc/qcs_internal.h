@@ -21,6 +21,10 @@ constexpr int kMaxSub = 1 << kMaxTargets;
 
 std::string strformat(const char *fmt, ...);
 
+// Pass a message to the exception callback installed through
+// qcs_set_exception_callback (no-op when none is installed).
+void report_error(const char *message);
+
 #define QCSB_CUDA(call)                                                                 \
     do                                                                                  \
     {                                                                                   \

@@ -137,6 +137,7 @@ class Library:
             "qcs_simulator_sample": [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)],
             "qcs_simulator_get_stats": [_P, ctypes.POINTER(Stats)],
             "qcs_simulator_reset_stats": [_P],
+            "qcs_b200_zsums_noalloc": [_P, ctypes.c_int, _P, _P],
             "qcs_simulator_set_kernel_timing": [_P, ctypes.c_int],
             "qcs_simulator_get_kernel_times": [_P, ctypes.POINTER(KernelTimes)],
         }
