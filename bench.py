@@ -70,6 +70,7 @@ def parse_args():
     ap.add_argument("--depth", type=int, default=40)
     ap.add_argument("--no-plain-compare", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-peak", action="store_true")
     return ap.parse_args()
 
 
@@ -139,16 +140,25 @@ class Clocks:
                 "sm_max_mhz": max(maxsm) if maxsm else None, "reasons": reasons, "samples": len(mine)}
 
 
-def dist_init():
+def dist_init(backend="nccl"):
+    """One process per GPU (replicas): the group only carries the barrier
+    and the max-over-ranks of the timings. nccl on GPUs, gloo on CPU."""
     if WORLD == 1:
         return None
     import torch
     import torch.distributed as dist
     from datetime import timedelta
 
-    torch.cuda.set_device(0)
-    dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", 0))
+    if backend == "nccl":
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", 0))
+    else:
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
     return dist
+
+
+def _device(dist):
+    return "cuda" if dist is not None and dist.get_backend() == "nccl" else "cpu"
 
 
 def barrier(dist):
@@ -156,7 +166,8 @@ def barrier(dist):
         import torch
 
         dist.barrier()
-        torch.cuda.synchronize()
+        if _device(dist) == "cuda":
+            torch.cuda.synchronize()
 
 
 def max_over_ranks(dist, x):
@@ -164,9 +175,18 @@ def max_over_ranks(dist, x):
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_device(dist))
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_replica_times(dist, per_step_seconds, world):
+    """Whole-job numbers from each rank's per-step device times: the slowest
+    rank's total, seconds per step, and seconds per circuit for the job
+    (world replicas ran one circuit per step each)."""
+    total = max_over_ranks(dist, float(sum(per_step_seconds)))
+    steps = len(per_step_seconds)
+    return {"total_s": total, "sec_per_step": total / steps, "value": total / steps / world}
 
 
 def run_step(sim, circuit, with_outputs=True):
@@ -178,6 +198,51 @@ def run_step(sim, circuit, with_outputs=True):
         return z, norm, shots
     sim.synchronize()
     return None
+
+
+def fp64_flops(circuit, n):
+    """Useful FP64 flops of one step: a dense 2x2 complex gate costs 16
+    flops per amplitude of its control subspace (four complex multiply-adds
+    per pair), a one-sided phase 6 per changed amplitude; permutations (X,
+    CX, Toffoli, SWAP) cost none."""
+    one_sided = {"z", "s", "sdg", "t", "tdg", "u1", "p"}
+    perm = {"x", "swap", "id"}
+    total = 0.0
+    for op, params, targets, neg, pos in circuit:
+        c = len(neg) + len(pos)
+        if op in perm or op == "measure":
+            continue
+        if op in one_sided:
+            total += 6.0 * 2.0 ** (n - c - 1)
+        else:
+            total += 16.0 * 2.0 ** (n - c)
+    return total
+
+
+def dgemm_peak_tflops():
+    """FP64 peak of this GPU, measured as cuBLAS DGEMM (8192^3) throughput."""
+    try:
+        import torch
+
+        a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            torch.cuda.synchronize()
+            t = s.elapsed_time(e) * 1e-3
+            best = t if best is None else min(best, t)
+        del a, b
+        torch.cuda.empty_cache()
+        return 2 * 8192 ** 3 / best / 1e12
+    except Exception:
+        return None
 
 
 def cpu_baseline(n_full, depth):
@@ -232,11 +297,17 @@ def main():
         per_step.append(sim.elapsed(e0, e1))
     barrier(dist)
     ktimes = sim.kernel_times()
+    pass_feats, pass_ms = sim.pass_records()
     sim.set_kernel_timing(False)
     stats = sim.stats()
     clk = clocks.stop(0)
-    total = max_over_ranks(dist, sum(per_step))
-    sec_per_step = total / args.steps
+    agg = aggregate_replica_times(dist, per_step, WORLD)
+    sec_per_step = agg["sec_per_step"]
+    passes = None
+    if len(pass_ms):
+        passes = {"per_step": len(pass_ms) / args.steps, "median_ms": float(np.median(pass_ms)),
+                  "max_ms": float(np.max(pass_ms)), "gates_per_pass": float(np.mean(pass_feats[:, 2])),
+                  "hbm_floor_ms": 2 * 16 * (1 << n) / (hbm_peak()[0] * 1e9) * 1e3}
 
     # end to end through the C ABI: host wall clock, host inputs (gate
     # parameters, sampler uniforms) in, results (<Z>, shots) out
@@ -288,10 +359,17 @@ def main():
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(n, depth)
+    fp64 = None
+    if RANK == 0 and WORLD == 1 and not args.no_fp64_peak:
+        flops = fp64_flops(circuit, n)
+        peak_tf = dgemm_peak_tflops()
+        fp64 = {"achieved_tflops": flops / sec_per_step / 1e12, "useful_flops_per_step": flops,
+                "peak_tflops": peak_tf, "peak_kind": "measured: cuBLAS DGEMM 8192^3 (torch.matmul float64)",
+                "frac": (flops / sec_per_step / 1e12) / peak_tf if peak_tf else None}
 
     line = {
         "metric": f"circuit wall s at {n}q (plain-method circuit at scale)",
-        "value": sec_per_step / WORLD,
+        "value": agg["value"],
         "unit": "s",
         "n_gpus": WORLD,
         "steps": args.steps,
@@ -310,6 +388,9 @@ def main():
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(stats["kernel_launches"] / args.steps),
         "roofline": roofline,
+        "fp64": fp64,
+        "passes": passes,
+        "step_s": per_step,
         "cpu_baseline": cpu,
         "plain": plain,
         "clocks": clk,

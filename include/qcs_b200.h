@@ -127,6 +127,59 @@ int qcs_simulator_set_kernel_timing(qcs_simulator *sim, int enable);
 int qcs_simulator_get_kernel_times(qcs_simulator *sim, qcs_b200_kernel_times *times);
 
 /*
+ * Planner knobs for the fused modes: the most gates one pass may carry
+ * (default 64) and the number of local qubits of a pass (default 11, range
+ * 9..11). 0 keeps a default. Used to tune, and to record diverse pass
+ * timings for the cost model.
+ */
+int qcs_simulator_set_planner_options(qcs_simulator *sim, int max_gates_per_pass, int local_qubits);
+
+/*
+ * Pass timings recorded while kernel timing is enabled: for each fused pass
+ * its features (4 floats: local qubits, highest local physical qubit, gate
+ * count, bytes per amplitude) and its device time in milliseconds. Reading
+ * synchronizes, returns up to capacity records in *count and clears them.
+ */
+int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *milliseconds, uint32_t capacity,
+                                   uint32_t *count);
+
+/*
+ * Learned cost model of fused passes: an MLP 4 -> 64 -> 64 -> 1 (FP32, ReLU)
+ * whose training and inference run as this library's own CUDA kernels.
+ * Inputs are the pass features above; the target is log(device time per
+ * amplitude in nanoseconds) = log(ms * 1e6 / 2^n). Attach a trained model to
+ * a simulator and select QCS_FUSION_LEARNED to let it plan passes; measured
+ * device time then decides, per gate queue, between its plan and the greedy
+ * one.
+ */
+typedef struct qcs_b200_cost_model qcs_b200_cost_model;
+#define QCS_COST_MODEL_PARAMS 4545
+#define QCS_COST_MODEL_SCALING 10
+
+int qcs_b200_cost_model_create(qcs_b200_cost_model **model, uint32_t seed);
+int qcs_b200_cost_model_destroy(qcs_b200_cost_model *model);
+/* Adam on mini-batches; final_loss (may be NULL) gets the mean squared error
+   on the standardised training set. */
+int qcs_b200_cost_model_train(qcs_b200_cost_model *model, const float *features, const float *targets,
+                              uint32_t count, uint32_t epochs, uint32_t batch, float learning_rate, float *final_loss);
+int qcs_b200_cost_model_predict(qcs_b200_cost_model *model, const float *features, uint32_t count, float *predictions);
+/* Gradient of the mean squared error w.r.t. the parameters (layout W1[64x4],
+   b1[64], W2[64x64], b2[64], W3[64], b3) for inputs and targets that are
+   already standardised; loss (may be NULL) gets the loss. */
+int qcs_b200_cost_model_gradients(qcs_b200_cost_model *model, const float *inputs, const float *targets,
+                                  uint32_t count, float *gradients, float *loss);
+/* params: QCS_COST_MODEL_PARAMS floats; scaling: input means[4], input
+   deviations[4], target mean, target deviation. */
+int qcs_b200_cost_model_get_params(qcs_b200_cost_model *model, float *params, float *scaling);
+int qcs_b200_cost_model_set_params(qcs_b200_cost_model *model, const float *params, const float *scaling);
+/* The simulator keeps a pointer (the caller keeps the model alive). */
+int qcs_simulator_set_cost_model(qcs_simulator *sim, qcs_b200_cost_model *model);
+/* For the last flush in learned mode: which planner ran (1 learned, 0
+   greedy) and the device times the judge holds for that gate queue (ms, -1
+   when not measured yet). */
+int qcs_simulator_get_planner_judge(qcs_simulator *sim, int *learned_plan, double *greedy_ms, double *learned_ms);
+
+/*
  * Allocation-free squared-norm sums of a complex128 state vector held in the
  * caller's device memory. This entry point has no counterpart in the
  * reference library.

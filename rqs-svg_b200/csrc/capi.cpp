@@ -7,8 +7,10 @@
 
 #include "qcs.h"
 #include "qcs_b200.h"
+#include "cost_model.h"
 #include "simulator.h"
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -543,5 +545,159 @@ extern "C" int qcs_simulator_get_kernel_times(qcs_simulator *sim, qcs_b200_kerne
         auto &c = core(sim);
         c.flush();
         c.timer.collect(*times);
+    });
+}
+
+// ------------------------------------------------------------ planner and cost model
+
+struct qcs_b200_cost_model
+{
+    qcsb::CostModel *m = nullptr;
+};
+
+namespace
+{
+qcsb::CostModel &model_of(qcs_b200_cost_model *model)
+{
+    if (model == nullptr || model->m == nullptr)
+        throw std::runtime_error("cost model handle must not be NULL");
+    return *model->m;
+}
+} // namespace
+
+extern "C" int qcs_simulator_set_planner_options(qcs_simulator *sim, int max_gates_per_pass, int local_qubits)
+{
+    return guarded([&] { core(sim).set_planner_options(max_gates_per_pass, local_qubits); });
+}
+
+extern "C" int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *milliseconds,
+                                              uint32_t capacity, uint32_t *count)
+{
+    return guarded([&] {
+        if (count == nullptr || (capacity > 0 && (features == nullptr || milliseconds == nullptr)))
+            throw std::runtime_error("get_pass_records: output pointers must not be NULL");
+        auto &c = core(sim);
+        c.flush();
+        std::vector<qcsb::PassFeatures> f;
+        std::vector<float> ms;
+        c.timer.take_pass_log(f, ms);
+        const uint32_t n = static_cast<uint32_t>(std::min<size_t>(capacity, f.size()));
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            for (int j = 0; j < 4; ++j)
+                features[4 * i + j] = f[i].f[j];
+            milliseconds[i] = ms[i];
+        }
+        *count = n;
+    });
+}
+
+extern "C" int qcs_b200_cost_model_create(qcs_b200_cost_model **model, uint32_t seed)
+{
+    return guarded([&] {
+        if (model == nullptr)
+            throw std::runtime_error("result pointer must not be NULL");
+        auto *h = new qcs_b200_cost_model();
+        try
+        {
+            h->m = new qcsb::CostModel(seed);
+        }
+        catch (...)
+        {
+            delete h;
+            throw;
+        }
+        *model = h;
+    });
+}
+
+extern "C" int qcs_b200_cost_model_destroy(qcs_b200_cost_model *model)
+{
+    return guarded([&] {
+        if (model == nullptr)
+            return;
+        delete model->m;
+        delete model;
+    });
+}
+
+extern "C" int qcs_b200_cost_model_train(qcs_b200_cost_model *model, const float *features, const float *targets,
+                                         uint32_t count, uint32_t epochs, uint32_t batch, float learning_rate,
+                                         float *final_loss)
+{
+    return guarded([&] {
+        if (features == nullptr || targets == nullptr)
+            throw std::runtime_error("cost model train: data pointers must not be NULL");
+        const float loss = model_of(model).train(features, targets, (int)count, (int)epochs, (int)batch,
+                                                 learning_rate, 12345u);
+        if (final_loss)
+            *final_loss = loss;
+    });
+}
+
+extern "C" int qcs_b200_cost_model_predict(qcs_b200_cost_model *model, const float *features, uint32_t count,
+                                           float *predictions)
+{
+    return guarded([&] {
+        if (features == nullptr || predictions == nullptr)
+            throw std::runtime_error("cost model predict: pointers must not be NULL");
+        model_of(model).predict(features, (int)count, predictions);
+    });
+}
+
+extern "C" int qcs_b200_cost_model_gradients(qcs_b200_cost_model *model, const float *inputs, const float *targets,
+                                             uint32_t count, float *gradients, float *loss)
+{
+    return guarded([&] {
+        if (inputs == nullptr || targets == nullptr || gradients == nullptr || count == 0)
+            throw std::runtime_error("cost model gradients: pointers must not be NULL and count positive");
+        const float l = model_of(model).gradients(inputs, targets, (int)count, gradients);
+        if (loss)
+            *loss = l;
+    });
+}
+
+extern "C" int qcs_b200_cost_model_get_params(qcs_b200_cost_model *model, float *params, float *scaling)
+{
+    return guarded([&] {
+        auto &m = model_of(model);
+        if (params)
+            m.get_params(params);
+        if (scaling)
+            m.get_scaling(scaling);
+    });
+}
+
+extern "C" int qcs_b200_cost_model_set_params(qcs_b200_cost_model *model, const float *params, const float *scaling)
+{
+    return guarded([&] {
+        auto &m = model_of(model);
+        if (params)
+            m.set_params(params);
+        if (scaling)
+            m.set_scaling(scaling);
+    });
+}
+
+extern "C" int qcs_simulator_set_cost_model(qcs_simulator *sim, qcs_b200_cost_model *model)
+{
+    return guarded([&] { core(sim).set_cost_model(model ? model->m : nullptr); });
+}
+
+extern "C" int qcs_simulator_get_planner_judge(qcs_simulator *sim, int *learned_plan, double *greedy_ms,
+                                               double *learned_ms)
+{
+    return guarded([&] {
+        auto &c = core(sim);
+        c.flush();
+        auto *f = c.fused_executor();
+        if (f == nullptr)
+            throw std::runtime_error("get_planner_judge: allocate_memory must be called first");
+        if (learned_plan)
+            *learned_plan = f->last_plan_learned;
+        if (greedy_ms)
+            *greedy_ms = f->last_greedy_ms;
+        if (learned_ms)
+            *learned_ms = f->last_learned_ms;
     });
 }

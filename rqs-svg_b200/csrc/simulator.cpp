@@ -123,6 +123,9 @@ void Simulator::allocate_memory()
     n_ = n;
     perm_p2l_.assign(n, 0);
     perm_l2p_.assign(n, 0);
+    ref_l2p_.assign(n, 0);
+    for (int q = 0; q < n; ++q)
+        perm_p2l_[q] = perm_l2p_[q] = ref_l2p_[q] = q;
     reinitialize_mapping();
     QCSB_CUDA(cudaMalloc(&red_partials_, sizeof(double2) * kReduceBlocks));
     QCSB_CUDA(cudaMalloc(&red_result_, sizeof(double2)));
@@ -131,7 +134,30 @@ void Simulator::allocate_memory()
     host_pinned_bytes_ = 1 << 16;
     QCSB_CUDA(cudaMallocHost(&host_pinned_, host_pinned_bytes_));
     fused_ = new FusedExecutor(stream_);
+    fused_->set_options(opt_max_ops_, opt_local_bits_);
+    fused_->set_cost_model(model_);
     set_zero_state();
+}
+
+void Simulator::set_planner_options(int max_ops, int local_bits)
+{
+    if (max_ops < 0 || local_bits < 0)
+        throw std::runtime_error("planner options must be non-negative (0 keeps the default)");
+    if (allocated())
+        flush();
+    opt_max_ops_ = max_ops;
+    opt_local_bits_ = local_bits;
+    if (fused_)
+        fused_->set_options(max_ops, local_bits);
+}
+
+void Simulator::set_cost_model(CostModel *model)
+{
+    if (allocated())
+        flush();
+    model_ = model;
+    if (fused_)
+        fused_->set_cost_model(model);
 }
 
 void Simulator::dispose()
@@ -193,21 +219,38 @@ void Simulator::set_mapping(const std::vector<int> &perm_p2l)
 
 void Simulator::reinitialize_mapping()
 {
-    // reference reinitialize_mapping, src/qcs.cu:1860-1885
+    // reference reinitialize_mapping, src/qcs.cu:1860-1885: the mapping
+    // becomes the initial one (identity when none was set) and the data stay
+    // where they are. Relabelled swaps (apply_gate) moved logical qubits to
+    // other physical bits here but not in the reference; logical qubit q sat
+    // at the reference's physical bit ref(q) and sits at ours(q), so the
+    // reference's bit v is our bit ours(ref^-1(v)). After the reset the
+    // reference holds q at init(q), i.e. at our bit ours(ref^-1(init(q))).
     if (n_ == 0)
         return;
+    std::vector<int> init_l2p(n_);
     if (initial_perm_p2l_.empty())
     {
         for (int q = 0; q < n_; ++q)
-            perm_p2l_[q] = perm_l2p_[q] = q;
-        return;
+            init_l2p[q] = q;
     }
-    if ((int)initial_perm_p2l_.size() != n_)
-        throw std::runtime_error(strformat("mapping size %d does not match num_qubits %d", (int)initial_perm_p2l_.size(), n_));
-    flush();
-    perm_p2l_ = initial_perm_p2l_;
-    for (int p = 0; p < n_; ++p)
-        perm_l2p_[perm_p2l_[p]] = p;
+    else
+    {
+        if ((int)initial_perm_p2l_.size() != n_)
+            throw std::runtime_error(strformat("mapping size %d does not match num_qubits %d", (int)initial_perm_p2l_.size(), n_));
+        for (int p = 0; p < n_; ++p)
+            init_l2p[initial_perm_p2l_[p]] = p;
+    }
+    std::vector<int> ref_p2l(n_);
+    for (int q = 0; q < n_; ++q)
+        ref_p2l[ref_l2p_[q]] = q;
+    std::vector<int> ours(n_);
+    for (int q = 0; q < n_; ++q)
+        ours[q] = perm_l2p_[ref_p2l[init_l2p[q]]];
+    perm_l2p_ = ours;
+    for (int q = 0; q < n_; ++q)
+        perm_p2l_[perm_l2p_[q]] = q;
+    ref_l2p_ = init_l2p;
 }
 
 bool Simulator::identity_mapping() const
@@ -284,6 +327,19 @@ void Simulator::apply_gate(const char *name, const double *params, int nparams,
 
     if (op.na == 0)
         return;   // identity on every amplitude
+    if (fusion_mode_ != QCS_FUSION_PLAIN && arity == 2 && negctrls.empty() && ctrls.empty() &&
+        std::strcmp(name, "swap") == 0)
+    {
+        // An uncontrolled SWAP exchanges which physical bits hold the two
+        // logical qubits: exact, and no data moves. Implicit controls from
+        // measured qubits do not matter here, since the branch they exclude
+        // is all zeros and stays zeros under any qubit permutation.
+        std::swap(perm_l2p_[targets[0]], perm_l2p_[targets[1]]);
+        perm_p2l_[perm_l2p_[targets[0]]] = targets[0];
+        perm_p2l_[perm_l2p_[targets[1]]] = targets[1];
+        ++stats.gates_applied;
+        return;
+    }
     ++stats.gates_applied;
     stats.algorithmic_bytes += 2.0 * sizeof(double2) * op.changed_amps(n_);
     if (fusion_mode_ == QCS_FUSION_PLAIN)
@@ -364,11 +420,22 @@ void Simulator::clear_measurement_state()
     measured1_.clear();
 }
 
+// |0..0> and the flat state are unchanged by any qubit permutation, and a
+// loaded state is written through whatever map is current, so before those
+// the layout left by relabelled swaps can return to the reference's map.
+void Simulator::restore_reference_layout()
+{
+    perm_l2p_ = ref_l2p_;
+    for (int q = 0; q < n_; ++q)
+        perm_p2l_[perm_l2p_[q]] = q;
+}
+
 void Simulator::set_zero_state()
 {
     require_allocated("set_zero_state");
     discard_pending();
     clear_measurement_state();
+    restore_reference_layout();
     stats.kernel_launches += launch_init_zero(state_, n_, stream_);
 }
 
@@ -377,6 +444,7 @@ void Simulator::set_flat_state()
     require_allocated("set_flat_state");
     discard_pending();
     clear_measurement_state();
+    restore_reference_layout();
     stats.kernel_launches += launch_init_flat(state_, n_, stream_);
 }
 
@@ -521,6 +589,7 @@ void Simulator::set_statevector(const double *in, uint64_t count)
                                            (unsigned long long)count, (unsigned long long)(1ull << n_)));
     discard_pending();
     clear_measurement_state();
+    restore_reference_layout();
     logical_transfer(const_cast<double *>(in), count, false);
 }
 
@@ -606,11 +675,23 @@ cudaEvent_t KernelTimer::take()
     return e;
 }
 
-void KernelTimer::begin(cudaStream_t stream, int cls, double bytes)
+void KernelTimer::begin(cudaStream_t stream, int cls, double bytes, const PassFeatures *features)
 {
-    Rec r{cls, bytes, take(), take()};
+    Rec r{cls, bytes, take(), take(), PassFeatures{{0.0f, 0.0f, 0.0f, 0.0f}}};
+    if (features)
+        r.feat = *features;
     QCSB_CUDA(cudaEventRecord(r.a, stream));
     recs_.push_back(r);
+}
+
+void KernelTimer::take_pass_log(std::vector<PassFeatures> &features, std::vector<float> &ms)
+{
+    qcs_b200_kernel_times unused;
+    collect(unused);
+    features.swap(log_feat_);
+    ms.swap(log_ms_);
+    log_feat_.clear();
+    log_ms_.clear();
 }
 
 void KernelTimer::end(cudaStream_t stream) { QCSB_CUDA(cudaEventRecord(recs_.back().b, stream)); }
@@ -628,6 +709,8 @@ void KernelTimer::collect(qcs_b200_kernel_times &out)
             ++out.fused_launches;
             out.fused_ms += ms;
             out.fused_bytes += r.bytes;
+            log_feat_.push_back(r.feat);
+            log_ms_.push_back(ms);
         }
         else
         {

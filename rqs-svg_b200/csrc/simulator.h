@@ -11,8 +11,19 @@ namespace qcsb
 {
 
 class FusedExecutor;
+class CostModel;
+
+// Features of one fused pass, the cost model's inputs: local qubits k,
+// highest local physical qubit (log2 of the largest local stride), gate
+// count, bytes per amplitude.
+struct PassFeatures
+{
+    float f[4];
+};
 
 // Optional per-launch timing with CUDA events on the launching stream.
+// Fused passes also keep their features, so that their timings can train the
+// cost model.
 class KernelTimer
 {
   public:
@@ -23,9 +34,11 @@ class KernelTimer
     };
     ~KernelTimer();
     bool enabled = false;
-    void begin(cudaStream_t stream, int cls, double bytes);
+    void begin(cudaStream_t stream, int cls, double bytes, const PassFeatures *features = nullptr);
     void end(cudaStream_t stream);
     void collect(qcs_b200_kernel_times &out);   // synchronizes on the events
+    // Fused-pass samples gathered by collect() (and collected now), cleared on read.
+    void take_pass_log(std::vector<PassFeatures> &features, std::vector<float> &ms);
     void clear();
 
   private:
@@ -34,10 +47,13 @@ class KernelTimer
         int cls;
         double bytes;
         cudaEvent_t a, b;
+        PassFeatures feat;
     };
     cudaEvent_t take();
     std::vector<Rec> recs_;
     std::vector<cudaEvent_t> pool_;
+    std::vector<PassFeatures> log_feat_;
+    std::vector<float> log_ms_;
 };
 
 class Simulator
@@ -93,6 +109,10 @@ class Simulator
     void flush();
     void synchronize();
 
+    void set_planner_options(int max_ops, int local_bits);
+    void set_cost_model(CostModel *model);
+    FusedExecutor *fused_executor() { return fused_; }
+
     qcs_b200_stats stats{};
     KernelTimer timer;
 
@@ -103,6 +123,7 @@ class Simulator
     void ensure_staging();
     void logical_transfer(double *host, uint64_t count, bool to_host);
     void discard_pending() { pending_.clear(); }
+    void restore_reference_layout();
 
     bool disposed_ = false;
     int device_ = 0;
@@ -111,6 +132,9 @@ class Simulator
     double2 *state_ = nullptr;
 
     std::vector<int> perm_p2l_, perm_l2p_, initial_perm_p2l_;
+    // logical -> physical map the reference would hold (it differs from ours
+    // only through relabelled swaps)
+    std::vector<int> ref_l2p_;
     std::vector<int> measured0_, measured1_;   // logical qubits measured as 0 / 1
 
     uint32_t seed_ = 0;
@@ -119,6 +143,8 @@ class Simulator
     int fusion_mode_ = QCS_FUSION_GREEDY;
     std::vector<GateOp> pending_;
     FusedExecutor *fused_ = nullptr;
+    CostModel *model_ = nullptr;
+    int opt_max_ops_ = 0, opt_local_bits_ = 0;
 
     // scratch: reduction partials and results, pinned host mirror,
     // chunk staging for logical-order transfers, sampler tree
@@ -142,11 +168,38 @@ class FusedExecutor
     ~FusedExecutor();
     int run(double2 *state, int n, const std::vector<GateOp> &ops, int mode, qcs_b200_stats &stats, KernelTimer &timer);
 
+    // Planner knobs: 0 keeps the default (64 gates per pass, 11 local qubits).
+    void set_options(int max_ops, int local_bits)
+    {
+        max_ops_ = max_ops;
+        local_bits_ = local_bits;
+    }
+    void set_cost_model(CostModel *model) { model_ = model; }
+
+    // Which planner ran the last flush in learned mode (1 = learned,
+    // 0 = greedy) and the device times the judge holds for that queue.
+    int last_plan_learned = 0;
+    double last_greedy_ms = -1.0, last_learned_ms = -1.0;
+
   private:
+    struct JudgeEntry
+    {
+        double greedy_ms = -1.0;
+        double learned_ms = -1.0;
+    };
+    void settle_judge();
+
     cudaStream_t stream_;
-    void *prog_dev_ = nullptr;
-    size_t prog_bytes_ = 0;
-    void *prog_host_ = nullptr;
+    int max_ops_ = 0;
+    int local_bits_ = 0;
+    CostModel *model_ = nullptr;
+    // "measured device time is the judge": per queue signature, the device
+    // time of a flush under each planner; once both are known the faster one
+    // is used for that queue from then on.
+    std::vector<std::pair<uint64_t, JudgeEntry>> judge_;
+    cudaEvent_t judge_a_ = nullptr, judge_b_ = nullptr;
+    uint64_t pending_sig_ = 0;
+    int pending_learned_ = -1;
 };
 
 } // namespace qcsb

@@ -26,6 +26,10 @@ bit_t = ctypes.c_uint8
 event_num_t = ctypes.c_int16
 _P = ctypes.c_void_p
 _BN = ctypes.POINTER(bit_num_t)
+_FP = ctypes.POINTER(ctypes.c_float)
+
+COST_MODEL_PARAMS = 4545
+COST_MODEL_SCALING = 10
 
 # name -> (number of double parameters, number of targets)
 GATES = {
@@ -137,9 +141,22 @@ class Library:
             "qcs_simulator_sample": [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)],
             "qcs_simulator_get_stats": [_P, ctypes.POINTER(Stats)],
             "qcs_simulator_reset_stats": [_P],
-            "qcs_b200_zsums_noalloc": [_P, ctypes.c_int, _P, _P],
             "qcs_simulator_set_kernel_timing": [_P, ctypes.c_int],
             "qcs_simulator_get_kernel_times": [_P, ctypes.POINTER(KernelTimes)],
+            "qcs_b200_zsums_noalloc": [_P, ctypes.c_int, _P, _P],
+            "qcs_simulator_set_planner_options": [_P, ctypes.c_int, ctypes.c_int],
+            "qcs_simulator_get_pass_records": [_P, _FP, _FP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)],
+            "qcs_b200_cost_model_create": [ctypes.POINTER(_P), ctypes.c_uint32],
+            "qcs_b200_cost_model_destroy": [_P],
+            "qcs_b200_cost_model_train": [_P, _FP, _FP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                          ctypes.c_float, _FP],
+            "qcs_b200_cost_model_predict": [_P, _FP, ctypes.c_uint32, _FP],
+            "qcs_b200_cost_model_gradients": [_P, _FP, _FP, ctypes.c_uint32, _FP, _FP],
+            "qcs_b200_cost_model_get_params": [_P, _FP, _FP],
+            "qcs_b200_cost_model_set_params": [_P, _FP, _FP],
+            "qcs_simulator_set_cost_model": [_P, _P],
+            "qcs_simulator_get_planner_judge": [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                                ctypes.POINTER(ctypes.c_double)],
         }
         for name, (np_, nt) in GATES.items():
             if name == "global_phase":
@@ -257,6 +274,10 @@ class Simulator:
     def reinitialize_mapping(self):
         self.lib.call("qcs_simulator_reinitialize_mapping", self.h)
 
+    def set_mapping(self, mapping):
+        arr, cnt = _arr(mapping)
+        self.lib.call("qcs_simulator_set_mapping", self.h, arr, cnt)
+
     # -- output
     def save_statevector(self, path: str):
         self.lib.call("qcs_simulator_save_statevector", self.h, str(path).encode())
@@ -331,6 +352,77 @@ class Simulator:
         t = KernelTimes()
         self.lib.call("qcs_simulator_get_kernel_times", self.h, ctypes.byref(t))
         return {f: getattr(t, f) for f, _ in KernelTimes._fields_}
+
+    def set_planner_options(self, max_gates_per_pass: int = 0, local_qubits: int = 0):
+        self.lib.call("qcs_simulator_set_planner_options", self.h, max_gates_per_pass, local_qubits)
+
+    def pass_records(self, capacity: int = 1 << 20):
+        feats = np.zeros((capacity, 4), dtype=np.float32)
+        ms = np.zeros(capacity, dtype=np.float32)
+        count = ctypes.c_uint32()
+        self.lib.call("qcs_simulator_get_pass_records", self.h, _fptr(feats), _fptr(ms), capacity, ctypes.byref(count))
+        return feats[: count.value].copy(), ms[: count.value].copy()
+
+    def set_cost_model(self, model):
+        self.lib.call("qcs_simulator_set_cost_model", self.h, model.h if model is not None else None)
+
+    def planner_judge(self):
+        used = ctypes.c_int()
+        g, lrn = ctypes.c_double(), ctypes.c_double()
+        self.lib.call("qcs_simulator_get_planner_judge", self.h, ctypes.byref(used), ctypes.byref(g), ctypes.byref(lrn))
+        return {"learned_plan": bool(used.value), "greedy_ms": g.value, "learned_ms": lrn.value}
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_FP)
+
+
+class CostModel:
+    """The learned pass-cost model (MLP 4 -> 64 -> 64 -> 1, trained on the GPU)."""
+
+    def __init__(self, lib: Library, seed: int = 1):
+        self.lib = lib
+        self.h = _P()
+        lib.call("qcs_b200_cost_model_create", ctypes.byref(self.h), seed)
+
+    def close(self):
+        if self.h:
+            self.lib.call("qcs_b200_cost_model_destroy", self.h)
+            self.h = _P()
+
+    def train(self, features, targets, epochs=200, batch=256, lr=1e-3) -> float:
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        loss = ctypes.c_float()
+        self.lib.call("qcs_b200_cost_model_train", self.h, _fptr(f), _fptr(t), len(t), epochs, batch, lr,
+                      ctypes.byref(loss))
+        return loss.value
+
+    def predict(self, features) -> np.ndarray:
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        out = np.zeros(len(f), dtype=np.float32)
+        self.lib.call("qcs_b200_cost_model_predict", self.h, _fptr(f), len(f), _fptr(out))
+        return out
+
+    def gradients(self, inputs, targets):
+        x = np.ascontiguousarray(inputs, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.zeros(COST_MODEL_PARAMS, dtype=np.float32)
+        loss = ctypes.c_float()
+        self.lib.call("qcs_b200_cost_model_gradients", self.h, _fptr(x), _fptr(t), len(t), _fptr(g), ctypes.byref(loss))
+        return g, loss.value
+
+    def params(self):
+        p = np.zeros(COST_MODEL_PARAMS, dtype=np.float32)
+        s = np.zeros(COST_MODEL_SCALING, dtype=np.float32)
+        self.lib.call("qcs_b200_cost_model_get_params", self.h, _fptr(p), _fptr(s))
+        return p, s
+
+    def set_params(self, params, scaling):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        s = np.ascontiguousarray(scaling, dtype=np.float32)
+        self.lib.call("qcs_b200_cost_model_set_params", self.h, _fptr(p), _fptr(s))
 
 
 def fidelity(a: np.ndarray, b: np.ndarray) -> float:

@@ -1,0 +1,69 @@
+"""Self-recorded pass timings and training of the learned cost model.
+
+The simulator times every fused pass it launches while kernel timing is on
+(features: local qubits, highest local physical qubit, gate count, bytes per
+amplitude). `collect_pass_timings` runs seeded random circuits with varied
+pass sizes to gather many such samples; `train_cost_model` fits the MLP on
+log(ns per amplitude) with the library's own CUDA kernels.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import FUSION_GREEDY, CostModel, Library, Simulator
+from . import circuits as C
+
+_MIX = ["u3", "x", "h", "rz", "p", "ry", "swap", "rzz", "rxx", "sx"]
+
+
+def collect_pass_timings(lib: Library, n: int, min_samples: int, seed: int = 1, max_rounds: int = 100000):
+    """Return (features [N x 4] float32, target [N] float32 = log(ns/amp))."""
+    rng = np.random.default_rng(seed)
+    feats, targets = [], []
+    total = 0
+    with Simulator(lib, n, fusion=FUSION_GREEDY) as sim:
+        sim.set_kernel_timing(True)
+        rounds = 0
+        while total < min_samples and rounds < max_rounds:
+            rounds += 1
+            max_ops = int(rng.integers(1, 65))
+            local = int(rng.integers(9, 12))
+            sim.set_planner_options(max_ops, local)
+            gates = list(rng.choice(_MIX, size=int(rng.integers(2, len(_MIX) + 1)), replace=False))
+            circ = C.random_circuit(n, int(rng.integers(64, 400)), seed=int(rng.integers(1 << 30)),
+                                    max_controls=int(rng.integers(0, 3)), gates=gates)
+            sim.run(circ)
+            sim.synchronize()
+            f, ms = sim.pass_records()
+            if len(ms):
+                feats.append(f)
+                targets.append(np.log(ms.astype(np.float64) * 1e6 / float(1 << n)).astype(np.float32))
+                total += len(ms)
+        sim.set_kernel_timing(False)
+        sim.set_planner_options(0, 0)
+    if not feats:
+        return np.zeros((0, 4), np.float32), np.zeros(0, np.float32)
+    return np.concatenate(feats), np.concatenate(targets)
+
+
+def train_cost_model(lib: Library, features, targets, epochs: int = 150, batch: int = 256, lr: float = 2e-3,
+                     seed: int = 7):
+    model = CostModel(lib, seed)
+    loss = model.train(features, targets, epochs=epochs, batch=batch, lr=lr)
+    return model, loss
+
+
+def predicted_pass_ms(model: CostModel, features, n: int) -> np.ndarray:
+    return np.exp(model.predict(features).astype(np.float64)) * float(1 << n) * 1e-6
+
+
+def relative_error(model: CostModel, features, targets) -> float:
+    """Median |predicted / measured - 1| of the time per amplitude."""
+    pred = model.predict(features).astype(np.float64)
+    return float(np.median(np.abs(np.exp(pred - np.asarray(targets, np.float64)) - 1.0)))
+
+
+__all__ = ["collect_pass_timings", "train_cost_model", "predicted_pass_ms", "relative_error", "math"]

@@ -82,6 +82,38 @@ def test_cli_mapping_options(oracle_lib, reverse):
         assert np.max(np.abs(np.fromfile(sv, dtype=np.complex128) - ref)) <= 1e-12
 
 
+REF_CLI = REPO / "oracle" / "_ref" / "qcs_ref"
+
+
+@pytest.mark.parametrize("fusion", ["0", "1"])
+def test_cli_matches_reference_cli(fusion):
+    """Both drivers, same plug-in, same pinned seed: identical JSON clbits on
+    every sample and the same saved state."""
+    if not REF_CLI.exists():
+        pytest.fail("oracle/_ref/qcs_ref is missing: run `make -C oracle ref` where the reference sources are")
+    n, samples, seed = 10, 24, 4242
+    circ = C.layered_u3_cz(n, 5, seed=11)
+    circ += [("measure", (q,), (q,), (), ()) for q in range(0, n, 2)]
+    circ += C.random_circuit(n, 30, seed=12, max_controls=1, gates=["u3", "x", "h", "rz"])
+    circ += [("measure", (q,), (q,), (), ()) for q in range(n)]
+    with tempfile.TemporaryDirectory() as d:
+        gl = Path(d) / "c.txt"
+        gl.write_text(C.to_gatelist(circ, n, n))
+        outs = []
+        for exe in (qcs_b200.CLI_PATH, REF_CLI):
+            sv = Path(d) / f"{exe.name}.bin"
+            env = dict(os.environ)
+            env.update({"QCS_GATELIST": str(gl), "LD_PRELOAD": str(SHIM), "QCS_REF_SEED": str(seed),
+                        "QCS_FUSION": fusion})
+            r = subprocess.run([str(exe), "-s", str(samples), "--output-statevector", str(sv), str(GATELIST_SO)],
+                               capture_output=True, text=True, env=env, timeout=300)
+            assert r.returncode == 0, r.stderr
+            lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+            outs.append(([ln["clbits"] for ln in lines], np.fromfile(sv, dtype=np.complex128)))
+        assert outs[0][0] == outs[1][0]
+        assert np.max(np.abs(outs[0][1] - outs[1][1])) <= 1e-12
+
+
 def test_cli_ghz_shots_are_all_zero_or_all_one():
     lines = _run_cli(["-s", "32", str(GHZ_SO)], {"NUM_QUBITS": "16"})
     assert len(lines) == 32

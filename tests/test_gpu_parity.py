@@ -101,6 +101,37 @@ def test_mapping_and_saved_file(gpu_lib, oracle_lib, mode):
         assert np.max(np.abs(a - b)) <= TOL
 
 
+@pytest.mark.parametrize("mode", MODES)
+def test_swaps_mappings_and_reinitialization(gpu_lib, oracle_lib, mode):
+    # uncontrolled swaps become relabels in the fused modes; mapping changes
+    # and reinitialize_mapping must still act exactly as in the reference
+    n = 10
+    rng = np.random.default_rng(5)
+    part_a = C.random_circuit(n, 80, seed=41, max_controls=1, gates=["swap", "u3", "x", "rz", "h", "p"])
+    part_a += [("swap", (), tuple(int(v) for v in rng.choice(n, 2, replace=False)), (), ()) for _ in range(12)]
+    part_a += [("measure", (q,), (q,), (), ()) for q in (1, 4, 7)]
+    part_b = C.random_circuit(n, 60, seed=42, max_controls=2, gates=["swap", "u3", "rxx", "x"])
+    m1 = [3, 9, 0, 6, 1, 8, 2, 7, 5, 4]
+    m2 = list(reversed(m1))
+    out = []
+    for lib, fus in ((gpu_lib, mode), (oracle_lib, None)):
+        with qcs_b200.Simulator(lib, n, n, mapping=m1, seed=9, fusion=fus) as sim:
+            sim.run(part_a)
+            sim.reinitialize_mapping()
+            sim.run(part_b)
+            sim.set_mapping(m2)
+            sim.reinitialize_mapping()
+            sim.run(part_b)
+            with tempfile.TemporaryDirectory() as d:
+                p = os.path.join(d, "s.bin")
+                sim.save_statevector(p)
+                saved = np.fromfile(p, dtype=np.complex128)
+            out.append((sim.statevector(), saved, sim.clbits_string()))
+    assert out[0][2] == out[1][2]
+    assert np.max(np.abs(out[0][0] - out[1][0])) <= TOL
+    assert np.max(np.abs(out[0][1] - out[1][1])) <= TOL
+
+
 def test_saved_file_bytes_equal_state(gpu_lib):
     n = 23   # several staging chunks
     with qcs_b200.Simulator(gpu_lib, n) as sim:

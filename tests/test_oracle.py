@@ -139,6 +139,27 @@ def test_oracle_errors_are_reported(oracle_lib):
             sim.gate("x", (), (1,), (), (1,))
 
 
+def test_mlp_oracle_gradient_matches_finite_differences():
+    import sys as _sys
+
+    _sys.path.insert(0, str(Path(__file__).resolve().parent.parent / "oracle"))
+    import mlp_oracle
+
+    rng = np.random.default_rng(0)
+    params = rng.normal(scale=0.3, size=mlp_oracle.NPARAMS)
+    x = rng.normal(size=(7, 4))
+    t = rng.normal(size=7)
+    _, g = mlp_oracle.loss_and_gradients(params, x, t)
+    idx = rng.choice(mlp_oracle.NPARAMS, size=60, replace=False)
+    eps = 1e-6
+    for i in idx:
+        p1, p2 = params.copy(), params.copy()
+        p1[i] += eps
+        p2[i] -= eps
+        fd = (mlp_oracle.loss_and_gradients(p1, x, t)[0] - mlp_oracle.loss_and_gradients(p2, x, t)[0]) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
+
+
 # ------------------------------------------------------------ golden fixtures
 
 
