@@ -39,6 +39,16 @@ int qcs_simulator_set_fusion(qcs_simulator *sim, int mode);
 int qcs_simulator_get_fusion(const qcs_simulator *sim, int *mode);
 
 /*
+ * Amplitude precision, set before allocate_memory: 128 (complex128, the
+ * reference's type and the default) or 64 (complex64: half the memory and
+ * traffic, FP32 gate arithmetic). Norms, probabilities, <Z> and the sampler
+ * accumulate in FP64 either way, and state transfers and saved files are
+ * complex128 (the reference's file format) in both.
+ */
+int qcs_simulator_set_precision(qcs_simulator *sim, int amplitude_bits);
+int qcs_simulator_get_precision(const qcs_simulator *sim, int *amplitude_bits);
+
+/*
  * Pin the measurement random-number generator. The engine is
  * std::mt19937_64 seeded with a 32-bit value, as in the reference
  * (src/qcs.cu:1845-1852), so the same seed gives the same sequence of

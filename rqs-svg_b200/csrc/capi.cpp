@@ -701,3 +701,13 @@ extern "C" int qcs_simulator_get_planner_judge(qcs_simulator *sim, int *learned_
             *learned_ms = f->last_learned_ms;
     });
 }
+
+extern "C" int qcs_simulator_set_precision(qcs_simulator *sim, int amplitude_bits)
+{
+    return guarded([&] { core(sim).set_precision(amplitude_bits); });
+}
+
+extern "C" int qcs_simulator_get_precision(const qcs_simulator *sim, int *amplitude_bits)
+{
+    return guarded([&] { write_result(amplitude_bits, core(sim).precision()); });
+}

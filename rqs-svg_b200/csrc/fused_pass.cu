@@ -73,7 +73,7 @@ struct FStage
 
 struct FPassParams
 {
-    double2 *state;
+    void *state;
     int n;
     int k;
     uint64_t chunks;
@@ -84,28 +84,54 @@ struct FPassParams
     FOp ops[kFusedMaxOps];
 };
 
-__device__ __forceinline__ int swz(int j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7); }
+// Shared-memory swizzle, an XOR of higher index bits into the bits that pick
+// the bank group: 16-byte amplitudes (8 per 128-byte line) fold 3 bits,
+// 8-byte amplitudes (16 per line) fold 4. Both are linear over GF(2).
+template <typename V>
+__device__ __forceinline__ int swz(int j);
+template <>
+__device__ __forceinline__ int swz<double2>(int j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7); }
+template <>
+__device__ __forceinline__ int swz<float2>(int j) { return j ^ (((j >> 4) ^ (j >> 8)) & 15); }
 
-__device__ __forceinline__ double2 cmul(double2 m, double2 v)
+template <typename V>
+__device__ __forceinline__ V cvt(double2 m);
+template <>
+__device__ __forceinline__ double2 cvt<double2>(double2 m) { return m; }
+template <>
+__device__ __forceinline__ float2 cvt<float2>(double2 m) { return make_float2(static_cast<float>(m.x), static_cast<float>(m.y)); }
+
+template <typename V>
+__device__ __forceinline__ V cmul(V m, V v)
 {
-    double2 r;
+    V r;
     r.x = fma(m.x, v.x, -m.y * v.y);
     r.y = fma(m.x, v.y, m.y * v.x);
     return r;
 }
 
-__device__ __forceinline__ double2 cmad2(double2 m0, double2 v0, double2 m1, double2 v1)
+template <typename V>
+__device__ __forceinline__ V cmad2(V m0, V v0, V m1, V v1)
 {
-    double2 r;
+    V r;
     r.x = fma(m0.x, v0.x, fma(-m0.y, v0.y, fma(m1.x, v1.x, -m1.y * v1.y)));
     r.y = fma(m0.x, v0.y, fma(m0.y, v0.x, fma(m1.x, v1.y, m1.y * v1.x)));
     return r;
 }
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+template <typename V>
+__device__ __forceinline__ void cp_async_amp(V *smem, const V *gmem);
+template <>
+__device__ __forceinline__ void cp_async_amp<double2>(double2 *smem, const double2 *gmem)
 {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+template <>
+__device__ __forceinline__ void cp_async_amp<float2>(float2 *smem, const float2 *gmem)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -118,10 +144,10 @@ constexpr int R = 1 << kStageBits;
 // local controls take the unconditional path; controlled ones predicate each
 // pair or amplitude on (jr & lcmask) == lcval.
 
-template <int B>
-__device__ __forceinline__ void apply_dense1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V, int B>
+__device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
-    const double2 m00 = op.m[0], m01 = op.m[1], m10 = op.m[2], m11 = op.m[3];
+    const V m00 = cvt<V>(op.m[0]), m01 = cvt<V>(op.m[1]), m10 = cvt<V>(op.m[2]), m11 = cvt<V>(op.m[3]);
     const uint32_t cm = op.lcmask, cv = op.lcval;
     if (cm == 0)
     {
@@ -131,7 +157,7 @@ __device__ __forceinline__ void apply_dense1(double2 (&a)[R], const FOp &op, con
             if (r & (1 << B))
                 continue;
             const int r1 = r | (1 << B);
-            const double2 x0 = a[r], x1 = a[r1];
+            const V x0 = a[r], x1 = a[r1];
             a[r] = cmad2(m00, x0, m01, x1);
             a[r1] = cmad2(m10, x0, m11, x1);
         }
@@ -145,15 +171,15 @@ __device__ __forceinline__ void apply_dense1(double2 (&a)[R], const FOp &op, con
         if ((jr[r] & cm) == cv)
         {
             const int r1 = r | (1 << B);
-            const double2 x0 = a[r], x1 = a[r1];
+            const V x0 = a[r], x1 = a[r1];
             a[r] = cmad2(m00, x0, m01, x1);
             a[r1] = cmad2(m10, x0, m11, x1);
         }
     }
 }
 
-template <int B>
-__device__ __forceinline__ void apply_swap1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V, int B>
+__device__ __forceinline__ void apply_swap1(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     const uint32_t cm = op.lcmask, cv = op.lcval;
     if (cm == 0)
@@ -164,7 +190,7 @@ __device__ __forceinline__ void apply_swap1(double2 (&a)[R], const FOp &op, cons
             if (r & (1 << B))
                 continue;
             const int r1 = r | (1 << B);
-            const double2 t = a[r];
+            const V t = a[r];
             a[r] = a[r1];
             a[r1] = t;
         }
@@ -178,15 +204,15 @@ __device__ __forceinline__ void apply_swap1(double2 (&a)[R], const FOp &op, cons
         if ((jr[r] & cm) == cv)
         {
             const int r1 = r | (1 << B);
-            const double2 t = a[r];
+            const V t = a[r];
             a[r] = a[r1];
             a[r1] = t;
         }
     }
 }
 
-template <int B0, int B1>
-__device__ __forceinline__ void apply_dense2(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V, int B0, int B1>
+__device__ __forceinline__ void apply_dense2(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
@@ -197,21 +223,21 @@ __device__ __forceinline__ void apply_dense2(double2 (&a)[R], const FOp &op, con
         if ((jr[r] & cm) != cv)
             continue;
         const int i1 = r | (1 << B0), i2 = r | (1 << B1), i3 = r | (1 << B0) | (1 << B1);
-        const double2 x0 = a[r], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+        const V x0 = a[r], x1 = a[i1], x2 = a[i2], x3 = a[i3];
         const double2 *m = op.m;
-        const double2 y0 = cmad2(m[0], x0, m[1], x1), t0 = cmad2(m[2], x2, m[3], x3);
-        const double2 y1 = cmad2(m[4], x0, m[5], x1), t1 = cmad2(m[6], x2, m[7], x3);
-        const double2 y2 = cmad2(m[8], x0, m[9], x1), t2 = cmad2(m[10], x2, m[11], x3);
-        const double2 y3 = cmad2(m[12], x0, m[13], x1), t3 = cmad2(m[14], x2, m[15], x3);
-        a[r] = make_double2(y0.x + t0.x, y0.y + t0.y);
-        a[i1] = make_double2(y1.x + t1.x, y1.y + t1.y);
-        a[i2] = make_double2(y2.x + t2.x, y2.y + t2.y);
-        a[i3] = make_double2(y3.x + t3.x, y3.y + t3.y);
+        const V y0 = cmad2(cvt<V>(m[0]), x0, cvt<V>(m[1]), x1), t0 = cmad2(cvt<V>(m[2]), x2, cvt<V>(m[3]), x3);
+        const V y1 = cmad2(cvt<V>(m[4]), x0, cvt<V>(m[5]), x1), t1 = cmad2(cvt<V>(m[6]), x2, cvt<V>(m[7]), x3);
+        const V y2 = cmad2(cvt<V>(m[8]), x0, cvt<V>(m[9]), x1), t2 = cmad2(cvt<V>(m[10]), x2, cvt<V>(m[11]), x3);
+        const V y3 = cmad2(cvt<V>(m[12]), x0, cvt<V>(m[13]), x1), t3 = cmad2(cvt<V>(m[14]), x2, cvt<V>(m[15]), x3);
+        a[r] = V{y0.x + t0.x, y0.y + t0.y};
+        a[i1] = V{y1.x + t1.x, y1.y + t1.y};
+        a[i2] = V{y2.x + t2.x, y2.y + t2.y};
+        a[i3] = V{y3.x + t3.x, y3.y + t3.y};
     }
 }
 
-template <int B0, int B1>
-__device__ __forceinline__ void apply_swap2(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V, int B0, int B1>
+__device__ __forceinline__ void apply_swap2(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
@@ -222,16 +248,17 @@ __device__ __forceinline__ void apply_swap2(double2 (&a)[R], const FOp &op, cons
         if ((jr[r] & cm) == cv)
         {
             const int i1 = r | (1 << B0), i2 = r | (1 << B1);
-            const double2 t = a[i1];
+            const V t = a[i1];
             a[i1] = a[i2];
             a[i2] = t;
         }
     }
 }
 
-__device__ __forceinline__ void apply_phase(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V>
+__device__ __forceinline__ void apply_phase(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
-    const double2 e = op.m[0];
+    const V e = cvt<V>(op.m[0]);
     const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
     for (int r = 0; r < R; ++r)
@@ -239,11 +266,12 @@ __device__ __forceinline__ void apply_phase(double2 (&a)[R], const FOp &op, cons
             a[r] = cmul(e, a[r]);
 }
 
-__device__ __forceinline__ void apply_diag(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R], uint64_t cbase)
+template <typename V>
+__device__ __forceinline__ void apply_diag(V (&a)[R], const FOp &op, const uint32_t (&jr)[R], uint64_t cbase)
 {
     // one or two targets: entries in registers, chosen per amplitude by its
     // target bits (from the local index, or from the chunk when not local)
-    const double2 d0 = op.m[0], d1 = op.m[1], d2 = op.m[2], d3 = op.m[3];
+    const V d0 = cvt<V>(op.m[0]), d1 = cvt<V>(op.m[1]), d2 = cvt<V>(op.m[2]), d3 = cvt<V>(op.m[3]);
     const uint32_t cm = op.lcmask, cv = op.lcval;
     const int l0 = op.loc[0], l1 = op.nt > 1 ? op.loc[1] : -1;
     const uint32_t c0 = l0 < 0 ? static_cast<uint32_t>((cbase >> op.phys[0]) & 1ull) : 0u;
@@ -259,65 +287,73 @@ __device__ __forceinline__ void apply_diag(double2 (&a)[R], const FOp &op, const
             continue;
         const uint32_t s0 = use0 ? ((j >> sh0) & 1u) : c0;
         const uint32_t s1 = use1 ? ((j >> sh1) & 1u) : c1;
-        const double2 d = s1 ? (s0 ? d3 : d2) : (s0 ? d1 : d0);
+        const V d = s1 ? (s0 ? d3 : d2) : (s0 ? d1 : d0);
         a[r] = cmul(d, a[r]);
     }
 }
 
-__device__ __forceinline__ void dispatch_dense1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V>
+__device__ __forceinline__ void dispatch_dense1(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     switch (op.b0)
     {
-    case 0: apply_dense1<0>(a, op, jr); break;
-    case 1: apply_dense1<1>(a, op, jr); break;
-    case 2: apply_dense1<2>(a, op, jr); break;
-    default: apply_dense1<3>(a, op, jr); break;
+    case 0: apply_dense1<V, 0>(a, op, jr); break;
+    case 1: apply_dense1<V, 1>(a, op, jr); break;
+    case 2: apply_dense1<V, 2>(a, op, jr); break;
+    default: apply_dense1<V, 3>(a, op, jr); break;
     }
 }
 
-__device__ __forceinline__ void dispatch_swap1(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V>
+__device__ __forceinline__ void dispatch_swap1(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     switch (op.b0)
     {
-    case 0: apply_swap1<0>(a, op, jr); break;
-    case 1: apply_swap1<1>(a, op, jr); break;
-    case 2: apply_swap1<2>(a, op, jr); break;
-    default: apply_swap1<3>(a, op, jr); break;
+    case 0: apply_swap1<V, 0>(a, op, jr); break;
+    case 1: apply_swap1<V, 1>(a, op, jr); break;
+    case 2: apply_swap1<V, 2>(a, op, jr); break;
+    default: apply_swap1<V, 3>(a, op, jr); break;
     }
 }
 
 // (b0, b1) with b0 < b1 encoded as b0 * 4 + b1
-__device__ __forceinline__ void dispatch_dense2(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V>
+__device__ __forceinline__ void dispatch_dense2(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     switch (op.b0 * 4 + op.b1)
     {
-    case 1: apply_dense2<0, 1>(a, op, jr); break;
-    case 2: apply_dense2<0, 2>(a, op, jr); break;
-    case 3: apply_dense2<0, 3>(a, op, jr); break;
-    case 6: apply_dense2<1, 2>(a, op, jr); break;
-    case 7: apply_dense2<1, 3>(a, op, jr); break;
-    default: apply_dense2<2, 3>(a, op, jr); break;
+    case 1: apply_dense2<V, 0, 1>(a, op, jr); break;
+    case 2: apply_dense2<V, 0, 2>(a, op, jr); break;
+    case 3: apply_dense2<V, 0, 3>(a, op, jr); break;
+    case 6: apply_dense2<V, 1, 2>(a, op, jr); break;
+    case 7: apply_dense2<V, 1, 3>(a, op, jr); break;
+    default: apply_dense2<V, 2, 3>(a, op, jr); break;
     }
 }
 
-__device__ __forceinline__ void dispatch_swap2(double2 (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V>
+__device__ __forceinline__ void dispatch_swap2(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
 {
     switch (op.b0 * 4 + op.b1)
     {
-    case 1: apply_swap2<0, 1>(a, op, jr); break;
-    case 2: apply_swap2<0, 2>(a, op, jr); break;
-    case 3: apply_swap2<0, 3>(a, op, jr); break;
-    case 6: apply_swap2<1, 2>(a, op, jr); break;
-    case 7: apply_swap2<1, 3>(a, op, jr); break;
-    default: apply_swap2<2, 3>(a, op, jr); break;
+    case 1: apply_swap2<V, 0, 1>(a, op, jr); break;
+    case 2: apply_swap2<V, 0, 2>(a, op, jr); break;
+    case 3: apply_swap2<V, 0, 3>(a, op, jr); break;
+    case 6: apply_swap2<V, 1, 2>(a, op, jr); break;
+    case 7: apply_swap2<V, 1, 3>(a, op, jr); break;
+    default: apply_swap2<V, 2, 3>(a, op, jr); break;
     }
 }
 
 // One CTA per chunk at a time; blockDim.x == 2^(k - kStageBits) <= 128, so
 // that three CTAs (12 warps, 3 x 64 KB of double-buffered chunks) share an SM.
-__global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constant__ FPassParams p)
+template <typename Real>
+__global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_kernel(const __grid_constant__ FPassParams p)
 {
-    extern __shared__ double2 smem[];
+    typedef typename Cx<Real>::T V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *smem = reinterpret_cast<V *>(smem_raw);
+    V *state = static_cast<V *>(p.state);
     const int k = p.k;
     const int T = 1 << (k - kStageBits);
     const int tid = threadIdx.x;
@@ -350,11 +386,11 @@ __global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constan
                 off |= hb[b];
         return off;
     };
-    auto issue_load = [&](uint64_t c, double2 *dst) {
+    auto issue_load = [&](uint64_t c, V *dst) {
         const uint64_t cb = chunk_base(c);
 #pragma unroll
         for (int m = 0; m < R; ++m)
-            cp_async16(dst + swz(tid + m * T), p.state + (cb | elem_offset(m)));
+            cp_async_amp<V>(dst + swz<V>(tid + m * T), state + (cb | elem_offset(m)));
         cp_async_commit();
     };
 
@@ -365,7 +401,7 @@ __global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constan
     int cur = 0;
     for (; c < p.chunks; c += gridDim.x)
     {
-        double2 *sb = smem + cur * chunk_elems;
+        V *sb = smem + cur * chunk_elems;
         const uint64_t next = c + gridDim.x;
         if (next < p.chunks)
         {
@@ -396,11 +432,11 @@ __global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constan
             for (int b = 0; b < kStageBits; ++b)
             {
                 bit[b] = 1u << S.sbits[b];
-                sbit[b] = static_cast<uint32_t>(swz(static_cast<int>(bit[b])));
+                sbit[b] = static_cast<uint32_t>(swz<V>(static_cast<int>(bit[b])));
             }
-            const uint32_t p0 = static_cast<uint32_t>(swz(static_cast<int>(j0)));
+            const uint32_t p0 = static_cast<uint32_t>(swz<V>(static_cast<int>(j0)));
             uint32_t jr[R], pos[R];
-            double2 a[R];
+            V a[R];
 #pragma unroll
             for (int r = 0; r < R; ++r)
             {
@@ -423,12 +459,12 @@ __global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constan
                     continue;
                 switch (op.kind)
                 {
-                case F_DENSE1: dispatch_dense1(a, op, jr); break;
-                case F_SWAP1: dispatch_swap1(a, op, jr); break;
-                case F_DENSE2: dispatch_dense2(a, op, jr); break;
-                case F_SWAP2: dispatch_swap2(a, op, jr); break;
-                case F_PHASE: apply_phase(a, op, jr); break;
-                default: apply_diag(a, op, jr, cbase); break;
+                case F_DENSE1: dispatch_dense1<V>(a, op, jr); break;
+                case F_SWAP1: dispatch_swap1<V>(a, op, jr); break;
+                case F_DENSE2: dispatch_dense2<V>(a, op, jr); break;
+                case F_SWAP2: dispatch_swap2<V>(a, op, jr); break;
+                case F_PHASE: apply_phase<V>(a, op, jr); break;
+                default: apply_diag<V>(a, op, jr, cbase); break;
                 }
             }
 #pragma unroll
@@ -440,7 +476,7 @@ __global__ void __launch_bounds__(128, 3) fused_pass_kernel(const __grid_constan
         const uint64_t cb = cbase;
 #pragma unroll
         for (int m = 0; m < R; ++m)
-            __stcs(p.state + (cb | elem_offset(m)), sb[swz(tid + m * T)]);
+            __stcs(state + (cb | elem_offset(m)), sb[swz<V>(tid + m * T)]);
         __syncthreads();
         cur ^= 1;
     }
@@ -800,22 +836,24 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
     return true;
 }
 
-int launch_fused_pass(double2 *state, int k, const FPassParams &prm, cudaStream_t stream)
+template <typename R>
+int launch_fused_pass(void *state, int k, const FPassParams &prm, cudaStream_t stream)
 {
+    typedef typename Cx<R>::T V;
     const int threads = 1 << (k - kStageBits);
-    const size_t smem = 2 * sizeof(double2) * (size_t(1) << k);
+    const size_t smem = 2 * sizeof(V) * (size_t(1) << k);
     static bool configured[64] = {};
     int dev = 0;
     QCSB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64 || !configured[dev])
     {
-        QCSB_CUDA(cudaFuncSetAttribute(fused_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       2 * 16 * (1 << kMaxLocal)));
+        QCSB_CUDA(cudaFuncSetAttribute(fused_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       2 * (int)sizeof(V) * (1 << kMaxLocal)));
         if (dev >= 0 && dev < 64)
             configured[dev] = true;
     }
     int per_sm = 0;
-    QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_pass_kernel, threads, smem));
+    QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_pass_kernel<R>, threads, smem));
     int sms = 148;
     QCSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     uint64_t grid = prm.chunks;
@@ -824,7 +862,7 @@ int launch_fused_pass(double2 *state, int k, const FPassParams &prm, cudaStream_
         grid = cap;
     FPassParams &p = const_cast<FPassParams &>(prm);
     p.state = state;
-    fused_pass_kernel<<<static_cast<unsigned>(grid), threads, smem, stream>>>(p);
+    fused_pass_kernel<R><<<static_cast<unsigned>(grid), threads, smem, stream>>>(p);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
@@ -853,7 +891,7 @@ int choose_local_bits(int n, int option)
     return clamp_local_bits(k, n);
 }
 
-PassFeatures pass_features(const PlannedPass &pp, int n)
+PassFeatures pass_features(const PlannedPass &pp, int n, int amp_bytes)
 {
     int top = 0;
     for (int b = 0; b < n; ++b)
@@ -863,7 +901,7 @@ PassFeatures pass_features(const PlannedPass &pp, int n)
     f.f[0] = static_cast<float>(pp.k);
     f.f[1] = static_cast<float>(top);
     f.f[2] = static_cast<float>(pp.ops.size());
-    f.f[3] = static_cast<float>(sizeof(double2));
+    f.f[3] = static_cast<float>(amp_bytes);
     return f;
 }
 
@@ -881,7 +919,8 @@ uint64_t fill_local(uint64_t local, int n, int k)
 // A candidate pass [i, j) with local qubits k is feasible when the low
 // qubits plus its dense targets fit in k and it holds at most max_ops gates.
 std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vector<Segment> &greedy, int n,
-                                  int max_ops, CostModel &model, double *predicted_greedy, double *predicted_learned)
+                                  int amp_bytes, int max_ops, CostModel &model, double *predicted_greedy,
+                                  double *predicted_learned)
 {
     const int kmin = clamp_local_bits(kStageBits + 5, n);
     const int kmax = clamp_local_bits(kMaxLocal, n);
@@ -902,7 +941,7 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
         while (gi < greedy.size() && greedy[gi].fused)
         {
             seq.insert(seq.end(), greedy[gi].pass.ops.begin(), greedy[gi].pass.ops.end());
-            greedy_feats.push_back(pass_features(greedy[gi].pass, n));
+            greedy_feats.push_back(pass_features(greedy[gi].pass, n, amp_bytes));
             ++gi;
         }
         const int L = (int)seq.size();
@@ -938,7 +977,7 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
                     pp.k = k;
                     pp.local = fill_local(d, n, k);
                     pp.ops.assign(j - i, 0);
-                    const PassFeatures f = pass_features(pp, n);
+                    const PassFeatures f = pass_features(pp, n, amp_bytes);
                     cands.push_back({i, j, k, pp.local});
                     feats.insert(feats.end(), f.f, f.f + 4);
                 }
@@ -1036,13 +1075,15 @@ void FusedExecutor::settle_judge()
     pending_learned_ = -1;
 }
 
-int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, int mode, qcs_b200_stats &stats,
-                       KernelTimer &timer)
+int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<GateOp> &ops, int mode,
+                       qcs_b200_stats &stats, KernelTimer &timer)
 {
+    const bool c64 = amp_bytes == (int)sizeof(float2);
     auto plain = [&](const GateOp &op) {
         if (timer.enabled)
-            timer.begin(stream_, KernelTimer::kPlain, 2.0 * sizeof(double2) * op.changed_amps(n));
-        const int k = launch_gate_plain(state, n, op, stream_);
+            timer.begin(stream_, KernelTimer::kPlain, 2.0 * amp_bytes * op.changed_amps(n));
+        const int k = c64 ? launch_gate_plain<float>(static_cast<float2 *>(state), n, op, stream_)
+                          : launch_gate_plain<double>(static_cast<double2 *>(state), n, op, stream_);
         if (timer.enabled)
             timer.end(stream_);
         stats.plain_gate_kernels += k;
@@ -1090,7 +1131,7 @@ int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, in
         if (use_learned)
         {
             double pg = 0.0, pl = 0.0;
-            segs = plan_learned(ops, segs, n, max_ops, *model_, &pg, &pl);
+            segs = plan_learned(ops, segs, n, amp_bytes, max_ops, *model_, &pg, &pl);
         }
         if (entry->learned_ms < 0.0 || entry->greedy_ms < 0.0)
         {
@@ -1122,10 +1163,11 @@ int FusedExecutor::run(double2 *state, int n, const std::vector<GateOp> &ops, in
         {
             if (timer.enabled)
             {
-                const PassFeatures f = pass_features(s.pass, n);
-                timer.begin(stream_, KernelTimer::kFused, 2.0 * sizeof(double2) * std::ldexp(1.0, n), &f);
+                const PassFeatures f = pass_features(s.pass, n, amp_bytes);
+                timer.begin(stream_, KernelTimer::kFused, 2.0 * amp_bytes * std::ldexp(1.0, n), &f);
             }
-            launches += launch_fused_pass(state, s.pass.k, *prm, stream_);
+            launches += c64 ? launch_fused_pass<float>(state, s.pass.k, *prm, stream_)
+                             : launch_fused_pass<double>(state, s.pass.k, *prm, stream_);
             if (timer.enabled)
                 timer.end(stream_);
             ++stats.fused_passes;

@@ -1,18 +1,19 @@
 // Plain-path kernels: one launch per gate, state preparation, measurement
-// reductions, collapse and <Z> sums.
+// reductions, collapse, <Z> sums and logical-order transfers.
 //
-// Layout: the register is one contiguous array of double2 (complex128,
-// 16-byte aligned); physical qubit q is bit q of the index. A gate on
-// targets T with controls C visits "groups": the 2^(n - |T u C|) indices
-// whose T and C bits are zero, enumerated by inserting zero bits at the
-// sorted operand positions (the role of thread_num_to_state_index_q*,
-// reference src/qcs.cu:156-376), then ORs in the control values and each
-// active target offset.
+// Layout: the register is one contiguous array of complex amplitudes
+// (double2 for complex128, float2 for complex64); physical qubit q is bit q
+// of the index. A gate on targets T with controls C visits "groups": the
+// 2^(n - |T u C|) indices whose T and C bits are zero, enumerated by
+// inserting zero bits at the sorted operand positions (the role of
+// thread_num_to_state_index_q*, reference src/qcs.cu:156-376), then ORs in
+// the control values and each active target offset.
 //
 // Consecutive threads take consecutive groups, so every warp reads and writes
-// contiguous 16-byte amplitudes wherever the operand bits are >= 5; loads use
-// the streaming cache hint (each amplitude is touched once per pass over a
-// register far larger than L2).
+// contiguous amplitudes wherever the operand bits are >= 5; loads and stores
+// use evict-first hints (each amplitude is touched once per pass over a
+// register far larger than L2). Gate arithmetic runs in the amplitude's
+// precision; every reduction accumulates in FP64.
 
 #include "qcs_internal.h"
 
@@ -29,7 +30,8 @@ constexpr int kThreads = 256;
 constexpr int kSMs = 148;
 constexpr int kMaxOps = kMaxQubits;
 
-__device__ __forceinline__ double2 cfma(double2 m, double2 v, double2 acc)
+template <typename V>
+__device__ __forceinline__ V cfma(V m, V v, V acc)
 {
     acc.x = fma(m.x, v.x, acc.x);
     acc.x = fma(-m.y, v.y, acc.x);
@@ -38,12 +40,30 @@ __device__ __forceinline__ double2 cfma(double2 m, double2 v, double2 acc)
     return acc;
 }
 
-__device__ __forceinline__ double2 cmul(double2 m, double2 v)
+template <typename V>
+__device__ __forceinline__ V cmul(V m, V v)
 {
-    double2 r;
+    V r;
     r.x = fma(m.x, v.x, -m.y * v.y);
     r.y = fma(m.x, v.y, m.y * v.x);
     return r;
+}
+
+template <typename V>
+__device__ __forceinline__ double norm2(V a)
+{
+    const double x = a.x, y = a.y;
+    return fma(x, x, y * y);
+}
+
+template <typename V>
+__host__ __device__ __forceinline__ V make_cx(double re, double im);
+template <>
+__host__ __device__ __forceinline__ double2 make_cx<double2>(double re, double im) { return make_double2(re, im); }
+template <>
+__host__ __device__ __forceinline__ float2 make_cx<float2>(double re, double im)
+{
+    return make_float2(static_cast<float>(re), static_cast<float>(im));
 }
 
 // Insert a zero bit below each mask boundary: masks[i] = (1 << pos_i) - 1
@@ -62,22 +82,23 @@ __device__ __forceinline__ uint64_t insert_zero_bits(uint64_t g, const uint64_t 
     return g;
 }
 
-template <int NA, bool DIAG>
+template <typename R, int NA, bool DIAG>
 struct PlainParams
 {
-    double2 *state;
+    typedef typename Cx<R>::T V;
+    V *state;
     uint64_t ngroups;
     uint64_t cval;
     int nops;
     uint64_t masks[kMaxOps];
     uint64_t off[NA];
-    double2 m[DIAG ? NA : NA * NA];
+    V m[DIAG ? NA : NA * NA];
 };
 
-template <bool STREAM>
-__device__ __forceinline__ double2 ld_amp(const double2 *p) { return STREAM ? __ldcs(p) : *p; }
-template <bool STREAM>
-__device__ __forceinline__ void st_amp(double2 *p, double2 v)
+template <bool STREAM, typename V>
+__device__ __forceinline__ V ld_amp(const V *p) { return STREAM ? __ldcs(p) : *p; }
+template <bool STREAM, typename V>
+__device__ __forceinline__ void st_amp(V *p, V v)
 {
     if (STREAM)
         __stcs(p, v);
@@ -86,14 +107,15 @@ __device__ __forceinline__ void st_amp(double2 *p, double2 v)
 }
 
 // STREAM selects evict-first cache hints; U groups per thread per iteration.
-template <int NA, bool DIAG, int U, bool STREAM>
-__global__ void __launch_bounds__(kThreads) gate_plain_kernel(const __grid_constant__ PlainParams<NA, DIAG> p)
+template <typename R, int NA, bool DIAG, int U, bool STREAM>
+__global__ void __launch_bounds__(kThreads) gate_plain_kernel(const __grid_constant__ PlainParams<R, NA, DIAG> p)
 {
+    typedef typename Cx<R>::T V;
     const uint64_t step = (uint64_t)gridDim.x * kThreads * U;
     for (uint64_t g0 = (uint64_t)blockIdx.x * kThreads * U + threadIdx.x; g0 < p.ngroups; g0 += step)
     {
         uint64_t base[U];
-        double2 v[U][NA];
+        V v[U][NA];
 #pragma unroll
         for (int u = 0; u < U; ++u)
         {
@@ -123,7 +145,7 @@ __global__ void __launch_bounds__(kThreads) gate_plain_kernel(const __grid_const
 #pragma unroll
                 for (int a = 0; a < NA; ++a)
                 {
-                    double2 acc = make_double2(0.0, 0.0);
+                    V acc = make_cx<V>(0.0, 0.0);
 #pragma unroll
                     for (int b = 0; b < NA; ++b)
                         acc = cfma(p.m[a * NA + b], v[u][b], acc);
@@ -176,11 +198,12 @@ int plain_variant()
     return v;
 }
 
-template <int NA, bool DIAG>
-int launch_plain_na(double2 *state, int n, const GateOp &op, cudaStream_t stream)
+template <typename R, int NA, bool DIAG>
+int launch_plain_na(typename Cx<R>::T *state, int n, const GateOp &op, cudaStream_t stream)
 {
+    typedef typename Cx<R>::T V;
     constexpr int U = NA == 1 ? 4 : (NA == 2 ? 2 : 1);
-    PlainParams<NA, DIAG> p;
+    PlainParams<R, NA, DIAG> p;
     std::memset(&p, 0, sizeof(p));
     p.state = state;
     p.nops = fill_masks(op, p.masks);
@@ -196,41 +219,41 @@ int launch_plain_na(double2 *state, int n, const GateOp &op, cudaStream_t stream
     }
     const int nm = DIAG ? NA : NA * NA;
     for (int k = 0; k < nm; ++k)
-        p.m[k] = make_double2(op.mat[k].re, op.mat[k].im);
+        p.m[k] = make_cx<V>(op.mat[k].re, op.mat[k].im);
     const uint64_t one_shot_cap = 1ull << 31;
     switch (plain_variant())
     {
     case 0:
-        gate_plain_kernel<NA, DIAG, U, true><<<grid_for(p.ngroups, kThreads * U), kThreads, 0, stream>>>(p);
+        gate_plain_kernel<R, NA, DIAG, U, true><<<grid_for(p.ngroups, kThreads * U), kThreads, 0, stream>>>(p);
         break;
     case 2:
-        gate_plain_kernel<NA, DIAG, 1, true><<<grid_for(p.ngroups, kThreads, one_shot_cap), kThreads, 0, stream>>>(p);
+        gate_plain_kernel<R, NA, DIAG, 1, true><<<grid_for(p.ngroups, kThreads, one_shot_cap), kThreads, 0, stream>>>(p);
         break;
     case 3:
-        gate_plain_kernel<NA, DIAG, U, false><<<grid_for(p.ngroups, kThreads * U), kThreads, 0, stream>>>(p);
+        gate_plain_kernel<R, NA, DIAG, U, false><<<grid_for(p.ngroups, kThreads * U), kThreads, 0, stream>>>(p);
         break;
     default:
-        gate_plain_kernel<NA, DIAG, 1, false><<<grid_for(p.ngroups, kThreads, one_shot_cap), kThreads, 0, stream>>>(p);
+        gate_plain_kernel<R, NA, DIAG, 1, false><<<grid_for(p.ngroups, kThreads, one_shot_cap), kThreads, 0, stream>>>(p);
         break;
     }
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
 
-template <bool DIAG>
-int launch_plain_dispatch(double2 *state, int n, const GateOp &op, cudaStream_t stream)
+template <typename R, bool DIAG>
+int launch_plain_dispatch(typename Cx<R>::T *state, int n, const GateOp &op, cudaStream_t stream)
 {
     switch (op.na)
     {
-    case 1: return launch_plain_na<1, DIAG>(state, n, op, stream);
-    case 2: return launch_plain_na<2, DIAG>(state, n, op, stream);
-    case 3: return launch_plain_na<3, DIAG>(state, n, op, stream);
-    case 4: return launch_plain_na<4, DIAG>(state, n, op, stream);
-    case 5: return launch_plain_na<5, DIAG>(state, n, op, stream);
-    case 6: return launch_plain_na<6, DIAG>(state, n, op, stream);
-    case 7: return launch_plain_na<7, DIAG>(state, n, op, stream);
-    case 8: return launch_plain_na<8, DIAG>(state, n, op, stream);
-    case 16: return launch_plain_na<16, DIAG>(state, n, op, stream);
+    case 1: return launch_plain_na<R, 1, DIAG>(state, n, op, stream);
+    case 2: return launch_plain_na<R, 2, DIAG>(state, n, op, stream);
+    case 3: return launch_plain_na<R, 3, DIAG>(state, n, op, stream);
+    case 4: return launch_plain_na<R, 4, DIAG>(state, n, op, stream);
+    case 5: return launch_plain_na<R, 5, DIAG>(state, n, op, stream);
+    case 6: return launch_plain_na<R, 6, DIAG>(state, n, op, stream);
+    case 7: return launch_plain_na<R, 7, DIAG>(state, n, op, stream);
+    case 8: return launch_plain_na<R, 8, DIAG>(state, n, op, stream);
+    case 16: return launch_plain_na<R, 16, DIAG>(state, n, op, stream);
     default: break;
     }
     // 9..15 active sub-indices: pad with inactive sub-indices (identity
@@ -266,24 +289,27 @@ int launch_plain_dispatch(double2 *state, int n, const GateOp &op, cudaStream_t 
                 padded.mat[a * 16 + b] = v;
             }
     }
-    return launch_plain_na<16, DIAG>(state, n, padded, stream);
+    return launch_plain_na<R, 16, DIAG>(state, n, padded, stream);
 }
 
 // ------------------------------------------------------------ preparation
 
-__global__ void fill_kernel(double2 *state, uint64_t count, double2 value)
+template <typename V>
+__global__ void fill_kernel(V *state, uint64_t count, V value)
 {
     for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (uint64_t)gridDim.x * kThreads)
         __stcs(state + i, value);
 }
 
-__global__ void sequential_kernel(double2 *state, uint64_t count)
+template <typename V>
+__global__ void sequential_kernel(V *state, uint64_t count)
 {
     for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (uint64_t)gridDim.x * kThreads)
-        __stcs(state + i, make_double2(static_cast<double>(i), 0.0));
+        __stcs(state + i, make_cx<V>(static_cast<double>(i), 0.0));
 }
 
-__global__ void set_one_kernel(double2 *state, uint64_t index, double2 value) { state[index] = value; }
+template <typename V>
+__global__ void set_one_kernel(V *state, uint64_t index, V value) { state[index] = value; }
 
 // ------------------------------------------------------------ reductions
 
@@ -295,9 +321,10 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+template <typename R>
 struct ProbParams
 {
-    const double2 *state;
+    const typename Cx<R>::T *state;
     uint64_t ngroups;
     uint64_t cval;
     uint64_t tbit;
@@ -308,16 +335,15 @@ struct ProbParams
 
 // Per-block (sum |a0|^2, sum |a1|^2) over the groups; fixed reduction order,
 // so repeated calls give identical sums.
-__global__ void __launch_bounds__(kThreads) measure_probs_kernel(const __grid_constant__ ProbParams p)
+template <typename R>
+__global__ void __launch_bounds__(kThreads) measure_probs_kernel(const __grid_constant__ ProbParams<R> p)
 {
     double s0 = 0.0, s1 = 0.0;
     for (uint64_t g = (uint64_t)blockIdx.x * kThreads + threadIdx.x; g < p.ngroups; g += (uint64_t)gridDim.x * kThreads)
     {
         const uint64_t i0 = insert_zero_bits<kMaxOps>(g, p.masks, p.nops) | p.cval;
-        const double2 a0 = __ldcs(p.state + i0);
-        const double2 a1 = __ldcs(p.state + (i0 | p.tbit));
-        s0 = fma(a0.x, a0.x, fma(a0.y, a0.y, s0));
-        s1 = fma(a1.x, a1.x, fma(a1.y, a1.y, s1));
+        s0 += norm2(__ldcs(p.state + i0));
+        s1 += norm2(__ldcs(p.state + (i0 | p.tbit)));
     }
     __shared__ double sh[2][kThreads / 32];
     s0 = warp_sum(s0);
@@ -372,13 +398,14 @@ __global__ void __launch_bounds__(kThreads) sum_partials2_kernel(const double2 *
     }
 }
 
-__global__ void collapse_kernel(double2 *state, uint64_t ngroups, uint64_t lowmask, uint64_t zero_bit)
+template <typename V>
+__global__ void collapse_kernel(V *state, uint64_t ngroups, uint64_t lowmask, uint64_t zero_bit)
 {
     for (uint64_t g = (uint64_t)blockIdx.x * kThreads + threadIdx.x; g < ngroups; g += (uint64_t)gridDim.x * kThreads)
     {
         const uint64_t lo = g & lowmask;
         const uint64_t i = lo | ((g ^ lo) << 1) | zero_bit;
-        __stcs(state + i, make_double2(0.0, 0.0));
+        __stcs(state + i, make_cx<V>(0.0, 0.0));
     }
 }
 
@@ -390,15 +417,15 @@ constexpr int kZThreads = 256;
 constexpr int kZMinBits = 12;                 // registers below this use one thread
 constexpr int kZMaxHi = kMaxQubits - kZMinBits; // "it" bits per thread
 
-__global__ void zsums_small_kernel(const double2 *state, int n, double *sums)
+template <typename V>
+__global__ void zsums_small_kernel(const V *state, int n, double *sums)
 {
     double s[kMaxQubits + 1];
     for (int j = 0; j <= n; ++j)
         s[j] = 0.0;
     for (uint64_t i = 0; i < (1ull << n); ++i)
     {
-        const double2 a = state[i];
-        const double pr = fma(a.x, a.x, a.y * a.y);
+        const double pr = norm2(state[i]);
         s[0] += pr;
         for (int q = 0; q < n; ++q)
             if ((i >> q) & 1)
@@ -408,7 +435,8 @@ __global__ void zsums_small_kernel(const double2 *state, int n, double *sums)
         sums[j] = s[j];
 }
 
-__global__ void __launch_bounds__(kZThreads) zsums_kernel(const double2 *state, int n, int gbits, double *partials)
+template <typename V>
+__global__ void __launch_bounds__(kZThreads) zsums_kernel(const V *state, int n, int gbits, double *partials)
 {
     const uint64_t gt = (uint64_t)blockIdx.x * kZThreads + threadIdx.x;
     const uint64_t G = 1ull << gbits;
@@ -429,10 +457,7 @@ __global__ void __launch_bounds__(kZThreads) zsums_kernel(const double2 *state, 
             double pr[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i)
-            {
-                const double2 a = __ldcs(state + ((blk << 4) + i) * G + gt);
-                pr[i] = fma(a.x, a.x, a.y * a.y);
-            }
+                pr[i] = norm2(__ldcs(state + ((blk << 4) + i) * G + gt));
             double t = 0.0;
 #pragma unroll
             for (int i = 0; i < 16; ++i)
@@ -458,8 +483,7 @@ __global__ void __launch_bounds__(kZThreads) zsums_kernel(const double2 *state, 
     {
         for (uint64_t it = 0; it < iters; ++it)
         {
-            const double2 a = __ldcs(state + it * G + gt);
-            const double pr = fma(a.x, a.x, a.y * a.y);
+            const double pr = norm2(__ldcs(state + it * G + gt));
             total += pr;
 #pragma unroll
             for (int q = 0; q < kZMaxHi; ++q)
@@ -516,7 +540,7 @@ __global__ void zsums_final_kernel(const double *partials, int nblocks, int nsum
     }
 }
 
-// ------------------------------------------------------------ gather
+// ------------------------------------------------------------ transfers
 
 struct PermParams
 {
@@ -532,16 +556,35 @@ __device__ __forceinline__ uint64_t logical_to_physical(uint64_t l, const PermPa
     return ph;
 }
 
-__global__ void gather_logical_kernel(const double2 *state, PermParams pp, uint64_t begin, uint64_t count, double2 *out)
+template <typename V>
+__global__ void gather_logical_kernel(const V *state, PermParams pp, uint64_t begin, uint64_t count, double2 *out)
 {
     for (uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (uint64_t)gridDim.x * kThreads)
-        out[k] = state[logical_to_physical(begin + k, pp)];
+    {
+        const V a = state[logical_to_physical(begin + k, pp)];
+        out[k] = make_double2(a.x, a.y);
+    }
 }
 
-__global__ void scatter_logical_kernel(double2 *state, PermParams pp, uint64_t begin, uint64_t count, const double2 *in)
+template <typename V>
+__global__ void scatter_logical_kernel(V *state, PermParams pp, uint64_t begin, uint64_t count, const double2 *in)
 {
     for (uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (uint64_t)gridDim.x * kThreads)
-        state[logical_to_physical(begin + k, pp)] = in[k];
+        state[logical_to_physical(begin + k, pp)] = make_cx<V>(in[k].x, in[k].y);
+}
+
+template <typename V>
+__global__ void widen_kernel(const V *in, uint64_t count, double2 *out)
+{
+    for (uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (uint64_t)gridDim.x * kThreads)
+        out[k] = make_double2(in[k].x, in[k].y);
+}
+
+template <typename V>
+__global__ void narrow_kernel(const double2 *in, uint64_t count, V *out)
+{
+    for (uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (uint64_t)gridDim.x * kThreads)
+        out[k] = make_cx<V>(in[k].x, in[k].y);
 }
 
 PermParams make_perm(int n, const int *l2p)
@@ -555,49 +598,59 @@ PermParams make_perm(int n, const int *l2p)
 
 } // namespace
 
-int launch_gate_plain(double2 *state, int n, const GateOp &op, cudaStream_t stream)
+template <typename R>
+int launch_gate_plain(typename Cx<R>::T *state, int n, const GateOp &op, cudaStream_t stream)
 {
     if (op.na == 0)
         return 0;
-    return op.diag ? launch_plain_dispatch<true>(state, n, op, stream)
-                   : launch_plain_dispatch<false>(state, n, op, stream);
+    return op.diag ? launch_plain_dispatch<R, true>(state, n, op, stream)
+                   : launch_plain_dispatch<R, false>(state, n, op, stream);
 }
 
-int launch_init_zero(double2 *state, int n, cudaStream_t stream)
+template <typename R>
+int launch_init_zero(typename Cx<R>::T *state, int n, cudaStream_t stream)
 {
-    QCSB_CUDA(cudaMemsetAsync(state, 0, sizeof(double2) << n, stream));
-    set_one_kernel<<<1, 1, 0, stream>>>(state, 0, make_double2(1.0, 0.0));
+    typedef typename Cx<R>::T V;
+    QCSB_CUDA(cudaMemsetAsync(state, 0, sizeof(V) << n, stream));
+    set_one_kernel<V><<<1, 1, 0, stream>>>(state, 0, make_cx<V>(1.0, 0.0));
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
 
-int launch_init_flat(double2 *state, int n, cudaStream_t stream)
+template <typename R>
+int launch_init_flat(typename Cx<R>::T *state, int n, cudaStream_t stream)
 {
+    typedef typename Cx<R>::T V;
     const uint64_t count = 1ull << n;
-    fill_kernel<<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, count, make_double2(1.0, 0.0));
+    fill_kernel<V><<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, count, make_cx<V>(1.0, 0.0));
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
 
-int launch_init_sequential(double2 *state, int n, cudaStream_t stream)
+template <typename R>
+int launch_init_sequential(typename Cx<R>::T *state, int n, cudaStream_t stream)
 {
+    typedef typename Cx<R>::T V;
     const uint64_t count = 1ull << n;
-    sequential_kernel<<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, count);
+    sequential_kernel<V><<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, count);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
 
-int launch_set_amplitude(double2 *state, uint64_t index, double re, double im, cudaStream_t stream)
+template <typename R>
+int launch_set_amplitude(typename Cx<R>::T *state, uint64_t index, double re, double im, cudaStream_t stream)
 {
-    set_one_kernel<<<1, 1, 0, stream>>>(state, index, make_double2(re, im));
+    typedef typename Cx<R>::T V;
+    set_one_kernel<V><<<1, 1, 0, stream>>>(state, index, make_cx<V>(re, im));
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
 
-int launch_measure_probs(const double2 *state, int n, int t, uint64_t cmask, uint64_t cval,
+template <typename R>
+int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t cmask, uint64_t cval,
                          double2 *partials, double2 *result, cudaStream_t stream)
 {
-    ProbParams p;
+    ProbParams<R> p;
     std::memset(&p, 0, sizeof(p));
     p.state = state;
     GateOp op;
@@ -610,55 +663,97 @@ int launch_measure_probs(const double2 *state, int n, int t, uint64_t cmask, uin
     p.tbit = 1ull << t;
     p.partials = partials;
     // A fixed grid (independent of n) keeps the partial count constant.
-    measure_probs_kernel<<<kReduceBlocks, kThreads, 0, stream>>>(p);
+    measure_probs_kernel<R><<<kReduceBlocks, kThreads, 0, stream>>>(p);
     QCSB_CUDA(cudaGetLastError());
     sum_partials2_kernel<<<1, kThreads, 0, stream>>>(partials, kReduceBlocks, result);
     QCSB_CUDA(cudaGetLastError());
     return 2;
 }
 
-int launch_collapse(double2 *state, int n, int t, int keep_value, cudaStream_t stream)
+template <typename R>
+int launch_collapse(typename Cx<R>::T *state, int n, int t, int keep_value, cudaStream_t stream)
 {
+    typedef typename Cx<R>::T V;
     const uint64_t ngroups = 1ull << (n - 1);
     const uint64_t zero_bit = keep_value ? 0ull : (1ull << t);
-    collapse_kernel<<<grid_for(ngroups, kThreads * 4), kThreads, 0, stream>>>(state, ngroups, (1ull << t) - 1, zero_bit);
+    collapse_kernel<V><<<grid_for(ngroups, kThreads * 4), kThreads, 0, stream>>>(state, ngroups, (1ull << t) - 1, zero_bit);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
 
-int launch_zsums(const double2 *state, int n, double *partials, double *sums, cudaStream_t stream)
+template <typename R>
+int launch_zsums(const typename Cx<R>::T *state, int n, double *partials, double *sums, cudaStream_t stream)
 {
+    typedef typename Cx<R>::T V;
     const int nsums = n + 1;
     if (n < kZMinBits)
     {
-        zsums_small_kernel<<<1, 1, 0, stream>>>(state, n, sums);
+        zsums_small_kernel<V><<<1, 1, 0, stream>>>(state, n, sums);
         QCSB_CUDA(cudaGetLastError());
         return 1;
     }
     // 2^gbits threads in total: at most 512 blocks of 256 threads.
     const int gbits = n < 17 ? n : 17;
     const int blocks = 1 << (gbits - 8);
-    zsums_kernel<<<blocks, kZThreads, 0, stream>>>(state, n, gbits, partials);
+    zsums_kernel<V><<<blocks, kZThreads, 0, stream>>>(state, n, gbits, partials);
     QCSB_CUDA(cudaGetLastError());
     zsums_final_kernel<<<1, 64, 0, stream>>>(partials, blocks, nsums, sums);
     QCSB_CUDA(cudaGetLastError());
     return 2;
 }
 
-int launch_gather_logical(const double2 *state, int n, const int *l2p, uint64_t begin,
+template <typename R>
+int launch_gather_logical(const typename Cx<R>::T *state, int n, const int *l2p, uint64_t begin,
                           uint64_t count, double2 *out, cudaStream_t stream)
 {
-    gather_logical_kernel<<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, make_perm(n, l2p), begin, count, out);
+    gather_logical_kernel<typename Cx<R>::T><<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, make_perm(n, l2p), begin, count, out);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
 
-int launch_scatter_logical(double2 *state, int n, const int *l2p, uint64_t begin,
+template <typename R>
+int launch_scatter_logical(typename Cx<R>::T *state, int n, const int *l2p, uint64_t begin,
                            uint64_t count, const double2 *in, cudaStream_t stream)
 {
-    scatter_logical_kernel<<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, make_perm(n, l2p), begin, count, in);
+    scatter_logical_kernel<typename Cx<R>::T><<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, make_perm(n, l2p), begin, count, in);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
+
+template <typename R>
+int launch_widen(const typename Cx<R>::T *in, uint64_t count, double2 *out, cudaStream_t stream)
+{
+    widen_kernel<typename Cx<R>::T><<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(in, count, out);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+template <typename R>
+int launch_narrow(const double2 *in, uint64_t count, typename Cx<R>::T *out, cudaStream_t stream)
+{
+    narrow_kernel<typename Cx<R>::T><<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(in, count, out);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+#define QCSB_INSTANTIATE(R)                                                                                         \
+    template int launch_gate_plain<R>(Cx<R>::T *, int, const GateOp &, cudaStream_t);                               \
+    template int launch_init_zero<R>(Cx<R>::T *, int, cudaStream_t);                                                \
+    template int launch_init_flat<R>(Cx<R>::T *, int, cudaStream_t);                                                \
+    template int launch_init_sequential<R>(Cx<R>::T *, int, cudaStream_t);                                          \
+    template int launch_set_amplitude<R>(Cx<R>::T *, uint64_t, double, double, cudaStream_t);                      \
+    template int launch_measure_probs<R>(const Cx<R>::T *, int, int, uint64_t, uint64_t, double2 *, double2 *,      \
+                                         cudaStream_t);                                                             \
+    template int launch_collapse<R>(Cx<R>::T *, int, int, int, cudaStream_t);                                       \
+    template int launch_zsums<R>(const Cx<R>::T *, int, double *, double *, cudaStream_t);                          \
+    template int launch_gather_logical<R>(const Cx<R>::T *, int, const int *, uint64_t, uint64_t, double2 *,        \
+                                          cudaStream_t);                                                            \
+    template int launch_scatter_logical<R>(Cx<R>::T *, int, const int *, uint64_t, uint64_t, const double2 *,       \
+                                           cudaStream_t);                                                           \
+    template int launch_widen<R>(const Cx<R>::T *, uint64_t, double2 *, cudaStream_t);                              \
+    template int launch_narrow<R>(const double2 *, uint64_t, Cx<R>::T *, cudaStream_t);
+
+QCSB_INSTANTIATE(double)
+QCSB_INSTANTIATE(float)
 
 } // namespace qcsb

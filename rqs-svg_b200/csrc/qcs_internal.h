@@ -79,51 +79,79 @@ int gate_arity(const char *name);
 GateOp make_gate_op(const GateMatrix &g, const int *tq, uint64_t cmask, uint64_t cval);
 
 // ---------------------------------------------------------------- kernels
-// Every launch helper below enqueues on `stream` and returns the number of
-// kernels launched (for the launch counters).
+// Amplitudes are complex128 (R = double, the reference's type) or complex64
+// (R = float, a B200 extension). Gate arithmetic runs in R; every norm and
+// probability reduction accumulates in FP64. Every launch helper below
+// enqueues on `stream` and returns the number of kernels launched.
+template <typename R>
+struct Cx;
+template <>
+struct Cx<double>
+{
+    typedef double2 T;
+};
+template <>
+struct Cx<float>
+{
+    typedef float2 T;
+};
 
 // Plain path: one kernel applying one GateOp to the whole register.
-int launch_gate_plain(double2 *state, int n, const GateOp &op, cudaStream_t stream);
+template <typename R>
+int launch_gate_plain(typename Cx<R>::T *state, int n, const GateOp &op, cudaStream_t stream);
 
 // |0..0>, flat (all 1), sequential (a[i] = i), and "entangled" (a[0] = 1,
 // leaving the rest as is) state preparation.
-int launch_init_zero(double2 *state, int n, cudaStream_t stream);
-int launch_init_flat(double2 *state, int n, cudaStream_t stream);
-int launch_init_sequential(double2 *state, int n, cudaStream_t stream);
-int launch_set_amplitude(double2 *state, uint64_t index, double re, double im, cudaStream_t stream);
+template <typename R>
+int launch_init_zero(typename Cx<R>::T *state, int n, cudaStream_t stream);
+template <typename R>
+int launch_init_flat(typename Cx<R>::T *state, int n, cudaStream_t stream);
+template <typename R>
+int launch_init_sequential(typename Cx<R>::T *state, int n, cudaStream_t stream);
+template <typename R>
+int launch_set_amplitude(typename Cx<R>::T *state, uint64_t index, double re, double im, cudaStream_t stream);
 
 // Squared-norm sums (P0, P1) of target qubit t over the subspace where
 // (index & cmask) == cval. partials must hold kReduceBlocks double2;
 // result receives one double2 on the device.
 constexpr int kReduceBlocks = 592;   // 4 x 148 SMs
-int launch_measure_probs(const double2 *state, int n, int t, uint64_t cmask, uint64_t cval,
+template <typename R>
+int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t cmask, uint64_t cval,
                          double2 *partials, double2 *result, cudaStream_t stream);
 
 // Zero every amplitude whose bit t differs from keep_value.
-int launch_collapse(double2 *state, int n, int t, int keep_value, cudaStream_t stream);
+template <typename R>
+int launch_collapse(typename Cx<R>::T *state, int n, int t, int keep_value, cudaStream_t stream);
 
 // sums[0] = sum |a|^2, sums[1 + q] = sum over amplitudes with bit q set of
 // |a|^2 (physical qubits q = 0..n-1). partials must hold
-// kReduceBlocks * (n + 1) doubles; sums receives n + 1 doubles.
-int launch_zsums(const double2 *state, int n, double *partials, double *sums, cudaStream_t stream);
+// 512 * (n + 1) doubles; sums receives n + 1 doubles.
+template <typename R>
+int launch_zsums(const typename Cx<R>::T *state, int n, double *partials, double *sums, cudaStream_t stream);
+inline int launch_zsums(const double2 *state, int n, double *partials, double *sums, cudaStream_t stream)
+{
+    return launch_zsums<double>(state, n, partials, sums, stream);
+}
 
-// Gather the register into logical order: out[l] = state[phys(l)], where
-// phys(l) deposits logical bit j of l at physical bit l2p[j]; for indices
-// [begin, begin + count). l2p lives in device-readable memory (kernel arg).
-int launch_gather_logical(const double2 *state, int n, const int *l2p, uint64_t begin,
+// Gather the register into logical order as complex128: out[l] =
+// state[phys(l)], where phys(l) deposits logical bit j of l at physical bit
+// l2p[j]; for indices [begin, begin + count). Scatter is the inverse.
+template <typename R>
+int launch_gather_logical(const typename Cx<R>::T *state, int n, const int *l2p, uint64_t begin,
                           uint64_t count, double2 *out, cudaStream_t stream);
-int launch_scatter_logical(double2 *state, int n, const int *l2p, uint64_t begin,
+template <typename R>
+int launch_scatter_logical(typename Cx<R>::T *state, int n, const int *l2p, uint64_t begin,
                            uint64_t count, const double2 *in, cudaStream_t stream);
+// Same-precision conversions for identity-mapped transfers.
+template <typename R>
+int launch_widen(const typename Cx<R>::T *in, uint64_t count, double2 *out, cudaStream_t stream);
+template <typename R>
+int launch_narrow(const double2 *in, uint64_t count, typename Cx<R>::T *out, cudaStream_t stream);
 
 // Shot sampler (chain rule over physical qubits in the order given by
 // order[0..n)). See sampler.cu for the data layout.
-struct SamplerWorkspace
-{
-    double *tree = nullptr;      // 2^(s+1) doubles
-    double2 *unused = nullptr;
-    size_t tree_bytes = 0;
-};
-int launch_sampler(const double2 *state, int n, const int *order, uint32_t num_shots,
+template <typename R>
+int launch_sampler(const typename Cx<R>::T *state, int n, const int *order, uint32_t num_shots,
                    const double *uniforms, uint64_t *out_bits, double *tree, int split,
                    cudaStream_t stream);
 size_t sampler_tree_bytes(int n, int *split_out);

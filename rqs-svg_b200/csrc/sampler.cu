@@ -43,7 +43,8 @@ __device__ __forceinline__ uint64_t deposit_steps(uint64_t v, const OrderParams 
     return idx;
 }
 
-__global__ void __launch_bounds__(kThreads) leaf_sums_kernel(const double2 *state, OrderParams op, double *leaves)
+template <typename V>
+__global__ void __launch_bounds__(kThreads) leaf_sums_kernel(const V *state, OrderParams op, double *leaves)
 {
     const uint64_t nleaves = 1ull << op.s;
     const uint64_t nh = 1ull << (op.n - op.s);
@@ -57,8 +58,9 @@ __global__ void __launch_bounds__(kThreads) leaf_sums_kernel(const double2 *stat
         for (uint64_t h = 0; h < nh; ++h)
         {
             const uint64_t idx = identity ? (base | (h << op.s)) : (base | deposit_steps(h, op, op.s, op.n - op.s));
-            const double2 a = __ldcs(state + idx);
-            acc = fma(a.x, a.x, fma(a.y, a.y, acc));
+            const V a = __ldcs(state + idx);
+            const double x = a.x, y = a.y;
+            acc = fma(x, x, fma(y, y, acc));
         }
         leaves[r] = acc;
     }
@@ -74,7 +76,8 @@ __global__ void tree_level_kernel(double *tree, int d)
         parent[p] = child[p] + child[p + size];
 }
 
-__global__ void __launch_bounds__(kThreads) shots_kernel(const double2 *state, OrderParams op, const double *tree,
+template <typename V>
+__global__ void __launch_bounds__(kThreads) shots_kernel(const V *state, OrderParams op, const double *tree,
                                                          uint32_t num_shots, const double *uniforms, uint64_t *out_bits)
 {
     __shared__ double local[2 << kMaxLocalBits];
@@ -112,8 +115,9 @@ __global__ void __launch_bounds__(kThreads) shots_kernel(const double2 *state, O
             {
                 const uint64_t idx = identity ? (base | ((uint64_t)h << op.s))
                                               : (base | deposit_steps((uint64_t)h, op, op.s, m_bits));
-                const double2 a = state[idx];
-                local[m + h] = fma(a.x, a.x, a.y * a.y);
+                const V a = state[idx];
+                const double x = a.x, y = a.y;
+                local[m + h] = fma(x, x, y * y);
             }
             __syncthreads();
             for (int e = m_bits - 1; e >= 0; --e)
@@ -162,10 +166,12 @@ size_t sampler_tree_bytes(int n, int *split_out)
     return sizeof(double) * (2ull << s);
 }
 
-int launch_sampler(const double2 *state, int n, const int *order, uint32_t num_shots,
+template <typename R>
+int launch_sampler(const typename Cx<R>::T *state, int n, const int *order, uint32_t num_shots,
                    const double *uniforms, uint64_t *out_bits, double *tree, int split,
                    cudaStream_t stream)
 {
+    typedef typename Cx<R>::T V;
     OrderParams op;
     op.n = n;
     op.s = split;
@@ -176,7 +182,7 @@ int launch_sampler(const double2 *state, int n, const int *order, uint32_t num_s
     unsigned grid = static_cast<unsigned>((nleaves + kThreads - 1) / kThreads);
     if (grid > 148 * 16)
         grid = 148 * 16;
-    leaf_sums_kernel<<<grid, kThreads, 0, stream>>>(state, op, tree + nleaves);
+    leaf_sums_kernel<V><<<grid, kThreads, 0, stream>>>(state, op, tree + nleaves);
     QCSB_CUDA(cudaGetLastError());
     ++launches;
     for (int d = split - 1; d >= 0; --d)
@@ -192,11 +198,16 @@ int launch_sampler(const double2 *state, int n, const int *order, uint32_t num_s
     if (num_shots > 0)
     {
         unsigned g = num_shots < 148u * 8u ? num_shots : 148u * 8u;
-        shots_kernel<<<g, kThreads, 0, stream>>>(state, op, tree, num_shots, uniforms, out_bits);
+        shots_kernel<V><<<g, kThreads, 0, stream>>>(state, op, tree, num_shots, uniforms, out_bits);
         QCSB_CUDA(cudaGetLastError());
         ++launches;
     }
     return launches;
 }
+
+template int launch_sampler<double>(const double2 *, int, const int *, uint32_t, const double *, uint64_t *, double *,
+                                    int, cudaStream_t);
+template int launch_sampler<float>(const float2 *, int, const int *, uint32_t, const double *, uint64_t *, double *,
+                                   int, cudaStream_t);
 
 } // namespace qcsb

@@ -22,6 +22,11 @@
 
 #include <curand.h>
 
+// Run a templated launch helper on the register in its precision.
+#define QCSB_ON_STATE(fn, ...)                                                   \
+    (c64() ? fn<float>(static_cast<float2 *>(state_), __VA_ARGS__)             \
+           : fn<double>(static_cast<double2 *>(state_), __VA_ARGS__))
+
 namespace qcsb
 {
 namespace
@@ -76,6 +81,15 @@ void Simulator::set_seed(uint32_t seed)
     engine_ = std::mt19937_64(seed);
 }
 
+void Simulator::set_precision(int amplitude_bits)
+{
+    if (amplitude_bits != 128 && amplitude_bits != 64)
+        throw std::runtime_error(strformat("precision %d is not 128 (complex128) or 64 (complex64)", amplitude_bits));
+    if (allocated())
+        throw std::runtime_error("set_precision: memory is already allocated");
+    amp_bytes_ = amplitude_bits / 8;
+}
+
 void Simulator::set_fusion(int mode)
 {
     if (mode < QCS_FUSION_PLAIN || mode > QCS_FUSION_LEARNED)
@@ -113,13 +127,13 @@ void Simulator::allocate_memory()
     QCSB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t usable = free_b > kScratchReserve ? free_b - kScratchReserve : 0;
     int max_n = 0;
-    while (max_n < 62 && (sizeof(double2) << (max_n + 1)) <= usable)
+    while (max_n < 62 && ((size_t)amp_bytes_ << (max_n + 1)) <= usable)
         ++max_n;
     if (max_n > kMaxQubits)
         max_n = kMaxQubits;
     if (n > max_n)
         throw std::runtime_error(strformat("num_qubits(%d) > max_num_qubits_local_device(%d) + log_num_procs(0)", n, max_n));
-    QCSB_CUDA(cudaMalloc(&state_, sizeof(double2) << n));
+    QCSB_CUDA(cudaMalloc(&state_, (size_t)amp_bytes_ << n));
     n_ = n;
     perm_p2l_.assign(n, 0);
     perm_l2p_.assign(n, 0);
@@ -341,12 +355,12 @@ void Simulator::apply_gate(const char *name, const double *params, int nparams,
         return;
     }
     ++stats.gates_applied;
-    stats.algorithmic_bytes += 2.0 * sizeof(double2) * op.changed_amps(n_);
+    stats.algorithmic_bytes += 2.0 * amp_bytes_ * op.changed_amps(n_);
     if (fusion_mode_ == QCS_FUSION_PLAIN)
     {
         if (timer.enabled)
-            timer.begin(stream_, KernelTimer::kPlain, 2.0 * sizeof(double2) * op.changed_amps(n_));
-        const int k = launch_gate_plain(state_, n_, op, stream_);
+            timer.begin(stream_, KernelTimer::kPlain, 2.0 * amp_bytes_ * op.changed_amps(n_));
+        const int k = QCSB_ON_STATE(launch_gate_plain, n_, op, stream_);
         if (timer.enabled)
             timer.end(stream_);
         stats.kernel_launches += k;
@@ -362,7 +376,7 @@ void Simulator::flush()
 {
     if (pending_.empty() || state_ == nullptr)
         return;
-    const int k = fused_->run(state_, n_, pending_, fusion_mode_, stats, timer);
+    const int k = fused_->run(state_, n_, amp_bytes_, pending_, fusion_mode_, stats, timer);
     stats.kernel_launches += k;
     pending_.clear();
 }
@@ -393,7 +407,7 @@ int Simulator::measure(int q)
         cval |= 1ull << perm_l2p_[m];
     }
     const int t = perm_l2p_[q];
-    stats.kernel_launches += launch_measure_probs(state_, n_, t, cmask, cval, red_partials_, red_result_, stream_);
+    stats.kernel_launches += QCSB_ON_STATE(launch_measure_probs, n_, t, cmask, cval, red_partials_, red_result_, stream_);
     double2 *h = static_cast<double2 *>(host_pinned_);
     QCSB_CUDA(cudaMemcpyAsync(h, red_result_, sizeof(double2), cudaMemcpyDeviceToHost, stream_));
     QCSB_CUDA(cudaStreamSynchronize(stream_));
@@ -403,7 +417,7 @@ int Simulator::measure(int q)
     const double r = dist(engine_);
     const int result = p0 < r;
     (result ? measured1_ : measured0_).push_back(q);
-    stats.kernel_launches += launch_collapse(state_, n_, t, result, stream_);
+    stats.kernel_launches += QCSB_ON_STATE(launch_collapse, n_, t, result, stream_);
     return result;
 }
 
@@ -436,7 +450,7 @@ void Simulator::set_zero_state()
     discard_pending();
     clear_measurement_state();
     restore_reference_layout();
-    stats.kernel_launches += launch_init_zero(state_, n_, stream_);
+    stats.kernel_launches += QCSB_ON_STATE(launch_init_zero, n_, stream_);
 }
 
 void Simulator::set_flat_state()
@@ -445,7 +459,7 @@ void Simulator::set_flat_state()
     discard_pending();
     clear_measurement_state();
     restore_reference_layout();
-    stats.kernel_launches += launch_init_flat(state_, n_, stream_);
+    stats.kernel_launches += QCSB_ON_STATE(launch_init_flat, n_, stream_);
 }
 
 void Simulator::set_sequential_state()
@@ -453,7 +467,7 @@ void Simulator::set_sequential_state()
     require_allocated("set_sequential_state");
     discard_pending();
     clear_measurement_state();
-    stats.kernel_launches += launch_init_sequential(state_, n_, stream_);
+    stats.kernel_launches += QCSB_ON_STATE(launch_init_sequential, n_, stream_);
 }
 
 void Simulator::set_entangled_state()
@@ -463,7 +477,7 @@ void Simulator::set_entangled_state()
     require_allocated("set_entangled_state");
     flush();
     clear_measurement_state();
-    stats.kernel_launches += launch_set_amplitude(state_, 0, 1.0, 0.0, stream_);
+    stats.kernel_launches += QCSB_ON_STATE(launch_set_amplitude, 0, 1.0, 0.0, stream_);
 }
 
 void Simulator::set_random_state()
@@ -480,7 +494,8 @@ void Simulator::set_random_state()
     if (st == CURAND_STATUS_SUCCESS)
         st = curandSetPseudoRandomGeneratorSeed(gen, seed_);
     if (st == CURAND_STATUS_SUCCESS)
-        st = curandGenerateNormalDouble(gen, reinterpret_cast<double *>(state_), 2ull << n_, 0.0, 1.0);
+        st = c64() ? curandGenerateNormal(gen, static_cast<float *>(state_), 2ull << n_, 0.0f, 1.0f)
+                   : curandGenerateNormalDouble(gen, static_cast<double *>(state_), 2ull << n_, 0.0, 1.0);
     curandDestroyGenerator(gen);
     if (st != CURAND_STATUS_SUCCESS)
         throw std::runtime_error(strformat("cuRAND failed with status %d", (int)st));
@@ -503,19 +518,13 @@ void Simulator::logical_transfer(double *host, uint64_t count, bool to_host)
     (void)count;
     ensure_staging();
     const uint64_t total = 1ull << n_;
-    const bool ident = identity_mapping();
     for (uint64_t begin = 0; begin < total; begin += staging_count_)
     {
         const uint64_t cnt = std::min<uint64_t>(staging_count_, total - begin);
         const size_t bytes = sizeof(double2) * cnt;
         if (to_host)
         {
-            const double2 *src = state_ + begin;
-            if (!ident)
-            {
-                stats.kernel_launches += launch_gather_logical(state_, n_, perm_l2p_.data(), begin, cnt, staging_dev_, stream_);
-                src = staging_dev_;
-            }
+            const double2 *src = stage_chunk_out(begin, cnt);
             QCSB_CUDA(cudaMemcpyAsync(staging_host_, src, bytes, cudaMemcpyDeviceToHost, stream_));
             QCSB_CUDA(cudaStreamSynchronize(stream_));
             std::memcpy(host + 2 * begin, staging_host_, bytes);
@@ -523,13 +532,34 @@ void Simulator::logical_transfer(double *host, uint64_t count, bool to_host)
         else
         {
             std::memcpy(staging_host_, host + 2 * begin, bytes);
-            double2 *dst = ident ? state_ + begin : staging_dev_;
+            const bool direct = !c64() && identity_mapping();
+            double2 *dst = direct ? static_cast<double2 *>(state_) + begin : staging_dev_;
             QCSB_CUDA(cudaMemcpyAsync(dst, staging_host_, bytes, cudaMemcpyHostToDevice, stream_));
-            if (!ident)
-                stats.kernel_launches += launch_scatter_logical(state_, n_, perm_l2p_.data(), begin, cnt, staging_dev_, stream_);
+            if (!direct)
+            {
+                if (identity_mapping())
+                    stats.kernel_launches += launch_narrow<float>(staging_dev_, cnt, static_cast<float2 *>(state_) + begin, stream_);
+                else
+                    stats.kernel_launches += QCSB_ON_STATE(launch_scatter_logical, n_, perm_l2p_.data(), begin, cnt, staging_dev_, stream_);
+            }
             QCSB_CUDA(cudaStreamSynchronize(stream_));
         }
     }
+}
+
+// Device pointer to logical amplitudes [begin, begin + cnt) as complex128:
+// the register itself when it is complex128 in logical order, else the
+// staging buffer filled by a gather or widening kernel.
+const double2 *Simulator::stage_chunk_out(uint64_t begin, uint64_t cnt)
+{
+    const bool ident = identity_mapping();
+    if (!c64() && ident)
+        return static_cast<const double2 *>(state_) + begin;
+    if (ident)
+        stats.kernel_launches += launch_widen<float>(static_cast<const float2 *>(state_) + begin, cnt, staging_dev_, stream_);
+    else
+        stats.kernel_launches += QCSB_ON_STATE(launch_gather_logical, n_, perm_l2p_.data(), begin, cnt, staging_dev_, stream_);
+    return staging_dev_;
 }
 
 void Simulator::save_statevector(const char *path)
@@ -545,16 +575,10 @@ void Simulator::save_statevector(const char *path)
         throw std::runtime_error("open failed");
     ensure_staging();
     const uint64_t total = 1ull << n_;
-    const bool ident = identity_mapping();
     for (uint64_t begin = 0; begin < total; begin += staging_count_)
     {
         const uint64_t cnt = std::min<uint64_t>(staging_count_, total - begin);
-        const double2 *src = state_ + begin;
-        if (!ident)
-        {
-            stats.kernel_launches += launch_gather_logical(state_, n_, perm_l2p_.data(), begin, cnt, staging_dev_, stream_);
-            src = staging_dev_;
-        }
+        const double2 *src = stage_chunk_out(begin, cnt);
         QCSB_CUDA(cudaMemcpyAsync(staging_host_, src, sizeof(double2) * cnt, cudaMemcpyDeviceToHost, stream_));
         QCSB_CUDA(cudaStreamSynchronize(stream_));
         if (std::fwrite(staging_host_, sizeof(double2), cnt, fp) != cnt)
@@ -599,7 +623,7 @@ void Simulator::expectation_z(double *out, double *norm)
     if (out == nullptr)
         throw std::runtime_error("expectation_z: output pointer must not be NULL");
     flush();
-    stats.kernel_launches += launch_zsums(state_, n_, zsum_partials_, zsum_result_, stream_);
+    stats.kernel_launches += QCSB_ON_STATE(launch_zsums, n_, zsum_partials_, zsum_result_, stream_);
     double *h = static_cast<double *>(host_pinned_);
     QCSB_CUDA(cudaMemcpyAsync(h, zsum_result_, sizeof(double) * (n_ + 1), cudaMemcpyDeviceToHost, stream_));
     QCSB_CUDA(cudaStreamSynchronize(stream_));
@@ -645,7 +669,7 @@ void Simulator::sample(uint32_t num_shots, uint64_t *out)
     QCSB_CUDA(cudaMallocAsync(&u_dev, sizeof(double) * std::max<size_t>(nu, 1), stream_));
     QCSB_CUDA(cudaMallocAsync(&bits_dev, sizeof(uint64_t) * std::max<uint32_t>(num_shots, 1), stream_));
     QCSB_CUDA(cudaMemcpyAsync(u_dev, u, sizeof(double) * nu, cudaMemcpyHostToDevice, stream_));
-    stats.kernel_launches += launch_sampler(state_, n_, perm_l2p_.data(), num_shots, u_dev, bits_dev, tree, split, stream_);
+    stats.kernel_launches += QCSB_ON_STATE(launch_sampler, n_, perm_l2p_.data(), num_shots, u_dev, bits_dev, tree, split, stream_);
     QCSB_CUDA(cudaStreamSynchronize(stream_));   // the pinned buffer is reused below
     QCSB_CUDA(cudaMemcpyAsync(host_pinned_, bits_dev, sizeof(uint64_t) * num_shots, cudaMemcpyDeviceToHost, stream_));
     QCSB_CUDA(cudaFreeAsync(tree, stream_));

@@ -78,6 +78,8 @@ class Simulator
     void reinitialize_mapping();
 
     void set_seed(uint32_t seed);
+    void set_precision(int amplitude_bits);
+    int precision() const { return amp_bytes_ * 8; }
     void set_fusion(int mode);
     int fusion() const { return fusion_mode_; }
 
@@ -122,6 +124,7 @@ class Simulator
     bool identity_mapping() const;
     void ensure_staging();
     void logical_transfer(double *host, uint64_t count, bool to_host);
+    const double2 *stage_chunk_out(uint64_t begin, uint64_t cnt);
     void discard_pending() { pending_.clear(); }
     void restore_reference_layout();
 
@@ -129,7 +132,9 @@ class Simulator
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
     int n_ = 0;
-    double2 *state_ = nullptr;
+    void *state_ = nullptr;
+    int amp_bytes_ = 16;   // 16: complex128 (the reference's), 8: complex64
+    bool c64() const { return amp_bytes_ == 8; }
 
     std::vector<int> perm_p2l_, perm_l2p_, initial_perm_p2l_;
     // logical -> physical map the reference would hold (it differs from ours
@@ -166,7 +171,8 @@ class FusedExecutor
   public:
     explicit FusedExecutor(cudaStream_t stream);
     ~FusedExecutor();
-    int run(double2 *state, int n, const std::vector<GateOp> &ops, int mode, qcs_b200_stats &stats, KernelTimer &timer);
+    int run(void *state, int n, int amp_bytes, const std::vector<GateOp> &ops, int mode, qcs_b200_stats &stats,
+            KernelTimer &timer);
 
     // Planner knobs: 0 keeps the default (64 gates per pass, 11 local qubits).
     void set_options(int max_ops, int local_bits)

@@ -145,6 +145,8 @@ class Library:
             "qcs_simulator_get_kernel_times": [_P, ctypes.POINTER(KernelTimes)],
             "qcs_b200_zsums_noalloc": [_P, ctypes.c_int, _P, _P],
             "qcs_simulator_set_planner_options": [_P, ctypes.c_int, ctypes.c_int],
+            "qcs_simulator_set_precision": [_P, ctypes.c_int],
+            "qcs_simulator_get_precision": [_P, ctypes.POINTER(ctypes.c_int)],
             "qcs_simulator_get_pass_records": [_P, _FP, _FP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)],
             "qcs_b200_cost_model_create": [ctypes.POINTER(_P), ctypes.c_uint32],
             "qcs_b200_cost_model_destroy": [_P],
@@ -186,12 +188,15 @@ class Simulator:
     """A qcs_simulator handle: create, configure, allocate, run, destroy."""
 
     def __init__(self, lib: Library, num_qubits: int, num_clbits: int = 0, mapping=None,
-                 seed: int | None = None, fusion: int | None = None, allocate: bool = True):
+                 seed: int | None = None, fusion: int | None = None, allocate: bool = True,
+                 precision: int | None = None):
         self.lib = lib
         self.n = num_qubits
         self.h = _P()
         lib.call("qcs_simulator_create", ctypes.byref(self.h))
         lib.call("qcs_simulator_set_num_qubits", self.h, num_qubits)
+        if precision is not None:
+            lib.call("qcs_simulator_set_precision", self.h, precision)
         if num_clbits:
             lib.call("qcs_simulator_set_num_clbits", self.h, num_clbits)
         if mapping is not None:
