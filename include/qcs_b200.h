@@ -98,6 +98,24 @@ int qcs_simulator_expectation_z(qcs_simulator *sim, double *expectations, double
 int qcs_simulator_sample(qcs_simulator *sim, uint32_t num_shots, uint64_t *bitstrings);
 
 /*
+ * Read single amplitudes: amplitudes[2k], amplitudes[2k+1] receive the real
+ * and imaginary part of the amplitude at LOGICAL index indices[k] (the index
+ * save_statevector would write it at, src/qcs.cu:2494-2543), as complex128.
+ * Indices must be below 2^n. For spot checks of registers too large to copy.
+ */
+int qcs_simulator_get_amplitudes(qcs_simulator *sim, const uint64_t *indices, uint64_t count, double *amplitudes);
+
+/*
+ * Compare two registers of the same size on the same device, either
+ * precision: <a|b> = sum over logical indices i of conj(a_i) b_i, max_i
+ * |a_i - b_i|, and the squared norms <a|a>, <b|b> (FP64 accumulation, one
+ * read of each register). Any output pointer may be NULL. The fidelity of the
+ * two states is |<a|b>|^2 / (<a|a> <b|b>).
+ */
+int qcs_simulator_compare(qcs_simulator *a, qcs_simulator *b, double *overlap_re, double *overlap_im,
+                          double *max_abs_diff, double *norm_a, double *norm_b);
+
+/*
  * Counters since creation (or the last reset_stats): kernels launched by the
  * library, gates received, passes executed by the fused path, and the
  * algorithmic bytes of the gates (2 * bytes_per_amplitude * amplitudes each
@@ -146,8 +164,10 @@ int qcs_simulator_set_planner_options(qcs_simulator *sim, int max_gates_per_pass
 
 /*
  * Pass timings recorded while kernel timing is enabled: for each fused pass
- * its features (4 floats: local qubits, highest local physical qubit, gate
- * count, bytes per amplitude) and its device time in milliseconds. Reading
+ * its features (4 floats: local qubits; arithmetic ops, which run complex
+ * multiply-adds on every amplitude; light ops, diagonal phases and
+ * permutations such as X, CX, SWAP; bytes per amplitude) and its device time
+ * in milliseconds. The features do not depend on the register size. Reading
  * synchronizes, returns up to capacity records in *count and clears them.
  */
 int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *milliseconds, uint32_t capacity,
@@ -188,6 +208,64 @@ int qcs_simulator_set_cost_model(qcs_simulator *sim, qcs_b200_cost_model *model)
    greedy) and the device times the judge holds for that gate queue (ms, -1
    when not measured yet). */
 int qcs_simulator_get_planner_judge(qcs_simulator *sim, int *learned_plan, double *greedy_ms, double *learned_ms);
+
+/*
+ * Batches: many independent circuits, each on its own register, run together
+ * from |0..0>. Circuits with the same gates on the same qubits (parameters
+ * may differ) share one plan of fused passes, and each pass runs over all of
+ * them in one launch; the whole run (gate entries in, passes, <Z> of every
+ * register, results out) is one CUDA graph, replayed on later runs. The first
+ * run tunes the number of local qubits of each shared plan by timing the
+ * candidates. The reference has no batch API: a batch replaces a host loop
+ * of create / allocate_memory / gate calls / destroy per circuit.
+ *
+ * A gate is given by its qcs API name and parameters; its qubits are the
+ * targets, then the negative controls, then the positive controls. Gates on
+ * at most two targets (any number of controls) are supported; measurements
+ * are not. Registers hold 9 to 30 qubits.
+ */
+typedef struct qcs_b200_batch qcs_b200_batch;
+
+typedef struct qcs_b200_gate
+{
+    char name[16];          /* "u3", "ry", "rz", "x", "swap", "p", ... (NUL-terminated) */
+    double params[4];       /* the gate's parameters in the API's order; the rest ignored */
+    int16_t num_targets;
+    int16_t num_negctrls;
+    int16_t num_ctrls;
+    int16_t reserved;       /* 0 */
+    int16_t qubits[12];
+} qcs_b200_gate;
+
+typedef struct qcs_b200_batch_info
+{
+    uint32_t circuits;
+    uint32_t groups;            /* distinct gate structures, one shared plan each */
+    uint32_t passes;            /* fused passes over all groups */
+    uint32_t launches_per_run;  /* kernels one run launches */
+    uint64_t amplitudes;        /* over all registers */
+    uint64_t parameters;        /* gate parameters over all circuits */
+    double pass_bytes;          /* bytes the passes move per run: 2 x bytes/amplitude x 2^n per pass and register
+                                   (the first pass of a register writes only) */
+    double last_run_ms;         /* device time of the last run */
+} qcs_b200_batch_info;
+
+/* amplitude_bits: 128 (complex128) or 64 (complex64). */
+int qcs_b200_batch_create(qcs_b200_batch **batch, int amplitude_bits);
+int qcs_b200_batch_destroy(qcs_b200_batch *batch);
+/* Append a circuit on num_qubits; *index (may be NULL) receives its position. */
+int qcs_b200_batch_add_circuit(qcs_b200_batch *batch, int num_qubits, const qcs_b200_gate *gates,
+                               uint32_t num_gates, uint32_t *index);
+/* Replace every gate parameter, circuit by circuit and gate by gate in the
+   order given, keeping the gates: count must equal info.parameters. */
+int qcs_b200_batch_set_parameters(qcs_b200_batch *batch, const double *params, uint64_t count);
+/* Run every circuit from |0..0> and compute <Z_q> of every register. */
+int qcs_b200_batch_run(qcs_b200_batch *batch);
+/* <Z_q> of the last run, circuit by circuit (num_qubits values each). */
+int qcs_b200_batch_expectation_z(qcs_b200_batch *batch, double *expectations, uint64_t count);
+/* The register of one circuit after the last run (2 * 2^n doubles). */
+int qcs_b200_batch_get_statevector(qcs_b200_batch *batch, uint32_t index, double *amplitudes, uint64_t count);
+int qcs_b200_batch_get_info(qcs_b200_batch *batch, qcs_b200_batch_info *info);
 
 /*
  * Allocation-free squared-norm sums of a complex128 state vector held in the

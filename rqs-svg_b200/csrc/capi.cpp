@@ -7,6 +7,7 @@
 
 #include "qcs.h"
 #include "qcs_b200.h"
+#include "batch.h"
 #include "cost_model.h"
 #include "simulator.h"
 
@@ -710,4 +711,103 @@ extern "C" int qcs_simulator_set_precision(qcs_simulator *sim, int amplitude_bit
 extern "C" int qcs_simulator_get_precision(const qcs_simulator *sim, int *amplitude_bits)
 {
     return guarded([&] { write_result(amplitude_bits, core(sim).precision()); });
+}
+
+extern "C" int qcs_simulator_get_amplitudes(qcs_simulator *sim, const uint64_t *indices, uint64_t count, double *amplitudes)
+{
+    return guarded([&] { core(sim).get_amplitudes(indices, count, amplitudes); });
+}
+
+extern "C" int qcs_simulator_compare(qcs_simulator *a, qcs_simulator *b, double *overlap_re, double *overlap_im,
+                                     double *max_abs_diff, double *norm_a, double *norm_b)
+{
+    return guarded([&] {
+        qcsb::Simulator::compare(core(a), core(b), overlap_re, overlap_im, max_abs_diff, norm_a, norm_b);
+    });
+}
+
+// ------------------------------------------------------------------ batches
+
+struct qcs_b200_batch
+{
+    qcsb::Batch *b = nullptr;
+};
+
+namespace
+{
+qcsb::Batch &batch_of(qcs_b200_batch *batch)
+{
+    if (batch == nullptr || batch->b == nullptr)
+        throw std::runtime_error("batch handle is NULL");
+    return *batch->b;
+}
+} // namespace
+
+extern "C" int qcs_b200_batch_create(qcs_b200_batch **batch, int amplitude_bits)
+{
+    return guarded([&] {
+        if (batch == nullptr)
+            throw std::runtime_error("result pointer must not be NULL");
+        auto *h = new qcs_b200_batch();
+        try
+        {
+            h->b = new qcsb::Batch(amplitude_bits);
+        }
+        catch (...)
+        {
+            delete h;
+            throw;
+        }
+        *batch = h;
+    });
+}
+
+extern "C" int qcs_b200_batch_destroy(qcs_b200_batch *batch)
+{
+    return guarded([&] {
+        if (batch == nullptr)
+            throw std::runtime_error("batch handle is NULL");
+        delete batch->b;
+        delete batch;
+    });
+}
+
+extern "C" int qcs_b200_batch_add_circuit(qcs_b200_batch *batch, int num_qubits, const qcs_b200_gate *gates,
+                                          uint32_t num_gates, uint32_t *index)
+{
+    return guarded([&] {
+        const uint32_t i = batch_of(batch).add_circuit(num_qubits, gates, num_gates);
+        if (index)
+            *index = i;
+    });
+}
+
+extern "C" int qcs_b200_batch_set_parameters(qcs_b200_batch *batch, const double *params, uint64_t count)
+{
+    return guarded([&] { batch_of(batch).set_parameters(params, count); });
+}
+
+extern "C" int qcs_b200_batch_run(qcs_b200_batch *batch)
+{
+    return guarded([&] { batch_of(batch).run(); });
+}
+
+extern "C" int qcs_b200_batch_expectation_z(qcs_b200_batch *batch, double *expectations, uint64_t count)
+{
+    return guarded([&] { batch_of(batch).expectation_z(expectations, count); });
+}
+
+extern "C" int qcs_b200_batch_get_statevector(qcs_b200_batch *batch, uint32_t index, double *amplitudes,
+                                              uint64_t count)
+{
+    return guarded([&] { batch_of(batch).get_statevector(index, amplitudes, count); });
+}
+
+extern "C" int qcs_b200_batch_get_info(qcs_b200_batch *batch, qcs_b200_batch_info *info)
+{
+    return guarded([&] {
+        if (info == nullptr)
+            throw std::runtime_error("result pointer must not be NULL");
+        batch_of(batch).info(info);
+    });
 }

@@ -2,8 +2,8 @@
 // ReLU activations, trained on the GPU by the kernels below (forward,
 // backward, Adam) on pass timings the simulator records itself.
 //
-// Inputs (per pass): block width (local qubits k), log2 of the largest local
-// stride (highest local physical qubit), gate count, bytes per amplitude.
+// Inputs (per pass): block width (local qubits k), arithmetic ops, light ops
+// (diagonal phases and permutations), bytes per amplitude.
 // Target: log(device time per amplitude in ns). Inputs and target are
 // standardised with the training set's mean and deviation.
 //

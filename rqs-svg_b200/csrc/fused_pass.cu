@@ -21,6 +21,8 @@
 // all dependencies, so the result equals the gate-by-gate result up to the
 // rounding of each individual product.
 
+#include "fused_pass.h"
+
 #include "cost_model.h"
 #include "simulator.h"
 
@@ -31,58 +33,6 @@ namespace qcsb
 {
 namespace
 {
-
-constexpr int kFusedMaxOps = 64;
-constexpr int kFusedMaxStages = 64;
-constexpr int kLowBits = 3;      // qubits 0..2 are always local: 128-byte runs
-constexpr int kStageBits = 4;    // amplitudes per thread in a stage: 2^4
-constexpr int kDefaultLocal = 11;
-constexpr int kMaxLocal = 12;
-constexpr size_t kPlanWindow = 4096;   // ops scanned past the first pending one
-
-enum FKind : uint8_t
-{
-    F_DENSE1 = 0,  // 2x2 on one stage bit
-    F_SWAP1 = 1,   // X: exchange the pair
-    F_DENSE2 = 2,  // 4x4 on two stage bits (b0 < b1)
-    F_SWAP2 = 3,   // exchange sub-indices 01 and 10
-    F_PHASE = 4,   // multiply by m[0] where the condition bits match
-    F_DIAG = 5,    // diagonal on one or two targets anywhere
-};
-
-// One gate of a pass. Conditions: (local index & lcmask) == lcval and
-// (physical chunk bits & gcmask) == gcval. For F_PHASE the condition includes
-// the target bits of the single changed sub-index.
-struct FOp
-{
-    uint8_t kind;
-    uint8_t nt;
-    uint8_t b0, b1;         // stage-bit positions (dense kinds)
-    int8_t loc[2];          // F_DIAG: local bit of target i, -1 when outside Q
-    uint8_t phys[2];        // F_DIAG: physical qubit of target i
-    uint32_t lcmask, lcval;
-    uint64_t gcmask, gcval;
-    double2 m[16];
-};
-
-struct FStage
-{
-    uint8_t sbits[kStageBits];   // local bit positions of the stage, ascending
-    uint16_t op_begin, op_end;
-};
-
-struct FPassParams
-{
-    void *state;
-    int n;
-    int k;
-    uint64_t chunks;
-    uint64_t qmasks[kMaxLocal];  // (1 << qphys[i]) - 1, ascending: chunk deposit
-    uint64_t qbit[kMaxLocal];    // 1 << qphys[i]
-    int nstages;
-    FStage stages[kFusedMaxStages];
-    FOp ops[kFusedMaxOps];
-};
 
 // Shared-memory swizzle, an XOR of higher index bits into the bits that pick
 // the bank group: 16-byte amplitudes (8 per 128-byte line) fold 3 bits,
@@ -144,10 +94,24 @@ constexpr int R = 1 << kStageBits;
 // local controls take the unconditional path; controlled ones predicate each
 // pair or amplitude on (jr & lcmask) == lcval.
 
-template <typename V, int B>
-__device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+// Where an op's matrix entries come from: the pass parameters (one register)
+// or the register's block of the entry buffer (batched passes).
+struct PoolEntries
 {
-    const V m00 = cvt<V>(op.m[0]), m01 = cvt<V>(op.m[1]), m10 = cvt<V>(op.m[2]), m11 = cvt<V>(op.m[3]);
+    const FPassParams &p;
+    uint32_t off;
+    __device__ __forceinline__ double2 operator[](int i) const { return p.entries[off + i]; }
+};
+struct BufferEntries
+{
+    const double2 *m;
+    __device__ __forceinline__ double2 operator[](int i) const { return __ldg(m + i); }
+};
+
+template <typename V, int B, typename M>
+__device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &e, const uint32_t (&jr)[R])
+{
+    const V m00 = cvt<V>(e[0]), m01 = cvt<V>(e[1]), m10 = cvt<V>(e[2]), m11 = cvt<V>(e[3]);
     const uint32_t cm = op.lcmask, cv = op.lcval;
     if (cm == 0)
     {
@@ -211,8 +175,8 @@ __device__ __forceinline__ void apply_swap1(V (&a)[R], const FOp &op, const uint
     }
 }
 
-template <typename V, int B0, int B1>
-__device__ __forceinline__ void apply_dense2(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V, int B0, int B1, typename M>
+__device__ __forceinline__ void apply_dense2(V (&a)[R], const FOp &op, const M &m, const uint32_t (&jr)[R])
 {
     const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
@@ -224,7 +188,6 @@ __device__ __forceinline__ void apply_dense2(V (&a)[R], const FOp &op, const uin
             continue;
         const int i1 = r | (1 << B0), i2 = r | (1 << B1), i3 = r | (1 << B0) | (1 << B1);
         const V x0 = a[r], x1 = a[i1], x2 = a[i2], x3 = a[i3];
-        const double2 *m = op.m;
         const V y0 = cmad2(cvt<V>(m[0]), x0, cvt<V>(m[1]), x1), t0 = cmad2(cvt<V>(m[2]), x2, cvt<V>(m[3]), x3);
         const V y1 = cmad2(cvt<V>(m[4]), x0, cvt<V>(m[5]), x1), t1 = cmad2(cvt<V>(m[6]), x2, cvt<V>(m[7]), x3);
         const V y2 = cmad2(cvt<V>(m[8]), x0, cvt<V>(m[9]), x1), t2 = cmad2(cvt<V>(m[10]), x2, cvt<V>(m[11]), x3);
@@ -255,10 +218,10 @@ __device__ __forceinline__ void apply_swap2(V (&a)[R], const FOp &op, const uint
     }
 }
 
-template <typename V>
-__device__ __forceinline__ void apply_phase(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V, typename M>
+__device__ __forceinline__ void apply_phase(V (&a)[R], const FOp &op, const M &m, const uint32_t (&jr)[R])
 {
-    const V e = cvt<V>(op.m[0]);
+    const V e = cvt<V>(m[0]);
     const uint32_t cm = op.lcmask, cv = op.lcval;
 #pragma unroll
     for (int r = 0; r < R; ++r)
@@ -266,12 +229,13 @@ __device__ __forceinline__ void apply_phase(V (&a)[R], const FOp &op, const uint
             a[r] = cmul(e, a[r]);
 }
 
-template <typename V>
-__device__ __forceinline__ void apply_diag(V (&a)[R], const FOp &op, const uint32_t (&jr)[R], uint64_t cbase)
+template <typename V, typename M>
+__device__ __forceinline__ void apply_diag(V (&a)[R], const FOp &op, const M &m, const uint32_t (&jr)[R],
+                                           uint64_t cbase)
 {
     // one or two targets: entries in registers, chosen per amplitude by its
     // target bits (from the local index, or from the chunk when not local)
-    const V d0 = cvt<V>(op.m[0]), d1 = cvt<V>(op.m[1]), d2 = cvt<V>(op.m[2]), d3 = cvt<V>(op.m[3]);
+    const V d0 = cvt<V>(m[0]), d1 = cvt<V>(m[1]), d2 = cvt<V>(m[2]), d3 = cvt<V>(m[3]);
     const uint32_t cm = op.lcmask, cv = op.lcval;
     const int l0 = op.loc[0], l1 = op.nt > 1 ? op.loc[1] : -1;
     const uint32_t c0 = l0 < 0 ? static_cast<uint32_t>((cbase >> op.phys[0]) & 1ull) : 0u;
@@ -292,15 +256,15 @@ __device__ __forceinline__ void apply_diag(V (&a)[R], const FOp &op, const uint3
     }
 }
 
-template <typename V>
-__device__ __forceinline__ void dispatch_dense1(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V, typename M>
+__device__ __forceinline__ void dispatch_dense1(V (&a)[R], const FOp &op, const M &e, const uint32_t (&jr)[R])
 {
     switch (op.b0)
     {
-    case 0: apply_dense1<V, 0>(a, op, jr); break;
-    case 1: apply_dense1<V, 1>(a, op, jr); break;
-    case 2: apply_dense1<V, 2>(a, op, jr); break;
-    default: apply_dense1<V, 3>(a, op, jr); break;
+    case 0: apply_dense1<V, 0>(a, op, e, jr); break;
+    case 1: apply_dense1<V, 1>(a, op, e, jr); break;
+    case 2: apply_dense1<V, 2>(a, op, e, jr); break;
+    default: apply_dense1<V, 3>(a, op, e, jr); break;
     }
 }
 
@@ -317,17 +281,17 @@ __device__ __forceinline__ void dispatch_swap1(V (&a)[R], const FOp &op, const u
 }
 
 // (b0, b1) with b0 < b1 encoded as b0 * 4 + b1
-template <typename V>
-__device__ __forceinline__ void dispatch_dense2(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+template <typename V, typename M>
+__device__ __forceinline__ void dispatch_dense2(V (&a)[R], const FOp &op, const M &e, const uint32_t (&jr)[R])
 {
     switch (op.b0 * 4 + op.b1)
     {
-    case 1: apply_dense2<V, 0, 1>(a, op, jr); break;
-    case 2: apply_dense2<V, 0, 2>(a, op, jr); break;
-    case 3: apply_dense2<V, 0, 3>(a, op, jr); break;
-    case 6: apply_dense2<V, 1, 2>(a, op, jr); break;
-    case 7: apply_dense2<V, 1, 3>(a, op, jr); break;
-    default: apply_dense2<V, 2, 3>(a, op, jr); break;
+    case 1: apply_dense2<V, 0, 1>(a, op, e, jr); break;
+    case 2: apply_dense2<V, 0, 2>(a, op, e, jr); break;
+    case 3: apply_dense2<V, 0, 3>(a, op, e, jr); break;
+    case 6: apply_dense2<V, 1, 2>(a, op, e, jr); break;
+    case 7: apply_dense2<V, 1, 3>(a, op, e, jr); break;
+    default: apply_dense2<V, 2, 3>(a, op, e, jr); break;
     }
 }
 
@@ -345,19 +309,91 @@ __device__ __forceinline__ void dispatch_swap2(V (&a)[R], const FOp &op, const u
     }
 }
 
+template <typename V, typename M>
+__device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, const uint32_t (&jr)[R], uint64_t cbase)
+{
+    switch (op.kind)
+    {
+    case F_DENSE1: dispatch_dense1<V>(a, op, e, jr); break;
+    case F_SWAP1: dispatch_swap1<V>(a, op, jr); break;
+    case F_DENSE2: dispatch_dense2<V>(a, op, e, jr); break;
+    case F_SWAP2: dispatch_swap2<V>(a, op, jr); break;
+    case F_PHASE: apply_phase<V>(a, op, e, jr); break;
+    default: apply_diag<V>(a, op, e, jr, cbase); break;
+    }
+}
+
+// A phase stage: a run of diagonal gates applied as one factor per
+// amplitude. Every diagonal gate multiplies the amplitudes whose bits match a
+// pattern by a unit-modulus entry d. Split the pattern into the stage bits
+// (which pick one of the thread's 16 amplitudes r) and the rest (fixed for the
+// thread: its other local bits and the chunk). On the stage bits,
+// [pattern matches r] expands by inclusion-exclusion into signed monomials
+// prod_{b in m} r_b, so d^[match] = prod over terms (d or conj d)^(monomial m
+// of r). The host emits one term (m, conjugate?, thread/chunk condition,
+// entry) per expansion member; the thread multiplies the terms that hold for
+// it into E[m], then amplitude r gets prod_{m subset of r} E[m] (a
+// subset-product transform, 32 complex products), whatever the number of
+// gates in the run.
+template <typename V, typename M>
+__device__ __forceinline__ void phase_stage(V *sb, const uint32_t (&pos)[R], uint32_t j0, uint64_t cbase,
+                                            const FOp *terms, int nterms, const M &entry_at)
+{
+    V E[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m)
+    {
+        E[m].x = 1;
+        E[m].y = 0;
+    }
+    for (int i = 0; i < nterms; ++i)
+    {
+        const FOp &t = terms[i];
+        if ((j0 & t.lcmask) != t.lcval || (cbase & t.gcmask) != t.gcval)
+            continue;
+        V d = cvt<V>(entry_at(t.moff));
+        if (t.b1)
+            d.y = -d.y;
+        switch (t.b0)
+        {
+#define QCSB_TERM(m)                                                                                               \
+    case m: E[m] = cmul(d, E[m]); break;
+            QCSB_TERM(0) QCSB_TERM(1) QCSB_TERM(2) QCSB_TERM(3) QCSB_TERM(4) QCSB_TERM(5) QCSB_TERM(6) QCSB_TERM(7)
+            QCSB_TERM(8) QCSB_TERM(9) QCSB_TERM(10) QCSB_TERM(11) QCSB_TERM(12) QCSB_TERM(13) QCSB_TERM(14)
+            QCSB_TERM(15)
+#undef QCSB_TERM
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < kStageBits; ++b)
+    {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if ((r >> b) & 1)
+                E[r] = cmul(E[r ^ (1 << b)], E[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        sb[pos[r]] = cmul(E[r], sb[pos[r]]);
+}
+
 // One CTA per chunk at a time; blockDim.x == 2^(k - kStageBits) <= 128, so
 // that three CTAs (12 warps, 3 x 64 KB of double-buffered chunks) share an SM.
-template <typename Real>
-__global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_kernel(const __grid_constant__ FPassParams p)
+// BATCH: the work items are the chunks of many registers of the same size
+// and plan (see FPassParams), each with its own gate entries.
+template <typename Real, bool BATCH>
+__global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
+    fused_pass_kernel(const __grid_constant__ FPassParams p)
 {
     typedef typename Cx<Real>::T V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *smem = reinterpret_cast<V *>(smem_raw);
-    V *state = static_cast<V *>(p.state);
+    V *const state = static_cast<V *>(p.state);
     const int k = p.k;
     const int T = 1 << (k - kStageBits);
     const int tid = threadIdx.x;
     const int chunk_elems = 1 << k;
+    const int cbits = p.n - k;   // log2(chunks of one register)
 
     // global offset of this thread's element tid + m*T, m < R
     uint64_t dep_tid = 0;
@@ -370,7 +406,7 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_ker
         hb[b] = p.qbit[k - kStageBits + b];
 
     auto chunk_base = [&](uint64_t c) -> uint64_t {
-        uint64_t g = c;
+        uint64_t g = BATCH ? (c & ((1ull << cbits) - 1)) : c;
         for (int i = 0; i < k; ++i)
         {
             const uint64_t lo = g & p.qmasks[i];
@@ -378,6 +414,7 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_ker
         }
         return g;
     };
+    auto reg_of = [&](uint64_t c) -> uint64_t { return BATCH ? (c >> cbits) : 0ull; };
     auto elem_offset = [&](int m) -> uint64_t {
         uint64_t off = dep_tid;
 #pragma unroll
@@ -388,9 +425,23 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_ker
     };
     auto issue_load = [&](uint64_t c, V *dst) {
         const uint64_t cb = chunk_base(c);
+        if (p.from_zero)
+        {
+            // |0..0>: the chunk holding index 0 starts with a one
 #pragma unroll
-        for (int m = 0; m < R; ++m)
-            cp_async_amp<V>(dst + swz<V>(tid + m * T), state + (cb | elem_offset(m)));
+            for (int m = 0; m < R; ++m)
+            {
+                const bool one = cb == 0 && m == 0 && tid == 0;
+                dst[swz<V>(tid + m * T)] = one ? V{1, 0} : V{0, 0};
+            }
+        }
+        else
+        {
+            const V *src = state + (reg_of(c) << p.n);
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+                cp_async_amp<V>(dst + swz<V>(tid + m * T), src + (cb | elem_offset(m)));
+        }
         cp_async_commit();
     };
 
@@ -414,6 +465,8 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_ker
         }
         __syncthreads();
         const uint64_t cbase = chunk_base(c);
+        const uint64_t reg = reg_of(c);
+        const double2 *entries = BATCH ? p.mats + reg * p.mat_stride : nullptr;
 
         for (int st = 0; st < p.nstages; ++st)
         {
@@ -436,7 +489,6 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_ker
             }
             const uint32_t p0 = static_cast<uint32_t>(swz<V>(static_cast<int>(j0)));
             uint32_t jr[R], pos[R];
-            V a[R];
 #pragma unroll
             for (int r = 0; r < R; ++r)
             {
@@ -450,22 +502,31 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_ker
                     }
                 jr[r] = j;
                 pos[r] = q;
-                a[r] = sb[q];
             }
+            if (S.kind == 1)
+            {
+                if (BATCH)
+                    phase_stage<V>(sb, pos, j0, cbase, p.ops + S.op_begin, S.op_end - S.op_begin,
+                                   [&](int off) { return __ldg(entries + off); });
+                else
+                    phase_stage<V>(sb, pos, j0, cbase, p.ops + S.op_begin, S.op_end - S.op_begin,
+                                   [&](int off) { return p.entries[off]; });
+                __syncthreads();
+                continue;
+            }
+            V a[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                a[r] = sb[pos[r]];
             for (int oi = S.op_begin; oi < S.op_end; ++oi)
             {
                 const FOp &op = p.ops[oi];
                 if ((cbase & op.gcmask) != op.gcval)
                     continue;
-                switch (op.kind)
-                {
-                case F_DENSE1: dispatch_dense1<V>(a, op, jr); break;
-                case F_SWAP1: dispatch_swap1<V>(a, op, jr); break;
-                case F_DENSE2: dispatch_dense2<V>(a, op, jr); break;
-                case F_SWAP2: dispatch_swap2<V>(a, op, jr); break;
-                case F_PHASE: apply_phase<V>(a, op, jr); break;
-                default: apply_diag<V>(a, op, jr, cbase); break;
-                }
+                if (BATCH)
+                    apply_op<V>(a, op, BufferEntries{entries + op.moff}, jr, cbase);
+                else
+                    apply_op<V>(a, op, PoolEntries{p, op.moff}, jr, cbase);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r)
@@ -473,23 +534,18 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4) fused_pass_ker
             __syncthreads();
         }
 
-        const uint64_t cb = cbase;
+        V *const dst = state + (reg << p.n);
 #pragma unroll
         for (int m = 0; m < R; ++m)
-            __stcs(state + (cb | elem_offset(m)), sb[swz<V>(tid + m * T)]);
+            __stcs(dst + (cbase | elem_offset(m)), sb[swz<V>(tid + m * T)]);
         __syncthreads();
         cur ^= 1;
     }
 }
 
-// ------------------------------------------------------------ planning
+} // namespace
 
-struct OpClass
-{
-    bool fusable;
-    uint64_t dense;   // qubits the op is non-diagonal on (dense targets)
-    uint64_t diag;    // qubits the op is diagonal on (controls, diag targets)
-};
+// ------------------------------------------------------------ planning
 
 OpClass classify(const GateOp &op)
 {
@@ -533,6 +589,15 @@ bool is_perm(const GateOp &op, int size)
 bool is_x(const GateOp &op) { return op.nt == 1 && is_perm(op, 2); }
 bool is_swap(const GateOp &op) { return op.nt == 2 && op.act[0] == 1 && op.act[1] == 2 && is_perm(op, 2); }
 
+int op_entry_count(const GateOp &op)
+{
+    if (op.diag)
+        return op.na == 1 ? 1 : 4;
+    if (op.nt == 1)
+        return is_x(op) ? 0 : 4;
+    return is_swap(op) ? 0 : 16;
+}
+
 // Full 2^nt x 2^nt matrix of a dense GateOp (row-major).
 void expand_dense(const GateOp &op, double2 *out)
 {
@@ -544,20 +609,6 @@ void expand_dense(const GateOp &op, double2 *out)
         for (int b = 0; b < op.na; ++b)
             out[op.act[a] * d + op.act[b]] = make_double2(op.mat[a * op.na + b].re, op.mat[a * op.na + b].im);
 }
-
-struct PlannedPass
-{
-    std::vector<int> ops;   // indices into the queue, in execution order
-    uint64_t local = 0;     // physical qubits of Q
-    int k = 0;              // |Q|
-};
-
-struct Segment
-{
-    bool fused;
-    int plain_op;           // when !fused
-    PlannedPass pass;
-};
 
 // Greedy pass construction. Ops are taken in queue order; an op joins the
 // current pass when its dense targets fit in Q (k qubits) and it commutes
@@ -594,6 +645,7 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
         s.plain_op = -1;
         uint64_t local = low_mask;
         uint64_t blocked_all = 0, blocked_dense = 0;
+        int entries = 0;
         const size_t window_end = std::min(N, first + kPlanWindow);
         for (size_t i = first; i < window_end; ++i)
         {
@@ -601,7 +653,8 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
                 continue;
             const OpClass &c = cls[i];
             const uint64_t support = c.dense | c.diag;
-            bool take = c.fusable && (int)s.pass.ops.size() < max_ops &&
+            const int ec = c.fusable ? op_entry_count(q[i]) : 0;
+            bool take = c.fusable && (int)s.pass.ops.size() < max_ops && entries + ec <= kFusedMaxEntries &&
                         (c.dense & blocked_all) == 0 && (c.diag & blocked_dense) == 0;
             if (take)
             {
@@ -615,6 +668,7 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
             {
                 s.pass.ops.push_back((int)i);
                 done[i] = true;
+                entries += ec;
             }
             else
             {
@@ -688,9 +742,121 @@ void schedule_stages(const std::vector<GateOp> &q, const PlannedPass &pp, const 
     }
 }
 
+// Unitary diagonal gates on at most two targets join phase runs. A run is
+// applied as one phase stage when its weight reaches phase_run_min() (tuning
+// knob QCS_PHASE_RUN_MIN, default 6): a one-entry phase (CZ, CP, T, ...)
+// weighs 1, a diagonal with two or four entries (RZ, RZZ) 2, the ratio of
+// their costs as single ops. A phase stage has a fixed cost of about six
+// one-entry phases (the 16-way subset products), measured on B200.
+int phase_run_min()
+{
+    static const int v = [] {
+        const char *e = std::getenv("QCS_PHASE_RUN_MIN");
+        const int x = (e && e[0]) ? std::atoi(e) : 6;
+        return x >= 2 ? x : 2;
+    }();
+    return v;
+}
+
+int phase_weight(const GateOp &op) { return op.na == 1 ? 1 : 2; }
+
+bool phase_run_op(const GateOp &op)
+{
+    if (!op.diag || op.nt > 2)
+        return false;
+    // the expansion divides by entries (conjugates them): unit modulus only,
+    // which excludes the zeroing ops of collapsed measurements
+    for (int a = 0; a < op.na; ++a)
+        if (std::fabs(op.mat[a].re * op.mat[a].re + op.mat[a].im * op.mat[a].im - 1.0) > 1e-12)
+            return false;
+    return true;
+}
+
+// Within one stage, move each diagonal op later past the non-diagonal ops it
+// commutes with, so that diagonal ops gather into runs (order among the
+// diagonal ops, and every non-commuting pair, is kept).
+std::vector<int> cluster_diagonals(const std::vector<GateOp> &q, const PlannedPass &pp, const std::vector<int> &ops)
+{
+    std::vector<int> out, held;
+    out.reserve(ops.size());
+    for (int oi : ops)
+    {
+        const GateOp &op = q[pp.ops[oi]];
+        if (phase_run_op(op))
+        {
+            held.push_back(oi);
+            continue;
+        }
+        const OpClass c = classify(op);
+        bool passes = true;
+        for (int h : held)
+            if (!commute(classify(q[pp.ops[h]]), c))
+            {
+                passes = false;
+                break;
+            }
+        if (!passes)
+        {
+            out.insert(out.end(), held.begin(), held.end());
+            held.clear();
+        }
+        out.push_back(oi);
+    }
+    out.insert(out.end(), held.begin(), held.end());
+    return out;
+}
+
+int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m)
+{
+    switch (f.kind)
+    {
+    case F_TERM:
+        // the entry of active sub-index phys[0]
+        m[0] = make_double2(op.mat[f.phys[0]].re, op.mat[f.phys[0]].im);
+        return 1;
+    case F_PHASE:
+        m[0] = make_double2(op.mat[0].re, op.mat[0].im);
+        return 1;
+    case F_DIAG:
+        for (int s = 0; s < 4; ++s)
+            m[s] = make_double2(1.0, 0.0);
+        for (int a = 0; a < op.na; ++a)
+            m[op.act[a]] = make_double2(op.mat[a].re, op.mat[a].im);
+        if (op.nt < 2)
+        {
+            // second target absent: entries 2, 3 repeat 0, 1
+            m[2] = m[0];
+            m[3] = m[1];
+        }
+        return 4;
+    case F_DENSE1:
+    {
+        double2 full[4];
+        expand_dense(op, full);
+        for (int i = 0; i < 4; ++i)
+            m[i] = full[i];
+        return 4;
+    }
+    case F_DENSE2:
+    {
+        double2 full[16];
+        expand_dense(op, full);
+        // exchanged targets: the two sub-index bits swap roles
+        auto sw = [&](int v) { return swapped ? (((v & 1) << 1) | ((v >> 1) & 1)) : v; };
+        for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c)
+                m[r * 4 + c] = full[sw(r) * 4 + sw(c)];
+        return 16;
+    }
+    default:
+        return 0;
+    }
+}
+
 // Fill the kernel parameters of a pass. Returns false when the pass does not
 // fit the parameter block limits.
-bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm)
+bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
+                  std::vector<FOpSource> *src)
 {
     std::memset(&prm, 0, sizeof(prm));
     prm.n = n;
@@ -718,31 +884,125 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
     schedule_stages(q, pp, loc_of, stage_ops, stage_bits);
     if (stage_ops.size() > (size_t)kFusedMaxStages)
         return false;
-    prm.nstages = (int)stage_ops.size();
-    int nops = 0;
+    int nops = 0, nentries = 0, ns = 0;
     for (size_t si = 0; si < stage_ops.size(); ++si)
     {
         // stage bits: the needed ones, padded with the lowest other local bits
         uint32_t bits = stage_bits[si];
         for (int l = 0; l < k && __builtin_popcount(bits) < kStageBits; ++l)
             bits |= 1u << l;
-        FStage &S = prm.stages[si];
+        uint8_t sbits[kStageBits];
         int pos_in_stage[kMaxLocal];
         int nb = 0;
         for (int l = 0; l < k; ++l)
             if ((bits >> l) & 1)
             {
                 pos_in_stage[l] = nb;
-                S.sbits[nb++] = static_cast<uint8_t>(l);
+                sbits[nb++] = static_cast<uint8_t>(l);
             }
-        S.op_begin = static_cast<uint16_t>(nops);
-        for (int oi : stage_ops[si])
+        // the scheduled stage becomes register stages split by phase stages
+        auto open_stage = [&](uint8_t kind) -> FStage * {
+            if (ns >= kFusedMaxStages)
+                return nullptr;
+            FStage &S = prm.stages[ns++];
+            std::memset(&S, 0, sizeof(S));
+            std::memcpy(S.sbits, sbits, sizeof(sbits));
+            S.kind = kind;
+            S.op_begin = static_cast<uint16_t>(nops);
+            return &S;
+        };
+        FStage *cur = nullptr;
+        const std::vector<int> sops = cluster_diagonals(q, pp, stage_ops[si]);
+        size_t idx = 0;
+        while (idx < sops.size())
         {
+            size_t run_end = idx;
+            int weight = 0;
+            while (run_end < sops.size() && phase_run_op(q[pp.ops[sops[run_end]]]))
+                weight += phase_weight(q[pp.ops[sops[run_end++]]]);
+            if (weight >= phase_run_min())
+            {
+                // a phase stage: one term per inclusion-exclusion member
+                if (cur)
+                {
+                    cur->op_end = static_cast<uint16_t>(nops);
+                    cur = nullptr;
+                }
+                FStage *ph = open_stage(1);
+                if (ph == nullptr)
+                    return false;
+                for (size_t ri = idx; ri < run_end; ++ri)
+                {
+                    const GateOp &op = q[pp.ops[sops[ri]]];
+                    for (int a = 0; a < op.na; ++a)
+                    {
+                        uint64_t cm = op.cmask, cv = op.cval;
+                        for (int i = 0; i < op.nt; ++i)
+                        {
+                            cm |= 1ull << op.tq[i];
+                            if ((op.act[a] >> i) & 1)
+                                cv |= 1ull << op.tq[i];
+                        }
+                        uint32_t s1 = 0, s0 = 0, lcm = 0, lcv = 0;
+                        uint64_t gcm = 0, gcv = 0;
+                        for (int b = 0; b < n; ++b)
+                        {
+                            if (!((cm >> b) & 1))
+                                continue;
+                            const bool v = (cv >> b) & 1;
+                            const int l = loc_of[b];
+                            if (l >= 0 && ((bits >> l) & 1))
+                                (v ? s1 : s0) |= 1u << pos_in_stage[l];
+                            else if (l >= 0)
+                            {
+                                lcm |= 1u << l;
+                                lcv |= v ? 1u << l : 0u;
+                            }
+                            else
+                            {
+                                gcm |= 1ull << b;
+                                gcv |= v ? 1ull << b : 0ull;
+                            }
+                        }
+                        for (uint32_t A = s0;; A = (A - 1) & s0)
+                        {
+                            if (nops >= kFusedMaxOps || nentries + 1 > kFusedMaxEntries)
+                                return false;
+                            FOp &t = prm.ops[nops++];
+                            std::memset(&t, 0, sizeof(t));
+                            t.kind = F_TERM;
+                            t.b0 = static_cast<uint8_t>(s1 | A);
+                            t.b1 = static_cast<uint8_t>(__builtin_popcount(A) & 1);
+                            t.phys[0] = static_cast<uint8_t>(a);
+                            t.lcmask = lcm;
+                            t.lcval = lcv;
+                            t.gcmask = gcm;
+                            t.gcval = gcv;
+                            t.moff = static_cast<uint16_t>(nentries);
+                            fop_entries(op, t, false, prm.entries + nentries);
+                            ++nentries;
+                            if (src)
+                                src->push_back({pp.ops[sops[ri]], false});
+                            if (A == 0)
+                                break;
+                        }
+                    }
+                }
+                ph->op_end = static_cast<uint16_t>(nops);
+                idx = run_end;
+                continue;
+            }
+            const int oi = sops[idx++];
             const GateOp &op = q[pp.ops[oi]];
+            if (nops >= kFusedMaxOps)
+                return false;
+            if (cur == nullptr && (cur = open_stage(0)) == nullptr)
+                return false;
             FOp &f = prm.ops[nops++];
             std::memset(&f, 0, sizeof(f));
             f.nt = static_cast<uint8_t>(op.nt);
             uint64_t cm = op.cmask, cv = op.cval;
+            bool swapped = false;
             if (op.diag && op.na == 1)
             {
                 // one changed sub-index: a phase on the amplitudes whose
@@ -754,15 +1014,10 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                     if ((op.act[0] >> i) & 1)
                         cv |= 1ull << op.tq[i];
                 }
-                f.m[0] = make_double2(op.mat[0].re, op.mat[0].im);
             }
             else if (op.diag)
             {
                 f.kind = F_DIAG;
-                for (int s = 0; s < 4; ++s)
-                    f.m[s] = make_double2(1.0, 0.0);
-                for (int a = 0; a < op.na; ++a)
-                    f.m[op.act[a]] = make_double2(op.mat[a].re, op.mat[a].im);
                 for (int i = 0; i < op.nt; ++i)
                 {
                     f.phys[i] = static_cast<uint8_t>(op.tq[i]);
@@ -770,9 +1025,6 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                 }
                 if (op.nt < 2)
                 {
-                    // second target absent: entries 2, 3 repeat 0, 1
-                    f.m[2] = f.m[0];
-                    f.m[3] = f.m[1];
                     f.loc[1] = -1;
                     f.phys[1] = 0;
                 }
@@ -781,32 +1033,30 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
             {
                 f.kind = is_x(op) ? F_SWAP1 : F_DENSE1;
                 f.b0 = static_cast<uint8_t>(pos_in_stage[loc_of[op.tq[0]]]);
-                expand_dense(op, f.m);
             }
             else
             {
                 f.kind = is_swap(op) ? F_SWAP2 : F_DENSE2;
                 int p0 = pos_in_stage[loc_of[op.tq[0]]];
                 int p1 = pos_in_stage[loc_of[op.tq[1]]];
-                double2 full[16];
-                expand_dense(op, full);
-                if (p0 < p1)
+                if (p0 > p1)
                 {
-                    for (int i = 0; i < 16; ++i)
-                        f.m[i] = full[i];
-                }
-                else
-                {
-                    // exchange the roles of the two targets: sub-index bits swap
-                    auto sw = [](int s) { return ((s & 1) << 1) | ((s >> 1) & 1); };
-                    for (int r = 0; r < 4; ++r)
-                        for (int c = 0; c < 4; ++c)
-                            f.m[r * 4 + c] = full[sw(r) * 4 + sw(c)];
                     std::swap(p0, p1);
+                    swapped = true;
                 }
                 f.b0 = static_cast<uint8_t>(p0);
                 f.b1 = static_cast<uint8_t>(p1);
             }
+            double2 m[16];
+            const int ne = fop_entries(op, f, swapped, m);
+            if (nentries + ne > kFusedMaxEntries)
+                return false;
+            f.moff = static_cast<uint16_t>(nentries);
+            for (int e = 0; e < ne; ++e)
+                prm.entries[nentries + e] = m[e];
+            nentries += ne;
+            if (src)
+                src->push_back({pp.ops[oi], swapped});
             uint32_t lcm = 0, lcv = 0;
             uint64_t gcm = 0, gcv = 0;
             for (int b = 0; b < n; ++b)
@@ -830,14 +1080,44 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
             f.lcval = lcv;
             f.gcmask = gcm;
             f.gcval = gcv;
-        }
-        S.op_end = static_cast<uint16_t>(nops);
+                }
+        if (cur)
+            cur->op_end = static_cast<uint16_t>(nops);
     }
+    prm.nstages = ns;
+    prm.nops = nops;
+    prm.nentries = nentries;
     return true;
 }
 
-template <typename R>
-int launch_fused_pass(void *state, int k, const FPassParams &prm, cudaStream_t stream)
+bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, std::vector<FPassParams> &params,
+                  std::vector<std::vector<FOpSource>> *srcs, std::vector<PlannedPass> *pieces)
+{
+    params.emplace_back();
+    std::vector<FOpSource> src;
+    if (build_params(q, pp, n, pp.k, params.back(), srcs ? &src : nullptr))
+    {
+        if (srcs)
+            srcs->push_back(std::move(src));
+        if (pieces)
+            pieces->push_back(pp);
+        return true;
+    }
+    params.pop_back();
+    if (pp.ops.size() <= 1)
+        return false;
+    const size_t half = pp.ops.size() / 2;
+    PlannedPass a = pp, b = pp;
+    a.ops.assign(pp.ops.begin(), pp.ops.begin() + half);
+    b.ops.assign(pp.ops.begin() + half, pp.ops.end());
+    return build_pieces(q, a, n, params, srcs, pieces) && build_pieces(q, b, n, params, srcs, pieces);
+}
+
+namespace
+{
+
+template <typename R, bool BATCH>
+int launch_pass_impl(void *state, int k, const FPassParams &prm, cudaStream_t stream)
 {
     typedef typename Cx<R>::T V;
     const int threads = 1 << (k - kStageBits);
@@ -847,13 +1127,13 @@ int launch_fused_pass(void *state, int k, const FPassParams &prm, cudaStream_t s
     QCSB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64 || !configured[dev])
     {
-        QCSB_CUDA(cudaFuncSetAttribute(fused_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        QCSB_CUDA(cudaFuncSetAttribute(fused_pass_kernel<R, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        2 * (int)sizeof(V) * (1 << kMaxLocal)));
         if (dev >= 0 && dev < 64)
             configured[dev] = true;
     }
     int per_sm = 0;
-    QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_pass_kernel<R>, threads, smem));
+    QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_pass_kernel<R, BATCH>, threads, smem));
     int sms = 148;
     QCSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     uint64_t grid = prm.chunks;
@@ -862,10 +1142,29 @@ int launch_fused_pass(void *state, int k, const FPassParams &prm, cudaStream_t s
         grid = cap;
     FPassParams &p = const_cast<FPassParams &>(prm);
     p.state = state;
-    fused_pass_kernel<R><<<static_cast<unsigned>(grid), threads, smem, stream>>>(p);
+    fused_pass_kernel<R, BATCH><<<static_cast<unsigned>(grid), threads, smem, stream>>>(p);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
+
+} // namespace
+
+template <typename R>
+int launch_fused_pass(void *state, int k, const FPassParams &prm, cudaStream_t stream)
+{
+    return launch_pass_impl<R, false>(state, k, prm, stream);
+}
+
+template <typename R>
+int launch_fused_batch(void *state, int k, const FPassParams &prm, cudaStream_t stream)
+{
+    return launch_pass_impl<R, true>(state, k, prm, stream);
+}
+
+template int launch_fused_pass<double>(void *, int, const FPassParams &, cudaStream_t);
+template int launch_fused_pass<float>(void *, int, const FPassParams &, cudaStream_t);
+template int launch_fused_batch<double>(void *, int, const FPassParams &, cudaStream_t);
+template int launch_fused_batch<float>(void *, int, const FPassParams &, cudaStream_t);
 
 int clamp_local_bits(int k, int n)
 {
@@ -891,18 +1190,29 @@ int choose_local_bits(int n, int option)
     return clamp_local_bits(k, n);
 }
 
-PassFeatures pass_features(const PlannedPass &pp, int n, int amp_bytes)
+// Permutations (X, SWAP and their controlled forms) and diagonal ops cost a
+// few instructions per amplitude; every other op runs complex multiply-adds.
+bool light_op(const GateOp &op) { return op.diag || is_x(op) || is_swap(op); }
+
+// Cost-model inputs of a pass: local qubits k, arithmetic (non-light) ops,
+// light ops, bytes per amplitude. None depends on the register size, so
+// timings recorded on small registers carry over to large ones.
+PassFeatures pass_features(int k, int heavy, int light, int amp_bytes)
 {
-    int top = 0;
-    for (int b = 0; b < n; ++b)
-        if ((pp.local >> b) & 1)
-            top = b;
     PassFeatures f;
-    f.f[0] = static_cast<float>(pp.k);
-    f.f[1] = static_cast<float>(top);
-    f.f[2] = static_cast<float>(pp.ops.size());
+    f.f[0] = static_cast<float>(k);
+    f.f[1] = static_cast<float>(heavy);
+    f.f[2] = static_cast<float>(light);
     f.f[3] = static_cast<float>(amp_bytes);
     return f;
+}
+
+PassFeatures pass_features(const std::vector<GateOp> &q, const PlannedPass &pp, int amp_bytes)
+{
+    int light = 0;
+    for (int oi : pp.ops)
+        light += light_op(q[oi]) ? 1 : 0;
+    return pass_features(pp.k, (int)pp.ops.size() - light, light, amp_bytes);
 }
 
 uint64_t fill_local(uint64_t local, int n, int k)
@@ -941,11 +1251,13 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
         while (gi < greedy.size() && greedy[gi].fused)
         {
             seq.insert(seq.end(), greedy[gi].pass.ops.begin(), greedy[gi].pass.ops.end());
-            greedy_feats.push_back(pass_features(greedy[gi].pass, n, amp_bytes));
+            greedy_feats.push_back(pass_features(q, greedy[gi].pass, amp_bytes));
             ++gi;
         }
         const int L = (int)seq.size();
         std::vector<uint64_t> dense(L);
+        std::vector<int> light_before(L + 1, 0);   // prefix counts of light ops
+        std::vector<int> entries_before(L + 1, 0); // and of gate entries
         for (int t = 0; t < L; ++t)
         {
             const GateOp &op = q[seq[t]];
@@ -954,6 +1266,8 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
                 for (int i = 0; i < op.nt; ++i)
                     d |= 1ull << op.tq[i];
             dense[t] = d;
+            light_before[t + 1] = light_before[t] + (light_op(op) ? 1 : 0);
+            entries_before[t + 1] = entries_before[t] + op_entry_count(op);
         }
         struct Cand
         {
@@ -969,16 +1283,13 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
             {
                 d |= dense[i];
                 const int need = __builtin_popcountll(d);
-                if (need > kmax)
+                if (need > kmax || entries_before[j] - entries_before[i] > kFusedMaxEntries)
                     break;
                 for (int k = std::max(need, kmin); k <= kmax; ++k)
                 {
-                    PlannedPass pp;
-                    pp.k = k;
-                    pp.local = fill_local(d, n, k);
-                    pp.ops.assign(j - i, 0);
-                    const PassFeatures f = pass_features(pp, n, amp_bytes);
-                    cands.push_back({i, j, k, pp.local});
+                    const int light = light_before[j] - light_before[i];
+                    const PassFeatures f = pass_features(k, j - i - light, light, amp_bytes);
+                    cands.push_back({i, j, k, fill_local(d, n, k)});
                     feats.insert(feats.end(), f.f, f.f + 4);
                 }
             }
@@ -1042,8 +1353,6 @@ uint64_t queue_signature(const std::vector<GateOp> &ops)
     mix(ops.size());
     return h;
 }
-
-} // namespace
 
 int fused_min_qubits() { return kStageBits + 5; }
 
@@ -1151,7 +1460,8 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         last_plan_learned = 0;
     }
 
-    FPassParams *prm = new FPassParams;
+    std::vector<FPassParams> params;
+    std::vector<PlannedPass> pieces;
     for (const Segment &s : segs)
     {
         if (!s.fused)
@@ -1159,26 +1469,28 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
             launches += plain(ops[s.plain_op]);
             continue;
         }
-        if (build_params(ops, s.pass, n, s.pass.k, *prm))
+        params.clear();
+        pieces.clear();
+        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces))
+        {
+            for (int oi : s.pass.ops)
+                launches += plain(ops[oi]);
+            continue;
+        }
+        for (size_t i = 0; i < params.size(); ++i)
         {
             if (timer.enabled)
             {
-                const PassFeatures f = pass_features(s.pass, n, amp_bytes);
+                const PassFeatures f = pass_features(ops, pieces[i], amp_bytes);
                 timer.begin(stream_, KernelTimer::kFused, 2.0 * amp_bytes * std::ldexp(1.0, n), &f);
             }
-            launches += c64 ? launch_fused_pass<float>(state, s.pass.k, *prm, stream_)
-                             : launch_fused_pass<double>(state, s.pass.k, *prm, stream_);
+            launches += c64 ? launch_fused_pass<float>(state, pieces[i].k, params[i], stream_)
+                             : launch_fused_pass<double>(state, pieces[i].k, params[i], stream_);
             if (timer.enabled)
                 timer.end(stream_);
             ++stats.fused_passes;
         }
-        else
-        {
-            for (int oi : s.pass.ops)
-                launches += plain(ops[oi]);
-        }
     }
-    delete prm;
     if (timed_flush)
         QCSB_CUDA(cudaEventRecord(judge_b_, stream_));
     return launches;

@@ -1,0 +1,142 @@
+// Fused passes: the data structures shared by the planner (host), the pass
+// kernel (device) and the batch executor. See fused_pass.cu for the
+// execution model.
+#pragma once
+
+#include "qcs_internal.h"
+
+#include <vector>
+
+namespace qcsb
+{
+
+constexpr int kFusedMaxOps = 256;       // ops of one pass
+constexpr int kFusedMaxEntries = 1024;  // gate entries (complex) of one pass
+constexpr int kFusedMaxStages = 96;
+constexpr int kLowBits = 3;      // qubits 0..2 are always local: 128-byte runs
+constexpr int kStageBits = 4;    // amplitudes per thread in a stage: 2^4
+constexpr int kDefaultLocal = 11;
+constexpr int kMaxLocal = 12;
+constexpr size_t kPlanWindow = 4096;   // ops scanned past the first pending one
+
+enum FKind : uint8_t
+{
+    F_DENSE1 = 0,  // 2x2 on one stage bit
+    F_SWAP1 = 1,   // X: exchange the pair
+    F_DENSE2 = 2,  // 4x4 on two stage bits (b0 < b1)
+    F_SWAP2 = 3,   // exchange sub-indices 01 and 10
+    F_PHASE = 4,   // multiply by entry 0 where the condition bits match
+    F_DIAG = 5,    // diagonal on one or two targets anywhere
+    F_TERM = 6,    // one factor of a phase stage (see fused_pass.cu)
+};
+
+// One gate of a pass. Conditions: (local index & lcmask) == lcval and
+// (physical chunk bits & gcmask) == gcval. For F_PHASE the condition includes
+// the target bits of the single changed sub-index. The op's matrix entries
+// start at moff: in the pass's entry pool, or, for a batched pass, in the
+// register's block of the entry buffer.
+struct FOp
+{
+    uint64_t gcmask, gcval;
+    uint32_t lcmask, lcval;
+    uint8_t kind;
+    uint8_t nt;
+    uint8_t b0, b1;         // stage-bit positions (dense kinds)
+    int8_t loc[2];          // F_DIAG: local bit of target i, -1 when outside Q
+    uint8_t phys[2];        // F_DIAG: physical qubit of target i
+    uint16_t moff;
+    uint16_t pad[3];
+};
+static_assert(sizeof(FOp) == 40, "FOp layout");
+
+// A stage applies ops [op_begin, op_end) on the amplitudes that differ in its
+// stage bits: a register stage (kind 0) runs the ops one by one on each
+// thread's 2^kStageBits amplitudes; a phase stage (kind 1) holds the F_TERM
+// factors of a run of diagonal gates.
+struct FStage
+{
+    uint8_t sbits[kStageBits];   // local bit positions of the stage, ascending
+    uint16_t op_begin, op_end;
+    uint8_t kind;
+    uint8_t pad[3];
+};
+
+// Kernel parameters of one pass (passed as a __grid_constant__ block, under
+// the 32 KiB kernel parameter limit).
+struct FPassParams
+{
+    void *state;
+    int n;
+    int k;
+    uint64_t chunks;             // work items: chunks of one register, or of all registers of a batch
+    uint64_t qmasks[kMaxLocal];  // (1 << qphys[i]) - 1, ascending: chunk deposit
+    uint64_t qbit[kMaxLocal];    // 1 << qphys[i]
+    int nstages;
+    int nops;
+    int nentries;
+    // batched passes: registers of 2^n amplitudes stored back to back; work
+    // item w is chunk w mod 2^(n-k) of register w >> (n-k); register r reads
+    // its gate entries at mats + r * mat_stride
+    const double2 *mats;
+    uint32_t mat_stride;
+    int from_zero;               // registers start as |0..0>: build chunks instead of loading them
+    FStage stages[kFusedMaxStages];
+    FOp ops[kFusedMaxOps];
+    double2 entries[kFusedMaxEntries];
+};
+static_assert(sizeof(FPassParams) <= 32764, "kernel parameter limit");
+
+struct OpClass
+{
+    bool fusable;
+    uint64_t dense;   // qubits the op is non-diagonal on (dense targets)
+    uint64_t diag;    // qubits the op is diagonal on (controls, diag targets)
+};
+
+struct PlannedPass
+{
+    std::vector<int> ops;   // indices into the queue, in execution order
+    uint64_t local = 0;     // physical qubits of Q
+    int k = 0;              // |Q|
+};
+
+struct Segment
+{
+    bool fused;
+    int plain_op;           // when !fused
+    PlannedPass pass;
+};
+
+// Which queued op an FOp came from, and whether its two targets were
+// exchanged to put them in stage-bit order.
+struct FOpSource
+{
+    int op;
+    bool swapped;
+};
+
+OpClass classify(const GateOp &op);
+std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int low, int max_ops);
+// Fill the kernel parameters of a pass (false when it does not fit the
+// parameter block); src, when given, receives one FOpSource per FOp.
+bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
+                  std::vector<FOpSource> *src = nullptr);
+// Entries an FOp of this kind reads (4 dense 1-target, 16 dense 2-target, 1
+// phase, 4 diagonal, 0 permutations), written to m from the GateOp.
+int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m);
+// Entries a queued op will need in a pass (the same counts, from the GateOp).
+int op_entry_count(const GateOp &op);
+// Kernel parameters of a planned pass, cut in two (in order, recursively)
+// while a piece does not fit one parameter block; every piece keeps the
+// pass's local qubits. False when a single op does not fit.
+bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, std::vector<FPassParams> &params,
+                  std::vector<std::vector<FOpSource>> *srcs = nullptr, std::vector<PlannedPass> *pieces = nullptr);
+int clamp_local_bits(int k, int n);
+int fused_min_qubits();
+
+template <typename R>
+int launch_fused_pass(void *state, int k, const FPassParams &prm, cudaStream_t stream);
+template <typename R>
+int launch_fused_batch(void *state, int k, const FPassParams &prm, cudaStream_t stream);
+
+} // namespace qcsb

@@ -83,6 +83,8 @@ const GateInfo &lookup(const char *name)
 
 int gate_arity(const char *name) { return lookup(name).nt; }
 
+int gate_nparams(const char *name) { return lookup(name).np; }
+
 GateMatrix gate_matrix(const char *name, const double *p, int np)
 {
     const GateInfo &gi = lookup(name);

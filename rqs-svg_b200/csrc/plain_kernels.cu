@@ -587,6 +587,59 @@ __global__ void narrow_kernel(const double2 *in, uint64_t count, V *out)
         out[k] = make_cx<V>(in[k].x, in[k].y);
 }
 
+template <typename V>
+__global__ void gather_indices_kernel(const V *state, const uint64_t *physical, uint64_t count, double2 *out)
+{
+    for (uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (uint64_t)gridDim.x * kThreads)
+    {
+        const V a = state[physical[k]];
+        out[k] = make_double2(a.x, a.y);
+    }
+}
+
+// Per block: sum of conj(x_i) * y_i (re, im), max |x_i - y_i|, sum |x_i|^2
+// and sum |y_i|^2, written as five doubles; a fixed grid and order make
+// repeated calls identical.
+__global__ void __launch_bounds__(kThreads) compare_kernel(const double2 *x, const double2 *y, uint64_t count,
+                                                           double *partials)
+{
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (uint64_t k = (uint64_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (uint64_t)gridDim.x * kThreads)
+    {
+        const double2 a = __ldcs(x + k), b = __ldcs(y + k);
+        v[0] += a.x * b.x + a.y * b.y;
+        v[1] += a.x * b.y - a.y * b.x;
+        const double dx = a.x - b.x, dy = a.y - b.y;
+        v[2] = fmax(v[2], sqrt(dx * dx + dy * dy));
+        v[3] += a.x * a.x + a.y * a.y;
+        v[4] += b.x * b.x + b.y * b.y;
+    }
+    __shared__ double sh[5][kThreads / 32];
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+    {
+        double t = v[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const double u = __shfl_xor_sync(0xffffffffu, t, o);
+            t = i == 2 ? fmax(t, u) : t + u;
+        }
+        if (l == 0)
+            sh[i][w] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5)
+    {
+        const int i = threadIdx.x;
+        double t = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k)
+            t = i == 2 ? fmax(t, sh[i][k]) : t + sh[i][k];
+        partials[5 * blockIdx.x + i] = t;
+    }
+}
+
 PermParams make_perm(int n, const int *l2p)
 {
     PermParams pp;
@@ -703,6 +756,22 @@ int launch_zsums(const typename Cx<R>::T *state, int n, double *partials, double
 }
 
 template <typename R>
+int launch_gather_indices(const typename Cx<R>::T *state, const uint64_t *physical, uint64_t count, double2 *out,
+                          cudaStream_t stream)
+{
+    gather_indices_kernel<typename Cx<R>::T><<<grid_for(count, kThreads), kThreads, 0, stream>>>(state, physical, count, out);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_compare(const double2 *x, const double2 *y, uint64_t count, double *partials, cudaStream_t stream)
+{
+    compare_kernel<<<kReduceBlocks, kThreads, 0, stream>>>(x, y, count, partials);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+template <typename R>
 int launch_gather_logical(const typename Cx<R>::T *state, int n, const int *l2p, uint64_t begin,
                           uint64_t count, double2 *out, cudaStream_t stream)
 {
@@ -751,7 +820,8 @@ int launch_narrow(const double2 *in, uint64_t count, typename Cx<R>::T *out, cud
     template int launch_scatter_logical<R>(Cx<R>::T *, int, const int *, uint64_t, uint64_t, const double2 *,       \
                                            cudaStream_t);                                                           \
     template int launch_widen<R>(const Cx<R>::T *, uint64_t, double2 *, cudaStream_t);                              \
-    template int launch_narrow<R>(const double2 *, uint64_t, Cx<R>::T *, cudaStream_t);
+    template int launch_narrow<R>(const double2 *, uint64_t, Cx<R>::T *, cudaStream_t);                           \
+    template int launch_gather_indices<R>(const Cx<R>::T *, const uint64_t *, uint64_t, double2 *, cudaStream_t);
 
 QCSB_INSTANTIATE(double)
 QCSB_INSTANTIATE(float)

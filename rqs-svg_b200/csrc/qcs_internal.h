@@ -74,6 +74,7 @@ struct GateMatrix
 // names or a wrong parameter count.
 GateMatrix gate_matrix(const char *name, const double *params, int nparams);
 int gate_arity(const char *name);
+int gate_nparams(const char *name);
 
 // Reduce a dense matrix on targets tq to a GateOp (active set + diag flag).
 GateOp make_gate_op(const GateMatrix &g, const int *tq, uint64_t cmask, uint64_t cval);
@@ -147,6 +148,14 @@ template <typename R>
 int launch_widen(const typename Cx<R>::T *in, uint64_t count, double2 *out, cudaStream_t stream);
 template <typename R>
 int launch_narrow(const double2 *in, uint64_t count, typename Cx<R>::T *out, cudaStream_t stream);
+// out[k] = state[physical[k]] widened to complex128 (physical indices in
+// device memory).
+template <typename R>
+int launch_gather_indices(const typename Cx<R>::T *state, const uint64_t *physical, uint64_t count, double2 *out,
+                          cudaStream_t stream);
+// kReduceBlocks x 5 partials: sum conj(x) y (re, im), max |x - y|, sum |x|^2,
+// sum |y|^2.
+int launch_compare(const double2 *x, const double2 *y, uint64_t count, double *partials, cudaStream_t stream);
 
 // Shot sampler (chain rule over physical qubits in the order given by
 // order[0..n)). See sampler.cu for the data layout.

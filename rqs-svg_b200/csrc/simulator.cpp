@@ -133,6 +133,7 @@ void Simulator::allocate_memory()
         max_n = kMaxQubits;
     if (n > max_n)
         throw std::runtime_error(strformat("num_qubits(%d) > max_num_qubits_local_device(%d) + log_num_procs(0)", n, max_n));
+    QCSB_CUDA(cudaGetDevice(&device_));
     QCSB_CUDA(cudaMalloc(&state_, (size_t)amp_bytes_ << n));
     n_ = n;
     perm_p2l_.assign(n, 0);
@@ -180,7 +181,7 @@ void Simulator::dispose()
     // counterpart in a single process)
     if (disposed_)
         throw std::runtime_error("dispose: the simulator has already been disposed");
-    pending_.clear();
+    discard_pending();
     disposed_ = true;
     if (stream_)
         cudaStreamSynchronize(stream_);
@@ -369,6 +370,7 @@ void Simulator::apply_gate(const char *name, const double *params, int nparams,
     else
     {
         pending_.push_back(op);
+        ++pending_gates_;
     }
 }
 
@@ -378,7 +380,7 @@ void Simulator::flush()
         return;
     const int k = fused_->run(state_, n_, amp_bytes_, pending_, fusion_mode_, stats, timer);
     stats.kernel_launches += k;
-    pending_.clear();
+    discard_pending();
 }
 
 void Simulator::synchronize()
@@ -397,7 +399,10 @@ int Simulator::measure(int q)
         return 0;
     if (contains(measured1_, q))
         return 1;
-    flush();
+    // Queued collapses of earlier measurements need not run first: the
+    // reduction below only reads the branch those measurements kept.
+    if (pending_gates_ > 0)
+        flush();
     uint64_t cmask = 0, cval = 0;
     for (int m : measured0_)
         cmask |= 1ull << perm_l2p_[m];
@@ -417,7 +422,23 @@ int Simulator::measure(int q)
     const double r = dist(engine_);
     const int result = p0 < r;
     (result ? measured1_ : measured0_).push_back(q);
-    stats.kernel_launches += QCSB_ON_STATE(launch_collapse, n_, t, result, stream_);
+    if (fusion_mode_ == QCS_FUSION_PLAIN)
+    {
+        stats.kernel_launches += QCSB_ON_STATE(launch_collapse, n_, t, result, stream_);
+    }
+    else
+    {
+        // zero the other branch as a queued diagonal op, so that it rides
+        // along with the next pass instead of costing a pass of its own
+        GateOp z;
+        z.nt = 1;
+        z.tq[0] = t;
+        z.diag = true;
+        z.na = 1;
+        z.act[0] = static_cast<uint8_t>(result ? 0 : 1);
+        z.mat[0] = cplx{0.0, 0.0};
+        pending_.push_back(z);
+    }
     return result;
 }
 
@@ -506,7 +527,7 @@ void Simulator::ensure_staging()
 {
     if (staging_dev_ != nullptr)
         return;
-    staging_count_ = std::min<uint64_t>(kStagingAmps, 1ull << n_);
+    staging_count_ = std::max<uint64_t>(2, std::min<uint64_t>(kStagingAmps, 1ull << n_));
     QCSB_CUDA(cudaMalloc(&staging_dev_, sizeof(double2) * staging_count_));
     QCSB_CUDA(cudaMallocHost(&staging_host_, sizeof(double2) * staging_count_));
 }
@@ -754,6 +775,103 @@ void KernelTimer::clear()
         pool_.push_back(r.b);
     }
     recs_.clear();
+}
+
+void Simulator::get_amplitudes(const uint64_t *indices, uint64_t count, double *out)
+{
+    require_allocated("get_amplitudes");
+    if (count > 0 && (indices == nullptr || out == nullptr))
+        throw std::runtime_error("get_amplitudes: index and output pointers must not be NULL");
+    const uint64_t total = 1ull << n_;
+    for (uint64_t k = 0; k < count; ++k)
+        if (indices[k] >= total)
+            throw std::runtime_error(strformat("get_amplitudes: index %llu is outside the register of %llu amplitudes",
+                                               (unsigned long long)indices[k], (unsigned long long)total));
+    flush();
+    ensure_staging();
+    // physical indices go through the pinned staging buffer (16 bytes per
+    // amplitude leaves room for the 8-byte index in its upper half)
+    const uint64_t chunk = staging_count_ / 2;
+    uint64_t *idx_host = reinterpret_cast<uint64_t *>(staging_host_ + chunk);
+    uint64_t *idx_dev = reinterpret_cast<uint64_t *>(staging_dev_ + chunk);
+    for (uint64_t begin = 0; begin < count; begin += chunk)
+    {
+        const uint64_t cnt = std::min<uint64_t>(chunk, count - begin);
+        for (uint64_t k = 0; k < cnt; ++k)
+        {
+            const uint64_t l = indices[begin + k];
+            uint64_t p = 0;
+            for (int q = 0; q < n_; ++q)
+                p |= ((l >> q) & 1ull) << perm_l2p_[q];
+            idx_host[k] = p;
+        }
+        QCSB_CUDA(cudaMemcpyAsync(idx_dev, idx_host, sizeof(uint64_t) * cnt, cudaMemcpyHostToDevice, stream_));
+        stats.kernel_launches += QCSB_ON_STATE(launch_gather_indices, idx_dev, cnt, staging_dev_, stream_);
+        QCSB_CUDA(cudaMemcpyAsync(staging_host_, staging_dev_, sizeof(double2) * cnt, cudaMemcpyDeviceToHost, stream_));
+        QCSB_CUDA(cudaStreamSynchronize(stream_));
+        std::memcpy(out + 2 * begin, staging_host_, sizeof(double2) * cnt);
+    }
+}
+
+void Simulator::compare(Simulator &a, Simulator &b, double *overlap_re, double *overlap_im, double *max_abs_diff,
+                        double *norm_a, double *norm_b)
+{
+    a.require_allocated("compare");
+    b.require_allocated("compare");
+    if (a.n_ != b.n_)
+        throw std::runtime_error(strformat("compare: registers of %d and %d qubits", a.n_, b.n_));
+    if (a.device_ != b.device_)
+        throw std::runtime_error("compare: the simulators are on different devices");
+    a.flush();
+    b.flush();
+    QCSB_CUDA(cudaStreamSynchronize(b.stream_));
+    a.ensure_staging();
+    b.ensure_staging();
+    double *partials = nullptr, *host = nullptr;
+    const size_t pbytes = sizeof(double) * 5 * kReduceBlocks;
+    QCSB_CUDA(cudaMalloc(&partials, pbytes));
+    if (cudaMallocHost(&host, pbytes) != cudaSuccess)
+    {
+        cudaFree(partials);
+        throw std::runtime_error("compare: cudaMallocHost failed");
+    }
+    double re = 0.0, im = 0.0, mx = 0.0, na = 0.0, nb = 0.0;
+    const uint64_t total = 1ull << a.n_;
+    cudaError_t err = cudaSuccess;
+    for (uint64_t begin = 0; begin < total && err == cudaSuccess; begin += a.staging_count_)
+    {
+        const uint64_t cnt = std::min<uint64_t>(a.staging_count_, total - begin);
+        const double2 *y = b.stage_chunk_out(begin, cnt);
+        err = cudaStreamSynchronize(b.stream_);
+        if (err != cudaSuccess)
+            break;
+        const double2 *x = a.stage_chunk_out(begin, cnt);
+        a.stats.kernel_launches += launch_compare(x, y, cnt, partials, a.stream_);
+        err = cudaMemcpyAsync(host, partials, pbytes, cudaMemcpyDeviceToHost, a.stream_);
+        if (err == cudaSuccess)
+            err = cudaStreamSynchronize(a.stream_);
+        for (int i = 0; i < kReduceBlocks && err == cudaSuccess; ++i)
+        {
+            re += host[5 * i];
+            im += host[5 * i + 1];
+            mx = std::max(mx, host[5 * i + 2]);
+            na += host[5 * i + 3];
+            nb += host[5 * i + 4];
+        }
+    }
+    cudaFree(partials);
+    cudaFreeHost(host);
+    QCSB_CUDA(err);
+    if (overlap_re)
+        *overlap_re = re;
+    if (overlap_im)
+        *overlap_im = im;
+    if (max_abs_diff)
+        *max_abs_diff = mx;
+    if (norm_a)
+        *norm_a = na;
+    if (norm_b)
+        *norm_b = nb;
 }
 
 int Simulator::event_create()

@@ -14,8 +14,8 @@ class FusedExecutor;
 class CostModel;
 
 // Features of one fused pass, the cost model's inputs: local qubits k,
-// highest local physical qubit (log2 of the largest local stride), gate
-// count, bytes per amplitude.
+// arithmetic ops (complex multiply-adds per amplitude), light ops (diagonal
+// phases and permutations), bytes per amplitude.
 struct PassFeatures
 {
     float f[4];
@@ -103,6 +103,12 @@ class Simulator
     void set_statevector(const double *in, uint64_t count);
     void expectation_z(double *out, double *norm);
     void sample(uint32_t num_shots, uint64_t *out);
+    // amplitudes at logical indices, as complex128 (re, im interleaved)
+    void get_amplitudes(const uint64_t *indices, uint64_t count, double *out);
+    // <a|b> over logical indices, max |a_i - b_i|, <a|a> and <b|b>; same
+    // register size and device, either precision
+    static void compare(Simulator &a, Simulator &b, double *overlap_re, double *overlap_im, double *max_abs_diff,
+                        double *norm_a, double *norm_b);
 
     int event_create();
     void event_record(int event_num);
@@ -125,7 +131,11 @@ class Simulator
     void ensure_staging();
     void logical_transfer(double *host, uint64_t count, bool to_host);
     const double2 *stage_chunk_out(uint64_t begin, uint64_t cnt);
-    void discard_pending() { pending_.clear(); }
+    void discard_pending()
+    {
+        pending_.clear();
+        pending_gates_ = 0;
+    }
     void restore_reference_layout();
 
     bool disposed_ = false;
@@ -147,6 +157,7 @@ class Simulator
     std::vector<cudaEvent_t> events_;
     int fusion_mode_ = QCS_FUSION_GREEDY;
     std::vector<GateOp> pending_;
+    size_t pending_gates_ = 0;   // queued ops other than deferred collapses
     FusedExecutor *fused_ = nullptr;
     CostModel *model_ = nullptr;
     int opt_max_ops_ = 0, opt_local_bits_ = 0;

@@ -73,6 +73,31 @@ class KernelTimes(ctypes.Structure):
     ]
 
 
+class BatchGate(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 16),
+        ("params", ctypes.c_double * 4),
+        ("num_targets", ctypes.c_int16),
+        ("num_negctrls", ctypes.c_int16),
+        ("num_ctrls", ctypes.c_int16),
+        ("reserved", ctypes.c_int16),
+        ("qubits", ctypes.c_int16 * 12),
+    ]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("circuits", ctypes.c_uint32),
+        ("groups", ctypes.c_uint32),
+        ("passes", ctypes.c_uint32),
+        ("launches_per_run", ctypes.c_uint32),
+        ("amplitudes", ctypes.c_uint64),
+        ("parameters", ctypes.c_uint64),
+        ("pass_bytes", ctypes.c_double),
+        ("last_run_ms", ctypes.c_double),
+    ]
+
+
 _CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_char_p, ctypes.c_size_t)
 
 
@@ -159,6 +184,18 @@ class Library:
             "qcs_simulator_set_cost_model": [_P, _P],
             "qcs_simulator_get_planner_judge": [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                                                 ctypes.POINTER(ctypes.c_double)],
+            "qcs_simulator_get_amplitudes": [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint64,
+                                             ctypes.POINTER(ctypes.c_double)],
+            "qcs_simulator_compare": [_P, _P] + [ctypes.POINTER(ctypes.c_double)] * 5,
+            "qcs_b200_batch_create": [ctypes.POINTER(_P), ctypes.c_int],
+            "qcs_b200_batch_destroy": [_P],
+            "qcs_b200_batch_add_circuit": [_P, ctypes.c_int, ctypes.POINTER(BatchGate), ctypes.c_uint32,
+                                           ctypes.POINTER(ctypes.c_uint32)],
+            "qcs_b200_batch_set_parameters": [_P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
+            "qcs_b200_batch_run": [_P],
+            "qcs_b200_batch_expectation_z": [_P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
+            "qcs_b200_batch_get_statevector": [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
+            "qcs_b200_batch_get_info": [_P, ctypes.POINTER(BatchInfo)],
         }
         for name, (np_, nt) in GATES.items():
             if name == "global_phase":
@@ -322,6 +359,25 @@ class Simulator:
     def synchronize(self):
         self.lib.call("qcs_simulator_synchronize", self.h)
 
+    def amplitudes(self, indices) -> np.ndarray:
+        """Amplitudes at the given logical indices (complex128)."""
+        idx = np.ascontiguousarray(indices, dtype=np.uint64)
+        out = np.empty(2 * idx.size, dtype=np.float64)
+        self.lib.call("qcs_simulator_get_amplitudes", self.h, idx.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                      idx.size, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out.view(np.complex128)
+
+    def compare(self, other: "Simulator") -> dict:
+        """<self|other>, max |self_i - other_i|, both squared norms and the
+        fidelity |<self|other>|^2 / (<self|self> <other|other>), over logical
+        indices."""
+        v = [ctypes.c_double() for _ in range(5)]
+        self.lib.call("qcs_simulator_compare", self.h, other.h, *[ctypes.byref(x) for x in v])
+        ovl = complex(v[0].value, v[1].value)
+        na, nb = v[3].value, v[4].value
+        return {"overlap": ovl, "max_abs_diff": v[2].value, "norm_self": na, "norm_other": nb,
+                "fidelity": abs(ovl) ** 2 / (na * nb) if na > 0 and nb > 0 else 0.0}
+
     def set_fusion(self, mode: int):
         self.lib.call("qcs_simulator_set_fusion", self.h, mode)
 
@@ -437,3 +493,86 @@ def fidelity(a: np.ndarray, b: np.ndarray) -> float:
     if na == 0 or nb == 0:
         return 1.0 if na == nb else 0.0
     return float(abs(np.vdot(a, b)) ** 2 / (na * nb))
+
+
+class Batch:
+    """Many independent circuits run together (qcs_b200_batch_*): circuits
+    with the same gates on the same qubits share one plan of fused passes,
+    and a run is one replayed CUDA graph."""
+
+    def __init__(self, lib: Library, precision: int = 128):
+        self.lib = lib
+        self.h = _P()
+        self.widths = []
+        lib.call("qcs_b200_batch_create", ctypes.byref(self.h), precision)
+
+    def close(self):
+        if self.h:
+            self.lib.call("qcs_b200_batch_destroy", self.h)
+            self.h = _P()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # numpy mirror of qcs_b200_gate (80 bytes, C layout)
+    GATE_DTYPE = np.dtype([("name", "S16"), ("params", "<f8", (4,)), ("num_targets", "<i2"),
+                           ("num_negctrls", "<i2"), ("num_ctrls", "<i2"), ("reserved", "<i2"),
+                           ("qubits", "<i2", (12,))])
+
+    @classmethod
+    def encode(cls, circuit) -> np.ndarray:
+        """Gate array of a circuit given as (op, params, targets, negctrls, ctrls) tuples."""
+        g = len(circuit)
+        arr = np.zeros(max(1, g), dtype=cls.GATE_DTYPE)
+        if g == 0:
+            return arr
+        params = np.zeros((g, 4))
+        qubits = np.zeros((g, 12), dtype=np.int16)
+        counts = np.zeros((g, 3), dtype=np.int16)
+        for i, (op, p, targets, neg, pos) in enumerate(circuit):
+            params[i, : len(p)] = p
+            qs = (*targets, *neg, *pos)
+            qubits[i, : len(qs)] = qs
+            counts[i] = (len(targets), len(neg), len(pos))
+        arr["name"] = [c[0].encode() for c in circuit]
+        arr["params"] = params
+        arr["qubits"] = qubits
+        arr["num_targets"], arr["num_negctrls"], arr["num_ctrls"] = counts[:, 0], counts[:, 1], counts[:, 2]
+        return arr
+
+    def add_circuit(self, num_qubits: int, circuit) -> int:
+        arr = self.encode(circuit)
+        idx = ctypes.c_uint32()
+        self.lib.call("qcs_b200_batch_add_circuit", self.h, num_qubits,
+                      arr.ctypes.data_as(ctypes.POINTER(BatchGate)), len(circuit), ctypes.byref(idx))
+        self.widths.append(num_qubits)
+        return idx.value
+
+    def set_parameters(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self.lib.call("qcs_b200_batch_set_parameters", self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), p.size)
+
+    def run(self):
+        self.lib.call("qcs_b200_batch_run", self.h)
+
+    def expectation_z(self):
+        """<Z_q> per circuit: a list of arrays (one value per qubit)."""
+        total = sum(self.widths)
+        out = np.empty(total, dtype=np.float64)
+        self.lib.call("qcs_b200_batch_expectation_z", self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), total)
+        return np.split(out, np.cumsum(self.widths)[:-1]) if self.widths else []
+
+    def statevector(self, index: int) -> np.ndarray:
+        size = 1 << self.widths[index]
+        out = np.empty(2 * size, dtype=np.float64)
+        self.lib.call("qcs_b200_batch_get_statevector", self.h, index,
+                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), size)
+        return out.view(np.complex128)
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        self.lib.call("qcs_b200_batch_get_info", self.h, ctypes.byref(i))
+        return {f: getattr(i, f) for f, _ in BatchInfo._fields_}

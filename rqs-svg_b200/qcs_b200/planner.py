@@ -1,8 +1,9 @@
 """Self-recorded pass timings and training of the learned cost model.
 
 The simulator times every fused pass it launches while kernel timing is on
-(features: local qubits, highest local physical qubit, gate count, bytes per
-amplitude). `collect_pass_timings` runs seeded random circuits with varied
+(features: local qubits, arithmetic ops, light ops -- diagonal phases and
+permutations -- and bytes per amplitude; none depends on the register size,
+so timings from small registers carry over to large ones). `collect_pass_timings` runs seeded random circuits with varied
 pass sizes to gather many such samples; `train_cost_model` fits the MLP on
 log(ns per amplitude) with the library's own CUDA kernels.
 """
@@ -19,12 +20,13 @@ from . import circuits as C
 _MIX = ["u3", "x", "h", "rz", "p", "ry", "swap", "rzz", "rxx", "sx"]
 
 
-def collect_pass_timings(lib: Library, n: int, min_samples: int, seed: int = 1, max_rounds: int = 100000):
+def collect_pass_timings(lib: Library, n: int, min_samples: int, seed: int = 1, max_rounds: int = 100000,
+                         precision: int = 128):
     """Return (features [N x 4] float32, target [N] float32 = log(ns/amp))."""
     rng = np.random.default_rng(seed)
     feats, targets = [], []
     total = 0
-    with Simulator(lib, n, fusion=FUSION_GREEDY) as sim:
+    with Simulator(lib, n, fusion=FUSION_GREEDY, precision=precision) as sim:
         sim.set_kernel_timing(True)
         rounds = 0
         while total < min_samples and rounds < max_rounds:

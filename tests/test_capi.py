@@ -78,3 +78,26 @@ def test_cli_help_lists_reference_options():
     assert r.returncode == 0
     for opt in ("--num-samples", "--mapping", "--reversed-mapping", "--output-statevector"):
         assert opt in r.stdout
+
+
+def test_python_structs_match_the_c_header(tmp_path):
+    """The ctypes mirrors of the extension structs have the C layout."""
+    import ctypes
+
+    src = tmp_path / "sizes.c"
+    src.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "qcs_b200.h"\n'
+        "int main(void) {\n"
+        '  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(qcs_b200_gate), offsetof(qcs_b200_gate, params),\n'
+        "         offsetof(qcs_b200_gate, num_targets), offsetof(qcs_b200_gate, qubits),\n"
+        "         sizeof(qcs_b200_batch_info), offsetof(qcs_b200_batch_info, amplitudes),\n"
+        "         offsetof(qcs_b200_batch_info, last_run_ms));\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "sizes"
+    inc = Path(__file__).resolve().parent.parent / "include"
+    subprocess.run(["gcc", "-std=c11", f"-I{inc}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    G, I = qcs_b200.BatchGate, qcs_b200.BatchInfo
+    want = [ctypes.sizeof(G), G.params.offset, G.num_targets.offset, G.qubits.offset,
+            ctypes.sizeof(I), I.amplitudes.offset, I.last_run_ms.offset]
+    assert got == want

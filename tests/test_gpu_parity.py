@@ -60,6 +60,36 @@ def test_mixed_random_circuits(gpu_lib, oracle_lib, n, mode):
     assert np.max(np.abs(got - ref)) <= TOL
 
 
+DIAGONAL_GATES = ["z", "s", "sdg", "t", "tdg", "rz", "u1", "p", "rzz", "global_phase"]
+
+
+@pytest.mark.parametrize("n", [10, 13, 16])
+def test_diagonal_runs_match_oracle(gpu_lib, oracle_lib, n):
+    """Long runs of diagonal gates (phase runs in a fused pass), with positive
+    and negative controls inside and outside the pass's local qubits, between
+    dense gates that bound the runs."""
+    rng = np.random.default_rng(n)
+    circ = []
+    for blk in range(12):
+        circ += C.random_circuit(n, int(rng.integers(1, 4)), seed=500 + blk, max_controls=1,
+                                 gates=["h", "u3", "rx", "sx", "swap"])
+        circ += C.random_circuit(n, int(rng.integers(2, 25)), seed=900 + blk, max_controls=3, gates=DIAGONAL_GATES)
+    start = _random_state(n, 3)
+    got, _ = _run(gpu_lib, n, circ, fusion=FUSION_GREEDY, start=start)
+    ref, _ = _run(oracle_lib, n, circ, start=start)
+    assert np.max(np.abs(got - ref)) <= 1e-12
+
+
+def test_long_diagonal_run_with_interleaved_commuting_gates(gpu_lib, oracle_lib):
+    # RZ after RY on each qubit: the stage reorders them into one run
+    n = 14
+    circ = C.hea_circuit(n, 6, seed=2) + C.qft(n, seed=3)[0]
+    start = _random_state(n, 4)
+    got, _ = _run(gpu_lib, n, circ, fusion=FUSION_GREEDY, start=start)
+    ref, _ = _run(oracle_lib, n, circ, start=start)
+    assert np.max(np.abs(got - ref)) <= 1e-12
+
+
 @pytest.mark.parametrize("mode", MODES)
 def test_twenty_qubit_layered_and_qft(gpu_lib, oracle_lib, mode):
     for circ in (C.layered_u3_cz(20, 6, seed=3), C.qft(20, seed=4)[0], C.layered_u3_cz_cx_toffoli(20, 4, seed=5)):
