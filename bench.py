@@ -88,7 +88,7 @@ WORKLOADS = {
     "cli": (None, 20, "bin/qcs -s " + str(CLI_SAMPLES) + " on a circuit plug-in: layered U3 + CZ, {n} qubits, "
                       "depth {d}, {p}, then a measurement of every qubit; each sample re-runs the circuit",
             False),
-    "hea_batch": (None, 8, str(BATCH_CIRCUITS) + " hardware-efficient-ansatz circuits (RY, RZ on every qubit, "
+    "hea_batch": (None, 8, "{c} hardware-efficient-ansatz circuits (RY, RZ on every qubit, "
                            "CX ladder per layer), widths uniform in 10..20, depth {d}, {p}, new parameters "
                            "every step -> <Z_q> of every circuit", False),
     "layered": (_layered, 40, "layered U3 + CZ/CX + Toffoli, {n} qubits, depth {d}, {p}, "
@@ -114,8 +114,10 @@ def parse_args():
                     help="amplitude bits (default 128; 64 for hea_batch)")
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--depth", type=int, default=None, help="layers (default 40 layered, 60 matching)")
-    ap.add_argument("--train-qubits", type=int, default=24, help="register size the cost model's timings come from")
+    ap.add_argument("--train-qubits", default="18,20,22,24",
+                    help="register sizes (comma-separated) the cost model's timings come from")
     ap.add_argument("--train-samples", type=int, default=20000, help="pass timings recorded to train the cost model")
+    ap.add_argument("--batch-circuits", type=int, default=BATCH_CIRCUITS, help="circuits of the hea_batch workload")
     ap.add_argument("--no-plain-compare", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-peak", action="store_true")
@@ -321,7 +323,8 @@ def train_planner(lib, args):
     from qcs_b200 import planner
 
     t0 = time.perf_counter()
-    feats, target = planner.collect_pass_timings(lib, args.train_qubits, args.train_samples, seed=11,
+    sizes = [int(v) for v in str(args.train_qubits).split(",")]
+    feats, target = planner.collect_pass_timings(lib, sizes, args.train_samples, seed=11,
                                                  precision=args.precision)
     t1 = time.perf_counter()
     model, loss = planner.train_cost_model(lib, feats, target, epochs=60)
@@ -521,10 +524,10 @@ def main():
         dist.destroy_process_group()
 
 
-def batch_circuits(depth, seed=1):
+def batch_circuits(depth, count=BATCH_CIRCUITS, seed=1):
     """The batch workload's circuits: widths uniform in 10..20 (seeded)."""
     rng = np.random.default_rng(seed)
-    widths = [int(w) for w in rng.integers(10, 21, size=BATCH_CIRCUITS)]
+    widths = [int(w) for w in rng.integers(10, 21, size=count)]
     return widths, [C.hea_circuit(w, depth, seed=1000 + i) for i, w in enumerate(widths)]
 
 
@@ -539,8 +542,8 @@ def main_batch(args, dist):
     precision = args.precision or 64
     depth = args.depth if args.depth is not None else 8
     gen, _, desc, _ = WORKLOADS["hea_batch"]
-    workload = desc.format(d=depth, p="complex128" if precision == 128 else "complex64")
-    widths, circs = batch_circuits(depth)
+    workload = desc.format(c=args.batch_circuits, d=depth, p="complex128" if precision == 128 else "complex64")
+    widths, circs = batch_circuits(depth, args.batch_circuits)
     if args.impl == "reference":
         return run_reference_batch(args, dist, widths, circs, depth, workload)
     lib = qcs_b200.Library(qcs_b200.LIB_PATH)
@@ -581,15 +584,15 @@ def main_batch(args, dist):
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_batch(widths, circs)
     line = {
-        "metric": f"batch wall s ({BATCH_CIRCUITS} HEA circuits)",
+        "metric": f"batch wall s ({len(circs)} HEA circuits)",
         "value": agg["value"], "unit": "s", "n_gpus": WORLD, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": sec * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "c128 (f64)" if precision == 128 else "c64 (f32 gates, f64 reductions)",
         "data": "synthetic (seeded circuits and parameters)",
-        "config": {"workload": workload, "circuits": BATCH_CIRCUITS, "depth": depth, "precision": precision,
+        "config": {"workload": workload, "circuits": len(circs), "depth": depth, "precision": precision,
                    "amplitudes": info["amplitudes"], "parallelism": f"replicas x{WORLD}",
                    "l2": f"registers ({info['amplitudes'] * precision // 8 >> 20} MiB) larger than L2; no flush"},
-        "circuits_per_s": BATCH_CIRCUITS / sec,
+        "circuits_per_s": len(circs) / sec,
         "hbm_gbs_algorithmic": alg / sec / 1e9,
         "e2e": {"value": e2e_total / args.steps / WORLD, "unit": "s", "h2d_bytes_per_step": nparams * 8,
                 "d2h_bytes_per_step": sum(widths) * 8},
@@ -641,7 +644,7 @@ def run_reference_batch(args, dist, widths, circs, depth, workload, stride=16):
     ref_so = REPO / "oracle" / "_ref" / "libqcs_ref.so"
     if not ref_so.exists():
         cpu = cpu_baseline_batch(widths, circs)
-        print(json.dumps({"impl": "reference", "metric": f"batch wall s ({BATCH_CIRCUITS} HEA circuits)",
+        print(json.dumps({"impl": "reference", "metric": f"batch wall s ({len(circs)} HEA circuits)",
                           "value": cpu["value"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
                           "higher_is_better": False, "config": {"workload": workload}, "cpu_baseline": cpu,
                           "e2e": {"value": cpu["value"], "unit": "s", "h2d_bytes_per_step": 0,
@@ -679,13 +682,13 @@ def run_reference_batch(args, dist, widths, circs, depth, workload, stride=16):
     for sim in sims.values():
         sim.close()
     value = sum(wall) / args.steps
-    line = {"impl": "reference", "metric": f"batch wall s ({BATCH_CIRCUITS} HEA circuits)", "value": value,
+    line = {"impl": "reference", "metric": f"batch wall s ({len(circs)} HEA circuits)", "value": value,
             "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)",
             "data": "synthetic (seeded circuits)",
             "config": {"workload": workload.replace("complex64", "complex128").split(" -> ")[0]
                        + " -> one measurement of every qubit, circuit by circuit (the reference has no batch, "
-                         "<Z> or complex64)", "circuits": BATCH_CIRCUITS, "depth": depth},
+                         "<Z> or complex64)", "circuits": len(circs), "depth": depth},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "reference",
                              "sample": f"reference library on the GPU (one simulator per register size, reset "

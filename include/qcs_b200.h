@@ -156,7 +156,7 @@ int qcs_simulator_get_kernel_times(qcs_simulator *sim, qcs_b200_kernel_times *ti
 
 /*
  * Planner knobs for the fused modes: the most gates one pass may carry
- * (default 64) and the number of local qubits of a pass (default 11, range
+ * (default 256) and the number of local qubits of a pass (default 11, range
  * 9..11). 0 keeps a default. Used to tune, and to record diverse pass
  * timings for the cost model.
  */
@@ -164,11 +164,11 @@ int qcs_simulator_set_planner_options(qcs_simulator *sim, int max_gates_per_pass
 
 /*
  * Pass timings recorded while kernel timing is enabled: for each fused pass
- * its features (4 floats: local qubits; arithmetic ops, which run complex
+ * its features (4 floats: local qubits k; arithmetic ops, which run complex
  * multiply-adds on every amplitude; light ops, diagonal phases and
- * permutations such as X, CX, SWAP; bytes per amplitude) and its device time
- * in milliseconds. The features do not depend on the register size. Reading
- * synchronizes, returns up to capacity records in *count and clears them.
+ * permutations such as X, CX, SWAP; log2 of the number of chunks, n - k,
+ * capped at 16) and its device time in milliseconds. Reading synchronizes,
+ * returns up to capacity records in *count and clears them.
  */
 int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *milliseconds, uint32_t capacity,
                                    uint32_t *count);
@@ -177,7 +177,8 @@ int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *m
  * Learned cost model of fused passes: an MLP 4 -> 64 -> 64 -> 1 (FP32, ReLU)
  * whose training and inference run as this library's own CUDA kernels.
  * Inputs are the pass features above; the target is log(device time per
- * amplitude in nanoseconds) = log(ms * 1e6 / 2^n). Attach a trained model to
+ * amplitude in nanoseconds) = log(ms * 1e6 / 2^n). A model is trained on
+ * timings of one amplitude type (complex128 or complex64). Attach a trained model to
  * a simulator and select QCS_FUSION_LEARNED to let it plan passes; measured
  * device time then decides, per gate queue, between its plan and the greedy
  * one.

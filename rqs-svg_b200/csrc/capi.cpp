@@ -83,14 +83,33 @@ std::vector<int> to_vector(const bit_num_t *values, bit_num_t count)
     return std::vector<int>(values, values + count);
 }
 
+// Qubit list of a gate call copied to ints; a list longer than any register
+// holds a repeated or out-of-range qubit, which the simulator reports.
+struct QubitList
+{
+    int q[qcsb::kMaxQubits + 1];
+    int n;
+    QubitList(const bit_num_t *values, bit_num_t count)
+    {
+        if (count < 0)
+            throw std::runtime_error("array element count must be non-negative");
+        if (count > 0 && values == nullptr)
+            throw std::runtime_error("array pointer must not be NULL when element count is positive");
+        n = std::min<int>(count, qcsb::kMaxQubits + 1);
+        for (int i = 0; i < n; ++i)
+            q[i] = values[i];
+    }
+};
+
 void gate(qcs_simulator *sim, const char *name, std::initializer_list<double> params,
           const bit_num_t *t, bit_num_t nt, const bit_num_t *neg, bit_num_t nneg, const bit_num_t *ctl, bit_num_t nctl)
 {
-    auto targets = to_vector(t, nt);
-    auto negs = to_vector(neg, nneg);
-    auto ctls = to_vector(ctl, nctl);
-    const std::vector<double> p(params);
-    core(sim).apply_gate(name, p.data(), (int)p.size(), targets, negs, ctls);
+    const QubitList targets(t, nt), negs(neg, nneg), ctls(ctl, nctl);
+    double p[4];
+    int np = 0;
+    for (double v : params)
+        p[np++] = v;
+    core(sim).apply_gate(name, p, np, targets.q, targets.n, negs.q, negs.n, ctls.q, ctls.n);
 }
 
 } // namespace

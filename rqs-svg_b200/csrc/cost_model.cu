@@ -3,7 +3,7 @@
 // backward, Adam) on pass timings the simulator records itself.
 //
 // Inputs (per pass): block width (local qubits k), arithmetic ops, light ops
-// (diagonal phases and permutations), bytes per amplitude.
+// (diagonal phases and permutations), log2 of the chunk count (capped).
 // Target: log(device time per amplitude in ns). Inputs and target are
 // standardised with the training set's mean and deviation.
 //

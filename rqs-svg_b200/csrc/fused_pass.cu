@@ -89,10 +89,12 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 constexpr int R = 1 << kStageBits;
 
-// Gate application on a thread's 2^kStageBits amplitudes a[r] (r = bits of
-// the stage's local bits; jr[r] = the amplitude's local index). Gates without
-// local controls take the unconditional path; controlled ones predicate each
-// pair or amplitude on (jr & lcmask) == lcval.
+// Gate application on a thread's 2^kStageBits amplitudes a[r] (r = the values
+// of the stage's local bits; j0 = the thread's local index with the stage
+// bits zero). A condition splits into the other local bits (checked once
+// against j0: when it fails the op does nothing for this thread) and the
+// stage bits (smask/sval, checked per slot r). Ops without a condition take
+// the unconditional path.
 
 // Where an op's matrix entries come from: the pass parameters (one register)
 // or the register's block of the entry buffer (batched passes).
@@ -109,11 +111,12 @@ struct BufferEntries
 };
 
 template <typename V, int B, typename M>
-__device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &e, const uint32_t (&jr)[R])
+__device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &e, uint32_t j0)
 {
     const V m00 = cvt<V>(e[0]), m01 = cvt<V>(e[1]), m10 = cvt<V>(e[2]), m11 = cvt<V>(e[3]);
-    const uint32_t cm = op.lcmask, cv = op.lcval;
-    if (cm == 0)
+    const bool tok = (j0 & op.lcmask) == op.lcval;
+    const uint32_t cm = op.smask, cv = op.sval;
+    if (cm == 0 && op.lcmask == 0)
     {
 #pragma unroll
         for (int r = 0; r < R; ++r)
@@ -132,7 +135,7 @@ __device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &
     {
         if (r & (1 << B))
             continue;
-        if ((jr[r] & cm) == cv)
+        if (tok && (r & cm) == cv)
         {
             const int r1 = r | (1 << B);
             const V x0 = a[r], x1 = a[r1];
@@ -142,11 +145,38 @@ __device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &
     }
 }
 
-template <typename V, int B>
-__device__ __forceinline__ void apply_swap1(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+// Real 2x2: each output component is a real combination of the same
+// component of the two inputs (half the multiply-adds of the complex case).
+template <typename V, int B, typename M>
+__device__ __forceinline__ void apply_dense1r(V (&a)[R], const FOp &op, const M &e, uint32_t j0)
 {
-    const uint32_t cm = op.lcmask, cv = op.lcval;
-    if (cm == 0)
+    typedef decltype(V::x) S;
+    const S m00 = static_cast<S>(e[0].x), m01 = static_cast<S>(e[1].x);
+    const S m10 = static_cast<S>(e[2].x), m11 = static_cast<S>(e[3].x);
+    const bool tok = (j0 & op.lcmask) == op.lcval;
+    const uint32_t cm = op.smask, cv = op.sval;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+        if (r & (1 << B))
+            continue;
+        if (!tok || (cm != 0 && (r & cm) != cv))
+            continue;
+        const int r1 = r | (1 << B);
+        const V x0 = a[r], x1 = a[r1];
+        a[r].x = fma(m00, x0.x, m01 * x1.x);
+        a[r].y = fma(m00, x0.y, m01 * x1.y);
+        a[r1].x = fma(m10, x0.x, m11 * x1.x);
+        a[r1].y = fma(m10, x0.y, m11 * x1.y);
+    }
+}
+
+template <typename V, int B>
+__device__ __forceinline__ void apply_swap1(V (&a)[R], const FOp &op, uint32_t j0)
+{
+    const bool tok = (j0 & op.lcmask) == op.lcval;
+    const uint32_t cm = op.smask, cv = op.sval;
+    if (cm == 0 && op.lcmask == 0)
     {
 #pragma unroll
         for (int r = 0; r < R; ++r)
@@ -165,7 +195,7 @@ __device__ __forceinline__ void apply_swap1(V (&a)[R], const FOp &op, const uint
     {
         if (r & (1 << B))
             continue;
-        if ((jr[r] & cm) == cv)
+        if (tok && (r & cm) == cv)
         {
             const int r1 = r | (1 << B);
             const V t = a[r];
@@ -176,15 +206,16 @@ __device__ __forceinline__ void apply_swap1(V (&a)[R], const FOp &op, const uint
 }
 
 template <typename V, int B0, int B1, typename M>
-__device__ __forceinline__ void apply_dense2(V (&a)[R], const FOp &op, const M &m, const uint32_t (&jr)[R])
+__device__ __forceinline__ void apply_dense2(V (&a)[R], const FOp &op, const M &m, uint32_t j0)
 {
-    const uint32_t cm = op.lcmask, cv = op.lcval;
+    const bool tok = (j0 & op.lcmask) == op.lcval;
+    const uint32_t cm = op.smask, cv = op.sval;
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
         if (r & ((1 << B0) | (1 << B1)))
             continue;
-        if ((jr[r] & cm) != cv)
+        if (!tok || (r & cm) != cv)
             continue;
         const int i1 = r | (1 << B0), i2 = r | (1 << B1), i3 = r | (1 << B0) | (1 << B1);
         const V x0 = a[r], x1 = a[i1], x2 = a[i2], x3 = a[i3];
@@ -200,15 +231,16 @@ __device__ __forceinline__ void apply_dense2(V (&a)[R], const FOp &op, const M &
 }
 
 template <typename V, int B0, int B1>
-__device__ __forceinline__ void apply_swap2(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+__device__ __forceinline__ void apply_swap2(V (&a)[R], const FOp &op, uint32_t j0)
 {
-    const uint32_t cm = op.lcmask, cv = op.lcval;
+    const bool tok = (j0 & op.lcmask) == op.lcval;
+    const uint32_t cm = op.smask, cv = op.sval;
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
         if (r & ((1 << B0) | (1 << B1)))
             continue;
-        if ((jr[r] & cm) == cv)
+        if (tok && (r & cm) == cv)
         {
             const int i1 = r | (1 << B0), i2 = r | (1 << B1);
             const V t = a[i1];
@@ -219,107 +251,161 @@ __device__ __forceinline__ void apply_swap2(V (&a)[R], const FOp &op, const uint
 }
 
 template <typename V, typename M>
-__device__ __forceinline__ void apply_phase(V (&a)[R], const FOp &op, const M &m, const uint32_t (&jr)[R])
+__device__ __forceinline__ void apply_phase(V (&a)[R], const FOp &op, const M &m, uint32_t j0)
 {
     const V e = cvt<V>(m[0]);
-    const uint32_t cm = op.lcmask, cv = op.lcval;
+    const bool tok = (j0 & op.lcmask) == op.lcval;
+    const uint32_t cm = op.smask, cv = op.sval;
 #pragma unroll
     for (int r = 0; r < R; ++r)
-        if ((jr[r] & cm) == cv)
+        if (tok && (r & cm) == cv)
             a[r] = cmul(e, a[r]);
 }
 
+// Sign flips on the integer pipe (the FP64/FP32 pipes are the busy ones).
+__device__ __forceinline__ double flip(double x) { return __longlong_as_double(__double_as_longlong(x) ^ (1ll << 63)); }
+__device__ __forceinline__ float flip(float x) { return __int_as_float(__float_as_int(x) ^ (1 << 31)); }
+
+template <typename V>
+__device__ __forceinline__ void apply_neg(V (&a)[R], const FOp &op, uint32_t j0)
+{
+    const bool tok = (j0 & op.lcmask) == op.lcval;
+    const uint32_t cm = op.smask, cv = op.sval;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (tok && (r & cm) == cv)
+        {
+            a[r].x = flip(a[r].x);
+            a[r].y = flip(a[r].y);
+        }
+}
+
+// times i: (x, y) -> (-y, x); times -i: (x, y) -> (y, -x)
+template <typename V>
+__device__ __forceinline__ void apply_muli(V (&a)[R], const FOp &op, uint32_t j0)
+{
+    const bool tok = (j0 & op.lcmask) == op.lcval;
+    const uint32_t cm = op.smask, cv = op.sval;
+    const bool minus = op.b1 != 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (tok && (r & cm) == cv)
+        {
+            const auto x = a[r].x, y = a[r].y;
+            a[r].x = minus ? y : flip(y);
+            a[r].y = minus ? flip(x) : x;
+        }
+}
+
 template <typename V, typename M>
-__device__ __forceinline__ void apply_diag(V (&a)[R], const FOp &op, const M &m, const uint32_t (&jr)[R],
-                                           uint64_t cbase)
+__device__ __forceinline__ void apply_diag(V (&a)[R], const FOp &op, const M &m, uint32_t j0, uint64_t cbase)
 {
     // one or two targets: entries in registers, chosen per amplitude by its
-    // target bits (from the local index, or from the chunk when not local)
+    // target bits (from the slot r for stage bits, the thread's local index
+    // for other local bits, or the chunk when not local)
+    const bool tok = (j0 & op.lcmask) == op.lcval;
     const V d0 = cvt<V>(m[0]), d1 = cvt<V>(m[1]), d2 = cvt<V>(m[2]), d3 = cvt<V>(m[3]);
-    const uint32_t cm = op.lcmask, cv = op.lcval;
-    const int l0 = op.loc[0], l1 = op.nt > 1 ? op.loc[1] : -1;
-    const uint32_t c0 = l0 < 0 ? static_cast<uint32_t>((cbase >> op.phys[0]) & 1ull) : 0u;
-    const uint32_t c1 = (op.nt > 1 && l1 < 0) ? static_cast<uint32_t>((cbase >> op.phys[1]) & 1ull) : 0u;
-    const uint32_t sh0 = l0 < 0 ? 0u : static_cast<uint32_t>(l0);
-    const uint32_t sh1 = l1 < 0 ? 0u : static_cast<uint32_t>(l1);
-    const uint32_t use0 = l0 < 0 ? 0u : 1u, use1 = l1 < 0 ? 0u : 1u;
+    const uint32_t cm = op.smask, cv = op.sval;
+    auto fixed_bit = [&](int i) -> uint32_t {
+        if (i >= op.nt)
+            return 0u;
+        if (op.loc[i] >= 0)
+            return (j0 >> op.loc[i]) & 1u;
+        return static_cast<uint32_t>((cbase >> op.phys[i]) & 1ull);
+    };
+    const uint32_t c0 = fixed_bit(0), c1 = fixed_bit(1);
+    const int p0 = op.spos[0], p1 = op.nt > 1 ? op.spos[1] : -1;
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
-        const uint32_t j = jr[r];
-        if ((j & cm) != cv)
+        if (!tok || (r & cm) != cv)
             continue;
-        const uint32_t s0 = use0 ? ((j >> sh0) & 1u) : c0;
-        const uint32_t s1 = use1 ? ((j >> sh1) & 1u) : c1;
+        const uint32_t s0 = p0 >= 0 ? ((r >> p0) & 1u) : c0;
+        const uint32_t s1 = p1 >= 0 ? ((r >> p1) & 1u) : c1;
         const V d = s1 ? (s0 ? d3 : d2) : (s0 ? d1 : d0);
         a[r] = cmul(d, a[r]);
     }
 }
 
 template <typename V, typename M>
-__device__ __forceinline__ void dispatch_dense1(V (&a)[R], const FOp &op, const M &e, const uint32_t (&jr)[R])
+__device__ __forceinline__ void dispatch_dense1(V (&a)[R], const FOp &op, const M &e, uint32_t j0)
 {
     switch (op.b0)
     {
-    case 0: apply_dense1<V, 0>(a, op, e, jr); break;
-    case 1: apply_dense1<V, 1>(a, op, e, jr); break;
-    case 2: apply_dense1<V, 2>(a, op, e, jr); break;
-    default: apply_dense1<V, 3>(a, op, e, jr); break;
+    case 0: apply_dense1<V, 0>(a, op, e, j0); break;
+    case 1: apply_dense1<V, 1>(a, op, e, j0); break;
+    case 2: apply_dense1<V, 2>(a, op, e, j0); break;
+    default: apply_dense1<V, 3>(a, op, e, j0); break;
+    }
+}
+
+template <typename V, typename M>
+__device__ __forceinline__ void dispatch_dense1r(V (&a)[R], const FOp &op, const M &e, uint32_t j0)
+{
+    switch (op.b0)
+    {
+    case 0: apply_dense1r<V, 0>(a, op, e, j0); break;
+    case 1: apply_dense1r<V, 1>(a, op, e, j0); break;
+    case 2: apply_dense1r<V, 2>(a, op, e, j0); break;
+    default: apply_dense1r<V, 3>(a, op, e, j0); break;
     }
 }
 
 template <typename V>
-__device__ __forceinline__ void dispatch_swap1(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+__device__ __forceinline__ void dispatch_swap1(V (&a)[R], const FOp &op, uint32_t j0)
 {
     switch (op.b0)
     {
-    case 0: apply_swap1<V, 0>(a, op, jr); break;
-    case 1: apply_swap1<V, 1>(a, op, jr); break;
-    case 2: apply_swap1<V, 2>(a, op, jr); break;
-    default: apply_swap1<V, 3>(a, op, jr); break;
+    case 0: apply_swap1<V, 0>(a, op, j0); break;
+    case 1: apply_swap1<V, 1>(a, op, j0); break;
+    case 2: apply_swap1<V, 2>(a, op, j0); break;
+    default: apply_swap1<V, 3>(a, op, j0); break;
     }
 }
 
 // (b0, b1) with b0 < b1 encoded as b0 * 4 + b1
 template <typename V, typename M>
-__device__ __forceinline__ void dispatch_dense2(V (&a)[R], const FOp &op, const M &e, const uint32_t (&jr)[R])
+__device__ __forceinline__ void dispatch_dense2(V (&a)[R], const FOp &op, const M &e, uint32_t j0)
 {
     switch (op.b0 * 4 + op.b1)
     {
-    case 1: apply_dense2<V, 0, 1>(a, op, e, jr); break;
-    case 2: apply_dense2<V, 0, 2>(a, op, e, jr); break;
-    case 3: apply_dense2<V, 0, 3>(a, op, e, jr); break;
-    case 6: apply_dense2<V, 1, 2>(a, op, e, jr); break;
-    case 7: apply_dense2<V, 1, 3>(a, op, e, jr); break;
-    default: apply_dense2<V, 2, 3>(a, op, e, jr); break;
+    case 1: apply_dense2<V, 0, 1>(a, op, e, j0); break;
+    case 2: apply_dense2<V, 0, 2>(a, op, e, j0); break;
+    case 3: apply_dense2<V, 0, 3>(a, op, e, j0); break;
+    case 6: apply_dense2<V, 1, 2>(a, op, e, j0); break;
+    case 7: apply_dense2<V, 1, 3>(a, op, e, j0); break;
+    default: apply_dense2<V, 2, 3>(a, op, e, j0); break;
     }
 }
 
 template <typename V>
-__device__ __forceinline__ void dispatch_swap2(V (&a)[R], const FOp &op, const uint32_t (&jr)[R])
+__device__ __forceinline__ void dispatch_swap2(V (&a)[R], const FOp &op, uint32_t j0)
 {
     switch (op.b0 * 4 + op.b1)
     {
-    case 1: apply_swap2<V, 0, 1>(a, op, jr); break;
-    case 2: apply_swap2<V, 0, 2>(a, op, jr); break;
-    case 3: apply_swap2<V, 0, 3>(a, op, jr); break;
-    case 6: apply_swap2<V, 1, 2>(a, op, jr); break;
-    case 7: apply_swap2<V, 1, 3>(a, op, jr); break;
-    default: apply_swap2<V, 2, 3>(a, op, jr); break;
+    case 1: apply_swap2<V, 0, 1>(a, op, j0); break;
+    case 2: apply_swap2<V, 0, 2>(a, op, j0); break;
+    case 3: apply_swap2<V, 0, 3>(a, op, j0); break;
+    case 6: apply_swap2<V, 1, 2>(a, op, j0); break;
+    case 7: apply_swap2<V, 1, 3>(a, op, j0); break;
+    default: apply_swap2<V, 2, 3>(a, op, j0); break;
     }
 }
 
 template <typename V, typename M>
-__device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, const uint32_t (&jr)[R], uint64_t cbase)
+__device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, uint32_t j0, uint64_t cbase)
 {
     switch (op.kind)
     {
-    case F_DENSE1: dispatch_dense1<V>(a, op, e, jr); break;
-    case F_SWAP1: dispatch_swap1<V>(a, op, jr); break;
-    case F_DENSE2: dispatch_dense2<V>(a, op, e, jr); break;
-    case F_SWAP2: dispatch_swap2<V>(a, op, jr); break;
-    case F_PHASE: apply_phase<V>(a, op, e, jr); break;
-    default: apply_diag<V>(a, op, e, jr, cbase); break;
+    case F_DENSE1: dispatch_dense1<V>(a, op, e, j0); break;
+    case F_DENSE1R: dispatch_dense1r<V>(a, op, e, j0); break;
+    case F_NEG: apply_neg<V>(a, op, j0); break;
+    case F_MULI: apply_muli<V>(a, op, j0); break;
+    case F_SWAP1: dispatch_swap1<V>(a, op, j0); break;
+    case F_DENSE2: dispatch_dense2<V>(a, op, e, j0); break;
+    case F_SWAP2: dispatch_swap2<V>(a, op, j0); break;
+    case F_PHASE: apply_phase<V>(a, op, e, j0); break;
+    default: apply_diag<V>(a, op, e, j0, cbase); break;
     }
 }
 
@@ -480,31 +566,27 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
             }
             // swz is linear over GF(2) and j0 shares no bit with a stage
             // offset, so swz(j0 | off) = swz(j0) ^ swz(off)
-            uint32_t bit[kStageBits], sbit[kStageBits];
+            uint32_t sbit[kStageBits];
 #pragma unroll
             for (int b = 0; b < kStageBits; ++b)
-            {
-                bit[b] = 1u << S.sbits[b];
-                sbit[b] = static_cast<uint32_t>(swz<V>(static_cast<int>(bit[b])));
-            }
+                sbit[b] = static_cast<uint32_t>(swz<V>(static_cast<int>(1u << S.sbits[b])));
             const uint32_t p0 = static_cast<uint32_t>(swz<V>(static_cast<int>(j0)));
-            uint32_t jr[R], pos[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-            {
-                uint32_t j = j0, q = p0;
+            // shared-memory position of slot r (recomputed where needed, so
+            // that the 16 positions do not stay live in registers)
+            auto pos_of = [&](int r) -> uint32_t {
+                uint32_t q = p0;
 #pragma unroll
                 for (int b = 0; b < kStageBits; ++b)
                     if ((r >> b) & 1)
-                    {
-                        j |= bit[b];
                         q ^= sbit[b];
-                    }
-                jr[r] = j;
-                pos[r] = q;
-            }
+                return q;
+            };
             if (S.kind == 1)
             {
+                uint32_t pos[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    pos[r] = pos_of(r);
                 if (BATCH)
                     phase_stage<V>(sb, pos, j0, cbase, p.ops + S.op_begin, S.op_end - S.op_begin,
                                    [&](int off) { return __ldg(entries + off); });
@@ -517,20 +599,20 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
             V a[R];
 #pragma unroll
             for (int r = 0; r < R; ++r)
-                a[r] = sb[pos[r]];
+                a[r] = sb[pos_of(r)];
             for (int oi = S.op_begin; oi < S.op_end; ++oi)
             {
                 const FOp &op = p.ops[oi];
                 if ((cbase & op.gcmask) != op.gcval)
                     continue;
                 if (BATCH)
-                    apply_op<V>(a, op, BufferEntries{entries + op.moff}, jr, cbase);
+                    apply_op<V>(a, op, BufferEntries{entries + op.moff}, j0, cbase);
                 else
-                    apply_op<V>(a, op, PoolEntries{p, op.moff}, jr, cbase);
+                    apply_op<V>(a, op, PoolEntries{p, op.moff}, j0, cbase);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r)
-                sb[pos[r]] = a[r];
+                sb[pos_of(r)] = a[r];
             __syncthreads();
         }
 
@@ -588,6 +670,15 @@ bool is_perm(const GateOp &op, int size)
 
 bool is_x(const GateOp &op) { return op.nt == 1 && is_perm(op, 2); }
 bool is_swap(const GateOp &op) { return op.nt == 2 && op.act[0] == 1 && op.act[1] == 2 && is_perm(op, 2); }
+
+bool is_real(const GateOp &op)
+{
+    const int ne = op.diag ? op.na : op.na * op.na;
+    for (int e = 0; e < ne; ++e)
+        if (op.mat[e].im != 0.0)
+            return false;
+    return true;
+}
 
 int op_entry_count(const GateOp &op)
 {
@@ -744,9 +835,10 @@ void schedule_stages(const std::vector<GateOp> &q, const PlannedPass &pp, const 
 
 // Unitary diagonal gates on at most two targets join phase runs. A run is
 // applied as one phase stage when its weight reaches phase_run_min() (tuning
-// knob QCS_PHASE_RUN_MIN, default 6): a one-entry phase (CZ, CP, T, ...)
-// weighs 1, a diagonal with two or four entries (RZ, RZZ) 2, the ratio of
-// their costs as single ops. A phase stage has a fixed cost of about six
+// knob QCS_PHASE_RUN_MIN, default 6): a one-entry phase (CP, T, ...) weighs
+// 1, a diagonal with two or four entries (RZ, RZZ) 2, the ratio of their
+// costs as single ops; phases by -1 or +-i (Z, CZ, S) weigh 0, since alone
+// they are sign flips and exchanges. A phase stage has a fixed cost of about six
 // one-entry phases (the 16-way subset products), measured on B200.
 int phase_run_min()
 {
@@ -758,7 +850,15 @@ int phase_run_min()
     return v;
 }
 
-int phase_weight(const GateOp &op) { return op.na == 1 ? 1 : 2; }
+int phase_weight(const GateOp &op)
+{
+    if (op.na != 1)
+        return 2;
+    // -1 and +-i run as sign flips and exchanges: cheaper alone than as terms
+    const cplx e = op.mat[0];
+    const bool clifford = (e.re == -1.0 && e.im == 0.0) || (e.re == 0.0 && (e.im == 1.0 || e.im == -1.0));
+    return clifford ? 0 : 1;
+}
 
 bool phase_run_op(const GateOp &op)
 {
@@ -830,6 +930,7 @@ int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m)
         }
         return 4;
     case F_DENSE1:
+    case F_DENSE1R:
     {
         double2 full[4];
         expand_dense(op, full);
@@ -1007,7 +1108,16 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
             {
                 // one changed sub-index: a phase on the amplitudes whose
                 // control and target bits all match
-                f.kind = F_PHASE;
+                const cplx e = op.mat[0];
+                if (e.re == -1.0 && e.im == 0.0)
+                    f.kind = F_NEG;
+                else if (e.re == 0.0 && (e.im == 1.0 || e.im == -1.0))
+                {
+                    f.kind = F_MULI;
+                    f.b1 = e.im < 0.0 ? 1 : 0;
+                }
+                else
+                    f.kind = F_PHASE;
                 for (int i = 0; i < op.nt; ++i)
                 {
                     cm |= 1ull << op.tq[i];
@@ -1018,20 +1128,24 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
             else if (op.diag)
             {
                 f.kind = F_DIAG;
-                for (int i = 0; i < op.nt; ++i)
+                for (int i = 0; i < 2; ++i)
                 {
+                    f.loc[i] = -1;
+                    f.spos[i] = -1;
+                    f.phys[i] = 0;
+                    if (i >= op.nt)
+                        continue;
+                    const int l = loc_of[op.tq[i]];
                     f.phys[i] = static_cast<uint8_t>(op.tq[i]);
-                    f.loc[i] = static_cast<int8_t>(loc_of[op.tq[i]]);
-                }
-                if (op.nt < 2)
-                {
-                    f.loc[1] = -1;
-                    f.phys[1] = 0;
+                    if (l >= 0 && ((bits >> l) & 1))
+                        f.spos[i] = static_cast<int8_t>(pos_in_stage[l]);
+                    else
+                        f.loc[i] = static_cast<int8_t>(l);
                 }
             }
             else if (op.nt == 1)
             {
-                f.kind = is_x(op) ? F_SWAP1 : F_DENSE1;
+                f.kind = is_x(op) ? F_SWAP1 : (is_real(op) ? F_DENSE1R : F_DENSE1);
                 f.b0 = static_cast<uint8_t>(pos_in_stage[loc_of[op.tq[0]]]);
             }
             else
@@ -1057,17 +1171,24 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
             nentries += ne;
             if (src)
                 src->push_back({pp.ops[oi], swapped});
-            uint32_t lcm = 0, lcv = 0;
+            uint32_t lcm = 0, lcv = 0, sm = 0, sv = 0;
             uint64_t gcm = 0, gcv = 0;
             for (int b = 0; b < n; ++b)
                 if ((cm >> b) & 1)
                 {
                     const bool v = (cv >> b) & 1;
-                    if (loc_of[b] >= 0)
+                    const int l = loc_of[b];
+                    if (l >= 0 && ((bits >> l) & 1))
                     {
-                        lcm |= 1u << loc_of[b];
+                        sm |= 1u << pos_in_stage[l];
                         if (v)
-                            lcv |= 1u << loc_of[b];
+                            sv |= 1u << pos_in_stage[l];
+                    }
+                    else if (l >= 0)
+                    {
+                        lcm |= 1u << l;
+                        if (v)
+                            lcv |= 1u << l;
                     }
                     else
                     {
@@ -1078,6 +1199,8 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                 }
             f.lcmask = lcm;
             f.lcval = lcv;
+            f.smask = static_cast<uint8_t>(sm);
+            f.sval = static_cast<uint8_t>(sv);
             f.gcmask = gcm;
             f.gcval = gcv;
                 }
@@ -1195,24 +1318,30 @@ int choose_local_bits(int n, int option)
 bool light_op(const GateOp &op) { return op.diag || is_x(op) || is_swap(op); }
 
 // Cost-model inputs of a pass: local qubits k, arithmetic (non-light) ops,
-// light ops, bytes per amplitude. None depends on the register size, so
-// timings recorded on small registers carry over to large ones.
-PassFeatures pass_features(int k, int heavy, int light, int amp_bytes)
+// light ops, and log2 of the number of chunks (n - k) capped at
+// kChunkFeatureCap. The chunk count decides how well a pass fills the GPU
+// (waves of CTAs, L2 residency of small registers); past 2^16 chunks a pass
+// streams and its time per amplitude no longer depends on it, which lets
+// timings from 24-qubit registers stand for 33-qubit ones. A model is
+// trained on registers of one amplitude type.
+constexpr float kChunkFeatureCap = 16.0f;
+
+PassFeatures pass_features(int k, int heavy, int light, int n)
 {
     PassFeatures f;
     f.f[0] = static_cast<float>(k);
     f.f[1] = static_cast<float>(heavy);
     f.f[2] = static_cast<float>(light);
-    f.f[3] = static_cast<float>(amp_bytes);
+    f.f[3] = std::min(static_cast<float>(n - k), kChunkFeatureCap);
     return f;
 }
 
-PassFeatures pass_features(const std::vector<GateOp> &q, const PlannedPass &pp, int amp_bytes)
+PassFeatures pass_features(const std::vector<GateOp> &q, const PlannedPass &pp, int n)
 {
     int light = 0;
     for (int oi : pp.ops)
         light += light_op(q[oi]) ? 1 : 0;
-    return pass_features(pp.k, (int)pp.ops.size() - light, light, amp_bytes);
+    return pass_features(pp.k, (int)pp.ops.size() - light, light, n);
 }
 
 uint64_t fill_local(uint64_t local, int n, int k)
@@ -1251,7 +1380,7 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
         while (gi < greedy.size() && greedy[gi].fused)
         {
             seq.insert(seq.end(), greedy[gi].pass.ops.begin(), greedy[gi].pass.ops.end());
-            greedy_feats.push_back(pass_features(q, greedy[gi].pass, amp_bytes));
+            greedy_feats.push_back(pass_features(q, greedy[gi].pass, n));
             ++gi;
         }
         const int L = (int)seq.size();
@@ -1288,7 +1417,7 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
                 for (int k = std::max(need, kmin); k <= kmax; ++k)
                 {
                     const int light = light_before[j] - light_before[i];
-                    const PassFeatures f = pass_features(k, j - i - light, light, amp_bytes);
+                    const PassFeatures f = pass_features(k, j - i - light, light, n);
                     cands.push_back({i, j, k, fill_local(d, n, k)});
                     feats.insert(feats.end(), f.f, f.f + 4);
                 }
@@ -1481,7 +1610,7 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         {
             if (timer.enabled)
             {
-                const PassFeatures f = pass_features(ops, pieces[i], amp_bytes);
+                const PassFeatures f = pass_features(ops, pieces[i], n);
                 timer.begin(stream_, KernelTimer::kFused, 2.0 * amp_bytes * std::ldexp(1.0, n), &f);
             }
             launches += c64 ? launch_fused_pass<float>(state, pieces[i].k, params[i], stream_)

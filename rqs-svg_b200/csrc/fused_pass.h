@@ -28,6 +28,9 @@ enum FKind : uint8_t
     F_PHASE = 4,   // multiply by entry 0 where the condition bits match
     F_DIAG = 5,    // diagonal on one or two targets anywhere
     F_TERM = 6,    // one factor of a phase stage (see fused_pass.cu)
+    F_DENSE1R = 7, // 2x2 with real entries (RY, H, real U3) on one stage bit
+    F_NEG = 8,     // F_PHASE by -1 (Z, CZ): sign flips, no multiplies
+    F_MULI = 9,    // F_PHASE by i (b1 = 0) or -i (b1 = 1) (S, Sdg): exchanges and sign flips
 };
 
 // One gate of a pass. Conditions: (local index & lcmask) == lcval and
@@ -42,10 +45,14 @@ struct FOp
     uint8_t kind;
     uint8_t nt;
     uint8_t b0, b1;         // stage-bit positions (dense kinds)
-    int8_t loc[2];          // F_DIAG: local bit of target i, -1 when outside Q
+    int8_t loc[2];          // F_DIAG: local bit of target i when it is not a stage bit, else -1
     uint8_t phys[2];        // F_DIAG: physical qubit of target i
     uint16_t moff;
-    uint16_t pad[3];
+    // register stages: the condition's stage bits, as bits of the amplitude
+    // slot r (lcmask/lcval then hold only the other local bits)
+    uint8_t smask, sval;
+    int8_t spos[2];         // F_DIAG: stage position of target i, -1 when not a stage bit
+    uint16_t pad;
 };
 static_assert(sizeof(FOp) == 40, "FOp layout");
 

@@ -13,6 +13,8 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <string>
+#include <unordered_map>
 
 namespace qcsb
 {
@@ -71,38 +73,62 @@ const GateInfo kGates[] = {
     {"xx_plus_yy", 2, 2}, {"xx_minus_yy", 2, 2}, {"rccx", 3, 0}, {"rcccx", 4, 0},
 };
 
-const GateInfo &lookup(const char *name)
+// ids: positions in kGates
+enum GateIdx
 {
-    for (const auto &gi : kGates)
-        if (std::strcmp(gi.name, name) == 0)
-            return gi;
-    throw std::runtime_error(strformat("unknown gate '%s'", name));
+    G_GLOBAL_PHASE, G_H, G_X, G_Y, G_Z, G_S, G_SDG, G_T, G_TDG, G_SX, G_RX, G_RY, G_RZ, G_U4, G_U3, G_U2, G_U1,
+    G_U, G_P, G_SWAP, G_ISWAP, G_ID, G_SXDG, G_R, G_RXX, G_RYY, G_RZZ, G_RZX, G_DCX, G_ECR, G_XX_PLUS_YY,
+    G_XX_MINUS_YY, G_RCCX, G_RCCCX, G_COUNT
+};
+static_assert(sizeof(kGates) / sizeof(kGates[0]) == G_COUNT, "gate table and ids");
+
+const GateInfo &info(int id)
+{
+    if (id < 0 || id >= G_COUNT)
+        throw std::runtime_error(strformat("unknown gate id %d", id));
+    return kGates[id];
 }
 
 } // namespace
 
-int gate_arity(const char *name) { return lookup(name).nt; }
-
-int gate_nparams(const char *name) { return lookup(name).np; }
-
-GateMatrix gate_matrix(const char *name, const double *p, int np)
+int gate_id(const char *name)
 {
-    const GateInfo &gi = lookup(name);
-    if (np != gi.np)
-        throw std::runtime_error(strformat("gate '%s' takes %d parameters, got %d", name, gi.np, np));
-    Builder b(gi.nt);
-    const std::string n(name);
+    static const std::unordered_map<std::string, int> ids = [] {
+        std::unordered_map<std::string, int> m;
+        for (int i = 0; i < G_COUNT; ++i)
+            m.emplace(kGates[i].name, i);
+        return m;
+    }();
+    const auto it = name ? ids.find(name) : ids.end();
+    if (it == ids.end())
+        throw std::runtime_error(strformat("unknown gate '%s'", name ? name : "(null)"));
+    return it->second;
+}
 
-    if (n == "global_phase")
+int gate_arity(int id) { return info(id).nt; }
+
+int gate_nparams(int id) { return info(id).np; }
+
+const char *gate_name(int id) { return info(id).name; }
+
+GateMatrix gate_matrix(int id, const double *p, int np)
+{
+    const GateInfo &gi = info(id);
+    if (np != gi.np)
+        throw std::runtime_error(strformat("gate '%s' takes %d parameters, got %d", gi.name, gi.np, np));
+    Builder b(gi.nt);
+    const int n = id;
+
+    if (n == G_GLOBAL_PHASE)
     {
         b.set(0, 0, cexpi(p[0]));
     }
-    else if (n == "u4" || n == "u3" || n == "u")
+    else if (n == G_U4 || n == G_U3 || n == G_U)
     {
         const double theta = p[0], phi = p[1], lambda = p[2];
         const double c = std::cos(0.5 * theta), s = std::sin(0.5 * theta);
         const cplx e_phi = cexpi(phi), e_lambda = cexpi(lambda);
-        if (n == "u4")
+        if (n == G_U4)
         {
             // e^{i gamma} [[c, -s e^{i lambda}], [e^{i phi} s, e^{i phi} e^{i lambda} c]]
             const cplx e_gamma = cexpi(p[3]);
@@ -120,7 +146,7 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
             b.set(1, 1, cscale(c, cexpi(phi + lambda)));
         }
     }
-    else if (n == "u2")
+    else if (n == G_U2)
     {
         const cplx e_phi = cexpi(p[0]), e_lambda = cexpi(p[1]);
         b.set(0, 0, C(kRsqrt2));
@@ -128,61 +154,61 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(1, 0, cscale(kRsqrt2, e_phi));
         b.set(1, 1, cscale(kRsqrt2, cexpi(p[0] + p[1])));
     }
-    else if (n == "u1" || n == "p")
+    else if (n == G_U1 || n == G_P)
     {
         b.set(1, 1, cexpi(p[0]));
     }
-    else if (n == "h")
+    else if (n == G_H)
     {
         b.set(0, 0, C(kRsqrt2));
         b.set(0, 1, C(kRsqrt2));
         b.set(1, 0, C(kRsqrt2));
         b.set(1, 1, C(-kRsqrt2));
     }
-    else if (n == "x")
+    else if (n == G_X)
     {
         b.set(0, 0, C(0));
         b.set(0, 1, C(1));
         b.set(1, 0, C(1));
         b.set(1, 1, C(0));
     }
-    else if (n == "y")
+    else if (n == G_Y)
     {
         b.set(0, 0, C(0));
         b.set(0, 1, C(0, -1));
         b.set(1, 0, C(0, 1));
         b.set(1, 1, C(0));
     }
-    else if (n == "z")
+    else if (n == G_Z)
     {
         b.set(1, 1, C(-1));
     }
-    else if (n == "s")
+    else if (n == G_S)
     {
         b.set(1, 1, C(0, 1));
     }
-    else if (n == "sdg")
+    else if (n == G_SDG)
     {
         b.set(1, 1, C(0, -1));
     }
-    else if (n == "t")
+    else if (n == G_T)
     {
         b.set(1, 1, C(kRsqrt2, kRsqrt2));
     }
-    else if (n == "tdg")
+    else if (n == G_TDG)
     {
         b.set(1, 1, C(kRsqrt2, -kRsqrt2));
     }
-    else if (n == "sx" || n == "sxdg")
+    else if (n == G_SX || n == G_SXDG)
     {
         // sx = 1/2 [[1+i, 1-i], [1-i, 1+i]]; sxdg is its conjugate.
-        const double sg = (n == "sx") ? 1.0 : -1.0;
+        const double sg = (n == G_SX) ? 1.0 : -1.0;
         b.set(0, 0, C(0.5, 0.5 * sg));
         b.set(0, 1, C(0.5, -0.5 * sg));
         b.set(1, 0, C(0.5, -0.5 * sg));
         b.set(1, 1, C(0.5, 0.5 * sg));
     }
-    else if (n == "rx")
+    else if (n == G_RX)
     {
         const double c = std::cos(0.5 * p[0]), s = std::sin(0.5 * p[0]);
         b.set(0, 0, C(c));
@@ -190,7 +216,7 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(1, 0, C(0, -s));
         b.set(1, 1, C(c));
     }
-    else if (n == "ry")
+    else if (n == G_RY)
     {
         const double c = std::cos(0.5 * p[0]), s = std::sin(0.5 * p[0]);
         b.set(0, 0, C(c));
@@ -198,17 +224,17 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(1, 0, C(s));
         b.set(1, 1, C(c));
     }
-    else if (n == "rz")
+    else if (n == G_RZ)
     {
         const double c = std::cos(0.5 * p[0]), s = std::sin(0.5 * p[0]);
         b.set(0, 0, C(c, -s));
         b.set(1, 1, C(c, s));
     }
-    else if (n == "id")
+    else if (n == G_ID)
     {
         // identity
     }
-    else if (n == "r")
+    else if (n == G_R)
     {
         // [[c, -i s e^{-i phi}], [-i s e^{i phi}, c]]
         const double c = std::cos(0.5 * p[0]), s = std::sin(0.5 * p[0]);
@@ -218,21 +244,21 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(1, 0, cscale(-s, mul_i(C(cp, sp))));
         b.set(1, 1, C(c));
     }
-    else if (n == "swap")
+    else if (n == G_SWAP)
     {
         b.set(1, 1, C(0));
         b.set(2, 2, C(0));
         b.set(1, 2, C(1));
         b.set(2, 1, C(1));
     }
-    else if (n == "iswap")
+    else if (n == G_ISWAP)
     {
         b.set(1, 1, C(0));
         b.set(2, 2, C(0));
         b.set(1, 2, C(0, 1));
         b.set(2, 1, C(0, 1));
     }
-    else if (n == "rzz")
+    else if (n == G_RZZ)
     {
         const double c = std::cos(0.5 * p[0]), s = std::sin(0.5 * p[0]);
         b.set(0, 0, C(c, -s));
@@ -240,11 +266,11 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(2, 2, C(c, s));
         b.set(3, 3, C(c, -s));
     }
-    else if (n == "rxx" || n == "ryy")
+    else if (n == G_RXX || n == G_RYY)
     {
         // diagonal c; anti-diagonal -i s, except ryy's 00<->11 entries (+i s).
         const double c = std::cos(0.5 * p[0]), s = std::sin(0.5 * p[0]);
-        const double outer = (n == "rxx") ? -s : s;
+        const double outer = (n == G_RXX) ? -s : s;
         for (int k = 0; k < 4; ++k)
             b.set(k, k, C(c));
         b.set(0, 3, C(0, outer));
@@ -252,7 +278,7 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(1, 2, C(0, -s));
         b.set(2, 1, C(0, -s));
     }
-    else if (n == "rzx")
+    else if (n == G_RZX)
     {
         const double c = std::cos(0.5 * p[0]), s = std::sin(0.5 * p[0]);
         for (int k = 0; k < 4; ++k)
@@ -262,20 +288,20 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(1, 3, C(0, s));
         b.set(3, 1, C(0, s));
     }
-    else if (n == "xx_plus_yy" || n == "xx_minus_yy")
+    else if (n == G_XX_PLUS_YY || n == G_XX_MINUS_YY)
     {
         // acts on {01, 10} (plus) or {00, 11} (minus):
         // [[c, -i s e^{-i beta}], [-i s e^{i beta}, c]]
         const double c = std::cos(0.5 * p[0]), s = std::sin(0.5 * p[0]);
         const double cb = std::cos(p[1]), sb = std::sin(p[1]);
-        const int lo = (n == "xx_plus_yy") ? 1 : 0;
-        const int hi = (n == "xx_plus_yy") ? 2 : 3;
+        const int lo = (n == G_XX_PLUS_YY) ? 1 : 0;
+        const int hi = (n == G_XX_PLUS_YY) ? 2 : 3;
         b.set(lo, lo, C(c));
         b.set(hi, hi, C(c));
         b.set(lo, hi, cscale(-s, mul_i(C(cb, -sb))));
         b.set(hi, lo, cscale(-s, mul_i(C(cb, sb))));
     }
-    else if (n == "dcx")
+    else if (n == G_DCX)
     {
         // 01 <- 11, 10 <- 01, 11 <- 10
         for (int k = 1; k < 4; ++k)
@@ -284,7 +310,7 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(2, 1, C(1));
         b.set(3, 2, C(1));
     }
-    else if (n == "ecr")
+    else if (n == G_ECR)
     {
         const double r = kRsqrt2;
         for (int k = 0; k < 4; ++k)
@@ -298,7 +324,7 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(3, 0, mul_mi(C(r)));
         b.set(3, 2, C(r));
     }
-    else if (n == "rccx")
+    else if (n == G_RCCX)
     {
         // 011 <- -i 111, 101 <- -101, 111 <- i 011
         b.set(3, 3, C(0));
@@ -307,7 +333,7 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
         b.set(5, 5, C(-1));
         b.set(7, 3, C(0, 1));
     }
-    else if (n == "rcccx")
+    else if (n == G_RCCCX)
     {
         // 0011 <- i 0011, 0111 <- 1111, 1011 <- -i 1011, 1111 <- -0111
         b.set(3, 3, C(0, 1));
@@ -319,7 +345,7 @@ GateMatrix gate_matrix(const char *name, const double *p, int np)
     }
     else
     {
-        throw std::runtime_error(strformat("gate '%s' has no matrix", name));
+        throw std::runtime_error(strformat("gate '%s' has no matrix", gi.name));
     }
     return b.g;
 }
@@ -351,7 +377,11 @@ GateOp make_gate_op(const GateMatrix &g, const int *tq, uint64_t cmask, uint64_t
         for (int k = 0; k < d && !active; ++k)
             active = !is_id(s, k) || !is_id(k, s);
         if (active)
+        {
+            if (op.na == kMaxActive)
+                throw std::runtime_error("gate changes more than four sub-indices");
             op.act[op.na++] = static_cast<uint8_t>(s);
+        }
     }
     bool diag = true;
     for (int a = 0; a < op.na && diag; ++a)

@@ -249,47 +249,8 @@ int launch_plain_dispatch(typename Cx<R>::T *state, int n, const GateOp &op, cud
     case 2: return launch_plain_na<R, 2, DIAG>(state, n, op, stream);
     case 3: return launch_plain_na<R, 3, DIAG>(state, n, op, stream);
     case 4: return launch_plain_na<R, 4, DIAG>(state, n, op, stream);
-    case 5: return launch_plain_na<R, 5, DIAG>(state, n, op, stream);
-    case 6: return launch_plain_na<R, 6, DIAG>(state, n, op, stream);
-    case 7: return launch_plain_na<R, 7, DIAG>(state, n, op, stream);
-    case 8: return launch_plain_na<R, 8, DIAG>(state, n, op, stream);
-    case 16: return launch_plain_na<R, 16, DIAG>(state, n, op, stream);
-    default: break;
+    default: throw std::runtime_error(strformat("internal: %d active sub-indices", op.na));
     }
-    // 9..15 active sub-indices: pad with inactive sub-indices (identity
-    // rows/columns), which exist because na < 2^nt.
-    GateOp padded = op;
-    const int d = 1 << op.nt;
-    const int na = op.na;
-    bool used[kMaxSub] = {};
-    for (int a = 0; a < na; ++a)
-        used[op.act[a]] = true;
-    int k = na;
-    for (int s = 0; s < d && k < 16; ++s)
-        if (!used[s])
-            padded.act[k++] = static_cast<uint8_t>(s);
-    if (k != 16)
-        throw std::runtime_error("internal: cannot pad gate operation");
-    padded.na = 16;
-    if (DIAG)
-    {
-        for (int a = na; a < 16; ++a)
-            padded.mat[a] = cplx{1.0, 0.0};
-    }
-    else
-    {
-        for (int a = 0; a < 16; ++a)
-            for (int b = 0; b < 16; ++b)
-            {
-                cplx v{0.0, 0.0};
-                if (a < na && b < na)
-                    v = op.mat[a * na + b];
-                else if (a == b)
-                    v = cplx{1.0, 0.0};
-                padded.mat[a * 16 + b] = v;
-            }
-    }
-    return launch_plain_na<R, 16, DIAG>(state, n, padded, stream);
 }
 
 // ------------------------------------------------------------ preparation
@@ -331,10 +292,44 @@ struct ProbParams
     int nops;
     uint64_t masks[kMaxOps];
     double2 *partials;
+    double2 *result;      // final (P0, P1); may be mapped host memory
+    unsigned *ticket;     // zero between calls
 };
 
+// Fixed-order sum of count double2 partials by one block of kThreads threads
+// (the same order in every call, so repeated measurements agree bit for bit).
+__device__ __forceinline__ double2 block_sum_partials(const double2 *partials, int count)
+{
+    double s0 = 0.0, s1 = 0.0;
+    for (int i = threadIdx.x; i < count; i += kThreads)
+    {
+        const double2 v = __ldcg(partials + i);
+        s0 += v.x;
+        s1 += v.y;
+    }
+    __shared__ double sh[2][kThreads / 32];
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    if (l == 0)
+    {
+        sh[0][w] = s0;
+        sh[1][w] = s1;
+    }
+    __syncthreads();
+    double t0 = 0.0, t1 = 0.0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kThreads / 32; ++k)
+        {
+            t0 += sh[0][k];
+            t1 += sh[1][k];
+        }
+    return make_double2(t0, t1);
+}
+
 // Per-block (sum |a0|^2, sum |a1|^2) over the groups; fixed reduction order,
-// so repeated calls give identical sums.
+// so repeated calls give identical sums. The last block to finish adds the
+// per-block partials and writes (P0, P1) to p.result.
 template <typename R>
 __global__ void __launch_bounds__(kThreads) measure_probs_kernel(const __grid_constant__ ProbParams<R> p)
 {
@@ -364,39 +359,23 @@ __global__ void __launch_bounds__(kThreads) measure_probs_kernel(const __grid_co
             t1 += sh[1][k];
         }
         p.partials[blockIdx.x] = make_double2(t0, t1);
+        __threadfence();
+    }
+    __shared__ bool last;
+    if (threadIdx.x == 0)
+        last = atomicAdd(p.ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    const double2 total = block_sum_partials(p.partials, gridDim.x);
+    if (threadIdx.x == 0)
+    {
+        *p.result = total;
+        *p.ticket = 0;
     }
 }
 
-// Sums count double2 partials in a fixed order into *out (one block).
-__global__ void __launch_bounds__(kThreads) sum_partials2_kernel(const double2 *partials, int count, double2 *out)
-{
-    double s0 = 0.0, s1 = 0.0;
-    for (int i = threadIdx.x; i < count; i += kThreads)
-    {
-        s0 += partials[i].x;
-        s1 += partials[i].y;
-    }
-    __shared__ double sh[2][kThreads / 32];
-    s0 = warp_sum(s0);
-    s1 = warp_sum(s1);
-    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
-    if (l == 0)
-    {
-        sh[0][w] = s0;
-        sh[1][w] = s1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        double t0 = 0.0, t1 = 0.0;
-        for (int k = 0; k < kThreads / 32; ++k)
-        {
-            t0 += sh[0][k];
-            t1 += sh[1][k];
-        }
-        *out = make_double2(t0, t1);
-    }
-}
 
 template <typename V>
 __global__ void collapse_kernel(V *state, uint64_t ngroups, uint64_t lowmask, uint64_t zero_bit)
@@ -701,7 +680,7 @@ int launch_set_amplitude(typename Cx<R>::T *state, uint64_t index, double re, do
 
 template <typename R>
 int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t cmask, uint64_t cval,
-                         double2 *partials, double2 *result, cudaStream_t stream)
+                         double2 *partials, double2 *result, unsigned *ticket, cudaStream_t stream)
 {
     ProbParams<R> p;
     std::memset(&p, 0, sizeof(p));
@@ -715,12 +694,12 @@ int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t 
     p.cval = cval;
     p.tbit = 1ull << t;
     p.partials = partials;
+    p.result = result;
+    p.ticket = ticket;
     // A fixed grid (independent of n) keeps the partial count constant.
     measure_probs_kernel<R><<<kReduceBlocks, kThreads, 0, stream>>>(p);
     QCSB_CUDA(cudaGetLastError());
-    sum_partials2_kernel<<<1, kThreads, 0, stream>>>(partials, kReduceBlocks, result);
-    QCSB_CUDA(cudaGetLastError());
-    return 2;
+    return 1;
 }
 
 template <typename R>
@@ -812,7 +791,7 @@ int launch_narrow(const double2 *in, uint64_t count, typename Cx<R>::T *out, cud
     template int launch_init_sequential<R>(Cx<R>::T *, int, cudaStream_t);                                          \
     template int launch_set_amplitude<R>(Cx<R>::T *, uint64_t, double, double, cudaStream_t);                      \
     template int launch_measure_probs<R>(const Cx<R>::T *, int, int, uint64_t, uint64_t, double2 *, double2 *,      \
-                                         cudaStream_t);                                                             \
+                                         unsigned *, cudaStream_t);                                                 \
     template int launch_collapse<R>(Cx<R>::T *, int, int, int, cudaStream_t);                                       \
     template int launch_zsums<R>(const Cx<R>::T *, int, double *, double *, cudaStream_t);                          \
     template int launch_gather_logical<R>(const Cx<R>::T *, int, const int *, uint64_t, uint64_t, double2 *,        \

@@ -18,6 +18,9 @@ constexpr int kMaxQubits = 40;
 // Most targets one gate operation may carry (API gates use <= 4).
 constexpr int kMaxTargets = 4;
 constexpr int kMaxSub = 1 << kMaxTargets;
+// Most sub-indices one API gate changes: 4 (two-target gates, and rcccx's
+// 0011/0111/1011/1111); rccx changes 3, one-target gates 2.
+constexpr int kMaxActive = 4;
 
 std::string strformat(const char *fmt, ...);
 
@@ -56,8 +59,8 @@ struct GateOp
     uint64_t cval = 0;
     bool diag = false;
     int na = 0;
-    uint8_t act[kMaxSub] = {};
-    cplx mat[kMaxSub * kMaxSub] = {};   // na*na (dense) or na (diag) entries used
+    uint8_t act[kMaxActive] = {};
+    cplx mat[kMaxActive * kMaxActive];   // na*na (dense) or na (diag) entries used
     // Number of amplitudes this gate can change in a 2^n register: the
     // algorithmic unit of work (2 * bytes_per_amp * changed amps per gate).
     double changed_amps(int n) const;
@@ -67,14 +70,23 @@ struct GateOp
 struct GateMatrix
 {
     int nt = 0;
-    cplx m[kMaxSub * kMaxSub] = {};
+    cplx m[kMaxSub * kMaxSub];   // the first 2^nt x 2^nt entries are set
 };
 
-// Builds the matrix of a named gate of the reference API. Throws on unknown
-// names or a wrong parameter count.
-GateMatrix gate_matrix(const char *name, const double *params, int nparams);
-int gate_arity(const char *name);
-int gate_nparams(const char *name);
+// Gates of the reference API by id (index into the gate table); the name
+// lookup throws on unknown names.
+int gate_id(const char *name);
+int gate_arity(int id);
+int gate_nparams(int id);
+const char *gate_name(int id);
+// Builds the matrix of a gate. Throws on a wrong parameter count.
+GateMatrix gate_matrix(int id, const double *params, int nparams);
+inline GateMatrix gate_matrix(const char *name, const double *params, int nparams)
+{
+    return gate_matrix(gate_id(name), params, nparams);
+}
+inline int gate_arity(const char *name) { return gate_arity(gate_id(name)); }
+inline int gate_nparams(const char *name) { return gate_nparams(gate_id(name)); }
 
 // Reduce a dense matrix on targets tq to a GateOp (active set + diag flag).
 GateOp make_gate_op(const GateMatrix &g, const int *tq, uint64_t cmask, uint64_t cval);
@@ -113,12 +125,14 @@ template <typename R>
 int launch_set_amplitude(typename Cx<R>::T *state, uint64_t index, double re, double im, cudaStream_t stream);
 
 // Squared-norm sums (P0, P1) of target qubit t over the subspace where
-// (index & cmask) == cval. partials must hold kReduceBlocks double2;
-// result receives one double2 on the device.
+// (index & cmask) == cval, in one launch. partials must hold kReduceBlocks
+// double2; result receives one double2 (device memory, or pinned host memory
+// the device can write); ticket is a device counter that must be zero before
+// the call and is zero again after it.
 constexpr int kReduceBlocks = 592;   // 4 x 148 SMs
 template <typename R>
 int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t cmask, uint64_t cval,
-                         double2 *partials, double2 *result, cudaStream_t stream);
+                         double2 *partials, double2 *result, unsigned *ticket, cudaStream_t stream);
 
 // Zero every amplitude whose bit t differs from keep_value.
 template <typename R>

@@ -144,6 +144,8 @@ void Simulator::allocate_memory()
     reinitialize_mapping();
     QCSB_CUDA(cudaMalloc(&red_partials_, sizeof(double2) * kReduceBlocks));
     QCSB_CUDA(cudaMalloc(&red_result_, sizeof(double2)));
+    QCSB_CUDA(cudaMalloc(&red_ticket_, sizeof(unsigned)));
+    QCSB_CUDA(cudaMemset(red_ticket_, 0, sizeof(unsigned)));
     QCSB_CUDA(cudaMalloc(&zsum_partials_, sizeof(double) * 512 * (kMaxQubits + 1)));
     QCSB_CUDA(cudaMalloc(&zsum_result_, sizeof(double) * (kMaxQubits + 1)));
     host_pinned_bytes_ = 1 << 16;
@@ -190,6 +192,8 @@ void Simulator::dispose()
     cudaFree(state_);
     cudaFree(red_partials_);
     cudaFree(red_result_);
+    cudaFree(red_ticket_);
+    red_ticket_ = nullptr;
     cudaFree(zsum_partials_);
     cudaFree(zsum_result_);
     cudaFree(staging_dev_);
@@ -276,58 +280,62 @@ bool Simulator::identity_mapping() const
     return true;
 }
 
-void Simulator::apply_gate(const char *name, const double *params, int nparams,
-                           const std::vector<int> &targets, const std::vector<int> &negctrls,
-                           const std::vector<int> &ctrls)
+void Simulator::apply_gate(const char *name, const double *params, int nparams, const int *targets, int ntargets,
+                           const int *negctrls, int nneg, const int *ctrls, int nctrl)
 {
     require_allocated("gate");
     ++stats.gates_received;
-    const int arity = gate_arity(name);
-    if ((int)targets.size() != arity)
-        throw std::runtime_error(strformat("gate %s takes %d target qubits, got %d", name, arity, (int)targets.size()));
+    const int id = gate_id(name);
+    const int arity = gate_arity(id);
+    if (ntargets != arity)
+        throw std::runtime_error(strformat("gate %s takes %d target qubits, got %d", name, arity, ntargets));
     uint64_t seen = 0;
-    auto claim = [&](int q, const char *role) {
-        check_qubit(q, role);
-        if ((seen >> q) & 1)
-            throw std::runtime_error(strformat("gate %s: qubit %d appears more than once among targets and controls", name, q));
-        seen |= 1ull << q;
+    auto claim = [&](const int *qs, int count, const char *role) {
+        uint64_t mask = 0;
+        for (int i = 0; i < count; ++i)
+        {
+            const int q = qs[i];
+            check_qubit(q, role);
+            if ((seen >> q) & 1)
+                throw std::runtime_error(
+                    strformat("gate %s: qubit %d appears more than once among targets and controls", name, q));
+            seen |= 1ull << q;
+            mask |= 1ull << q;
+        }
+        return mask;
     };
-    for (int q : targets)
-        claim(q, "target");
-    for (int q : negctrls)
-        claim(q, "negative control");
-    for (int q : ctrls)
-        claim(q, "control");
-    const GateMatrix gm = gate_matrix(name, params, nparams);
+    const uint64_t tmask = claim(targets, ntargets, "target");
+    uint64_t ctl[2] = {claim(negctrls, nneg, "negative control"), claim(ctrls, nctrl, "control")};
+    const GateMatrix gm = gate_matrix(id, params, nparams);
 
     // Measured qubits that are not targets become controls on their measured
     // value; a contradicting explicit control cancels the gate
     // (reference prepare_control_qubit_num_list, src/qcs.cu:2161-2204).
-    std::vector<int> ctrl_lists[2] = {negctrls, ctrls};
-    std::vector<int> keep[2];
-    const std::vector<int> *measured[2] = {&measured0_, &measured1_};
+    std::vector<int> *measured[2] = {&measured0_, &measured1_};
     bool condition = true;
     for (int v = 0; v < 2; ++v)
         for (int q : *measured[v])
         {
-            if (contains(targets, q))
+            const uint64_t bit = 1ull << q;
+            if (tmask & bit)
                 continue;   // a gate on a measured qubit makes it unmeasured
-            keep[v].push_back(q);
-            const bool same = contains(ctrl_lists[v], q);
-            const bool other = contains(ctrl_lists[1 - v], q);
-            if (!same && !other)
-                ctrl_lists[v].push_back(q);
-            else if (other)
+            if (ctl[1 - v] & bit)
                 condition = false;
+            else
+                ctl[v] |= bit;
         }
     if (!condition)
         return;   // measured lists are left as they were (src/qcs.cu:2689-2691)
+    for (int v = 0; v < 2; ++v)
+        measured[v]->erase(std::remove_if(measured[v]->begin(), measured[v]->end(),
+                                          [&](int q) { return (tmask >> q) & 1; }),
+                           measured[v]->end());
 
     uint64_t cmask = 0, cval = 0;
     for (int v = 0; v < 2; ++v)
-        for (int q : ctrl_lists[v])
+        for (uint64_t m = ctl[v]; m; m &= m - 1)
         {
-            const int p = perm_l2p_[q];
+            const int p = perm_l2p_[__builtin_ctzll(m)];
             cmask |= 1ull << p;
             if (v)
                 cval |= 1ull << p;
@@ -337,13 +345,9 @@ void Simulator::apply_gate(const char *name, const double *params, int nparams,
         tq[i] = perm_l2p_[targets[i]];
     const GateOp op = make_gate_op(gm, tq, cmask, cval);
 
-    measured0_ = keep[0];
-    measured1_ = keep[1];
-
     if (op.na == 0)
         return;   // identity on every amplitude
-    if (fusion_mode_ != QCS_FUSION_PLAIN && arity == 2 && negctrls.empty() && ctrls.empty() &&
-        std::strcmp(name, "swap") == 0)
+    if (fusion_mode_ != QCS_FUSION_PLAIN && arity == 2 && nneg == 0 && nctrl == 0 && std::strcmp(name, "swap") == 0)
     {
         // An uncontrolled SWAP exchanges which physical bits hold the two
         // logical qubits: exact, and no data moves. Implicit controls from
@@ -412,9 +416,9 @@ int Simulator::measure(int q)
         cval |= 1ull << perm_l2p_[m];
     }
     const int t = perm_l2p_[q];
-    stats.kernel_launches += QCSB_ON_STATE(launch_measure_probs, n_, t, cmask, cval, red_partials_, red_result_, stream_);
+    // (P0, P1) lands directly in pinned host memory
     double2 *h = static_cast<double2 *>(host_pinned_);
-    QCSB_CUDA(cudaMemcpyAsync(h, red_result_, sizeof(double2), cudaMemcpyDeviceToHost, stream_));
+    stats.kernel_launches += QCSB_ON_STATE(launch_measure_probs, n_, t, cmask, cval, red_partials_, h, red_ticket_, stream_);
     QCSB_CUDA(cudaStreamSynchronize(stream_));
     const double p0 = h->x, p1 = h->y;
     const double sum = p0 + p1;
@@ -446,7 +450,7 @@ void Simulator::reset_qubit(int q)
 {
     // reference qcs_simulator_reset_cxx, src/qcs.cu:3077-3081
     if (measure(q))
-        apply_gate("x", nullptr, 0, {q}, {}, {});
+        apply_gate("x", nullptr, 0, &q, 1, nullptr, 0, nullptr, 0);
 }
 
 void Simulator::clear_measurement_state()

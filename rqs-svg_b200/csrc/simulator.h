@@ -15,7 +15,7 @@ class CostModel;
 
 // Features of one fused pass, the cost model's inputs: local qubits k,
 // arithmetic ops (complex multiply-adds per amplitude), light ops (diagonal
-// phases and permutations), bytes per amplitude.
+// phases and permutations), log2 of the chunk count (capped at 16).
 struct PassFeatures
 {
     float f[4];
@@ -84,9 +84,8 @@ class Simulator
     int fusion() const { return fusion_mode_; }
 
     // A gate call of the C API, on logical qubits.
-    void apply_gate(const char *name, const double *params, int nparams,
-                    const std::vector<int> &targets, const std::vector<int> &negctrls,
-                    const std::vector<int> &ctrls);
+    void apply_gate(const char *name, const double *params, int nparams, const int *targets, int ntargets,
+                    const int *negctrls, int nneg, const int *ctrls, int nctrl);
 
     int measure(int qubit);
     void reset_qubit(int qubit);
@@ -166,6 +165,7 @@ class Simulator
     // chunk staging for logical-order transfers, sampler tree
     double2 *red_partials_ = nullptr;
     double2 *red_result_ = nullptr;
+    unsigned *red_ticket_ = nullptr;   // last-block counter of the measurement reduction
     double *zsum_partials_ = nullptr;
     double *zsum_result_ = nullptr;
     void *host_pinned_ = nullptr;

@@ -1,11 +1,13 @@
 """Self-recorded pass timings and training of the learned cost model.
 
 The simulator times every fused pass it launches while kernel timing is on
-(features: local qubits, arithmetic ops, light ops -- diagonal phases and
-permutations -- and bytes per amplitude; none depends on the register size,
-so timings from small registers carry over to large ones). `collect_pass_timings` runs seeded random circuits with varied
-pass sizes to gather many such samples; `train_cost_model` fits the MLP on
-log(ns per amplitude) with the library's own CUDA kernels.
+(features: local qubits k, arithmetic ops, light ops -- diagonal phases and
+permutations -- and log2 of the chunk count n - k, capped at 16, beyond which
+passes stream and the count no longer matters). `collect_pass_timings` runs
+seeded random circuits with varied pass sizes on registers of several sizes
+to gather many such samples; `train_cost_model` fits the MLP on log(ns per
+amplitude) with the library's own CUDA kernels. A model is trained on one
+amplitude type.
 """
 
 from __future__ import annotations
@@ -20,9 +22,18 @@ from . import circuits as C
 _MIX = ["u3", "x", "h", "rz", "p", "ry", "swap", "rzz", "rxx", "sx"]
 
 
-def collect_pass_timings(lib: Library, n: int, min_samples: int, seed: int = 1, max_rounds: int = 100000,
+def collect_pass_timings(lib: Library, n, min_samples: int, seed: int = 1, max_rounds: int = 100000,
                          precision: int = 128):
-    """Return (features [N x 4] float32, target [N] float32 = log(ns/amp))."""
+    """Return (features [N x 4] float32, target [N] float32 = log(ns/amp)),
+    recorded on registers of n qubits (an int or a list of sizes, which share
+    the samples equally)."""
+    sizes = [n] if isinstance(n, int) else list(n)
+    per = -(-min_samples // len(sizes))
+    parts = [_collect(lib, m, per, seed + i, max_rounds, precision) for i, m in enumerate(sizes)]
+    return np.concatenate([p[0] for p in parts]), np.concatenate([p[1] for p in parts])
+
+
+def _collect(lib: Library, n: int, min_samples: int, seed: int, max_rounds: int, precision: int):
     rng = np.random.default_rng(seed)
     feats, targets = [], []
     total = 0
@@ -31,7 +42,7 @@ def collect_pass_timings(lib: Library, n: int, min_samples: int, seed: int = 1, 
         rounds = 0
         while total < min_samples and rounds < max_rounds:
             rounds += 1
-            max_ops = int(rng.integers(1, 65))
+            max_ops = int(rng.integers(1, 257))
             local = int(rng.integers(9, 12))
             sim.set_planner_options(max_ops, local)
             gates = list(rng.choice(_MIX, size=int(rng.integers(2, len(_MIX) + 1)), replace=False))

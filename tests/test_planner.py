@@ -61,7 +61,7 @@ def test_pass_timings_and_learned_plans_keep_results_exact(gpu_lib, oracle_lib):
     feats, target = planner.collect_pass_timings(gpu_lib, n, min_samples=1500, seed=4)
     assert len(target) >= 1500
     assert np.all(feats[:, 0] >= 9) and np.all(feats[:, 0] <= 11)
-    assert np.all(feats[:, 3] == 16)
+    assert np.all(feats[:, 3] == n - feats[:, 0])   # log2 of the chunk count
     model, loss = planner.train_cost_model(gpu_lib, feats, target, epochs=40)
     try:
         assert loss < 1.0
