@@ -65,8 +65,10 @@ struct FStage
     uint8_t sbits[kStageBits];   // local bit positions of the stage, ascending
     uint16_t op_begin, op_end;
     uint8_t kind;
-    uint8_t pad[3];
+    uint8_t pad;
+    uint16_t monomials;          // phase stages: bit m set when a term has monomial m
 };
+static_assert(sizeof(FStage) == 12, "FStage layout");
 
 // Kernel parameters of one pass (passed as a __grid_constant__ block, under
 // the 32 KiB kernel parameter limit).

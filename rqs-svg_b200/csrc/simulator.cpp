@@ -143,7 +143,6 @@ void Simulator::allocate_memory()
         perm_p2l_[q] = perm_l2p_[q] = ref_l2p_[q] = q;
     reinitialize_mapping();
     QCSB_CUDA(cudaMalloc(&red_partials_, sizeof(double2) * kReduceBlocks));
-    QCSB_CUDA(cudaMalloc(&red_result_, sizeof(double2)));
     QCSB_CUDA(cudaMalloc(&red_ticket_, sizeof(unsigned)));
     QCSB_CUDA(cudaMemset(red_ticket_, 0, sizeof(unsigned)));
     QCSB_CUDA(cudaMalloc(&zsum_partials_, sizeof(double) * 512 * (kMaxQubits + 1)));
@@ -191,7 +190,6 @@ void Simulator::dispose()
     fused_ = nullptr;
     cudaFree(state_);
     cudaFree(red_partials_);
-    cudaFree(red_result_);
     cudaFree(red_ticket_);
     red_ticket_ = nullptr;
     cudaFree(zsum_partials_);
@@ -202,7 +200,7 @@ void Simulator::dispose()
     if (staging_host_)
         cudaFreeHost(staging_host_);
     state_ = nullptr;
-    red_partials_ = red_result_ = staging_dev_ = staging_host_ = nullptr;
+    red_partials_ = staging_dev_ = staging_host_ = nullptr;
     zsum_partials_ = zsum_result_ = nullptr;
     host_pinned_ = nullptr;
     for (cudaEvent_t e : events_)

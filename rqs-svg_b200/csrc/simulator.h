@@ -164,7 +164,6 @@ class Simulator
     // scratch: reduction partials and results, pinned host mirror,
     // chunk staging for logical-order transfers, sampler tree
     double2 *red_partials_ = nullptr;
-    double2 *red_result_ = nullptr;
     unsigned *red_ticket_ = nullptr;   // last-block counter of the measurement reduction
     double *zsum_partials_ = nullptr;
     double *zsum_result_ = nullptr;
@@ -185,7 +184,7 @@ class FusedExecutor
     int run(void *state, int n, int amp_bytes, const std::vector<GateOp> &ops, int mode, qcs_b200_stats &stats,
             KernelTimer &timer);
 
-    // Planner knobs: 0 keeps the default (64 gates per pass, 11 local qubits).
+    // Planner knobs: 0 keeps the default (256 gates per pass, 11 local qubits).
     void set_options(int max_ops, int local_bits)
     {
         max_ops_ = max_ops;

@@ -12,8 +12,6 @@ amplitude type.
 
 from __future__ import annotations
 
-import math
-
 import numpy as np
 
 from . import FUSION_GREEDY, CostModel, Library, Simulator
@@ -79,4 +77,4 @@ def relative_error(model: CostModel, features, targets) -> float:
     return float(np.median(np.abs(np.exp(pred - np.asarray(targets, np.float64)) - 1.0)))
 
 
-__all__ = ["collect_pass_timings", "train_cost_model", "predicted_pass_ms", "relative_error", "math"]
+__all__ = ["collect_pass_timings", "train_cost_model", "predicted_pass_ms", "relative_error"]
