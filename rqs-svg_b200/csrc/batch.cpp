@@ -242,7 +242,8 @@ void Batch::plan_group(Group &g, int k)
             if (off > 0xffffu)
                 throw std::runtime_error("batch: too many gate entries in one circuit");
             op.moff = static_cast<uint16_t>(off);
-            off += fop_entries(g.shape[p.src[f].op], op, p.src[f].swapped, scratch);
+            off += quad_kind(op.kind) ? quad_entries(g.shape, p.src[f], scratch)
+                                      : fop_entries(g.shape[p.src[f].op], op, p.src[f].swapped, scratch);
         }
     }
     g.stride = off;
@@ -291,7 +292,13 @@ void Batch::fill_group_range(const Group &g, size_t first, size_t last)
         double2 *block = mats_host_ + g.mats_off + (uint64_t)s * g.stride;
         for (const Pass &p : g.passes)
             for (int f = 0; f < p.prm.nops; ++f)
-                fop_entries(ops[p.src[f].op], p.prm.ops[f], p.src[f].swapped, block + p.prm.ops[f].moff);
+            {
+                const FOp &op = p.prm.ops[f];
+                if (quad_kind(op.kind))
+                    quad_entries(ops, p.src[f], block + op.moff);
+                else
+                    fop_entries(ops[p.src[f].op], op, p.src[f].swapped, block + op.moff);
+            }
     }
 }
 

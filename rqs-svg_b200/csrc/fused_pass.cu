@@ -171,6 +171,53 @@ __device__ __forceinline__ void apply_dense1r(V (&a)[R], const FOp &op, const M 
     }
 }
 
+// One uncontrolled 2x2 gate on each of the four stage bits, in bit order:
+// one dispatch, and the compiler keeps the amplitudes in place between them.
+template <typename V, typename M>
+__device__ __forceinline__ void apply_dense1rx4(V (&a)[R], const M &e)
+{
+    typedef decltype(V::x) S;
+#pragma unroll
+    for (int b = 0; b < kStageBits; ++b)
+    {
+        const S m00 = static_cast<S>(e[4 * b].x), m01 = static_cast<S>(e[4 * b + 1].x);
+        const S m10 = static_cast<S>(e[4 * b + 2].x), m11 = static_cast<S>(e[4 * b + 3].x);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            if (r & (1 << b))
+                continue;
+            const int r1 = r | (1 << b);
+            const V x0 = a[r], x1 = a[r1];
+            a[r].x = fma(m00, x0.x, m01 * x1.x);
+            a[r].y = fma(m00, x0.y, m01 * x1.y);
+            a[r1].x = fma(m11, x1.x, m10 * x0.x);
+            a[r1].y = fma(m11, x1.y, m10 * x0.y);
+        }
+    }
+}
+
+template <typename V, typename M>
+__device__ __forceinline__ void apply_dense1x4(V (&a)[R], const M &e)
+{
+#pragma unroll
+    for (int b = 0; b < kStageBits; ++b)
+    {
+        const V m00 = cvt<V>(e[4 * b]), m01 = cvt<V>(e[4 * b + 1]);
+        const V m10 = cvt<V>(e[4 * b + 2]), m11 = cvt<V>(e[4 * b + 3]);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            if (r & (1 << b))
+                continue;
+            const int r1 = r | (1 << b);
+            const V x0 = a[r], x1 = a[r1];
+            a[r] = cmad2(m00, x0, m01, x1);
+            a[r1] = cmad2(m11, x1, m10, x0);
+        }
+    }
+}
+
 template <typename V, int B>
 __device__ __forceinline__ void apply_swap1(V (&a)[R], const FOp &op, uint32_t j0)
 {
@@ -401,6 +448,8 @@ __device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, u
     case F_DENSE1R: dispatch_dense1r<V>(a, op, e, j0); break;
     case F_NEG: apply_neg<V>(a, op, j0); break;
     case F_MULI: apply_muli<V>(a, op, j0); break;
+    case F_DENSE1X4: apply_dense1x4<V>(a, e); break;
+    case F_DENSE1RX4: apply_dense1rx4<V>(a, e); break;
     case F_SWAP1: dispatch_swap1<V>(a, op, j0); break;
     case F_DENSE2: dispatch_dense2<V>(a, op, e, j0); break;
     case F_SWAP2: dispatch_swap2<V>(a, op, j0); break;
@@ -976,6 +1025,13 @@ int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m)
     }
 }
 
+int quad_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m)
+{
+    for (int b = 0; b < kStageBits; ++b)
+        expand_dense(q[src.quad[b]], m + 4 * b);
+    return 16;
+}
+
 // Fill the kernel parameters of a pass. Returns false when the pass does not
 // fit the parameter block limits.
 bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
@@ -1035,7 +1091,7 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
             return &S;
         };
         FStage *cur = nullptr;
-        const std::vector<int> sops = cluster_diagonals(q, pp, stage_ops[si]);
+        std::vector<int> sops = cluster_diagonals(q, pp, stage_ops[si]);
         size_t idx = 0;
         while (idx < sops.size())
         {
@@ -1116,6 +1172,81 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                     ph->monomials |= static_cast<uint16_t>(1u << prm.ops[t].b0);
                 idx = run_end;
                 continue;
+            }
+            // four uncontrolled 1-target dense gates, one per stage bit, run
+            // as one op: gather them from the ops ahead that commute with
+            // everything they are moved past (batched passes keep them apart)
+            {
+                auto single = [&](const GateOp &g) {
+                    if (g.diag || g.nt != 1 || g.cmask != 0 || g.na != 2 || is_x(g))
+                        return -1;
+                    const int l = loc_of[g.tq[0]];
+                    return (l >= 0 && ((bits >> l) & 1)) ? pos_in_stage[l] : -1;
+                };
+                int pick[kStageBits] = {-1, -1, -1, -1};
+                uint32_t seen = 0;
+                std::vector<size_t> skipped;
+                for (size_t j = idx; j < sops.size() && seen != (1u << kStageBits) - 1; ++j)
+                {
+                    const GateOp &g = q[pp.ops[sops[j]]];
+                    const int b = single(g);
+                    bool take = b >= 0 && !((seen >> b) & 1);
+                    if (take)
+                    {
+                        // it moves before the skipped ops: it must commute with them
+                        const OpClass cg = classify(g);
+                        for (size_t k : skipped)
+                            if (!commute(classify(q[pp.ops[sops[k]]]), cg))
+                            {
+                                take = false;
+                                break;
+                            }
+                    }
+                    if (take)
+                    {
+                        pick[b] = static_cast<int>(j);
+                        seen |= 1u << b;
+                    }
+                    else
+                        skipped.push_back(j);
+                    if (j == idx && !take)
+                        break;   // the run must start at the current op
+                }
+                if (seen == (1u << kStageBits) - 1)
+                {
+                    if (nops >= kFusedMaxOps || nentries + 16 > kFusedMaxEntries)
+                        return false;
+                    if (cur == nullptr && (cur = open_stage(0)) == nullptr)
+                        return false;
+                    FOp &f = prm.ops[nops++];
+                    std::memset(&f, 0, sizeof(f));
+                    bool real = true;
+                    FOpSource qs{pp.ops[sops[pick[0]]], false, {0, 0, 0, 0}};
+                    for (int b = 0; b < kStageBits; ++b)
+                    {
+                        qs.quad[b] = pp.ops[sops[pick[b]]];
+                        real = real && is_real(q[qs.quad[b]]);
+                    }
+                    f.kind = real ? F_DENSE1RX4 : F_DENSE1X4;
+                    f.moff = static_cast<uint16_t>(nentries);
+                    quad_entries(q, qs, prm.entries + nentries);
+                    nentries += 16;
+                    if (src)
+                        src->push_back(qs);
+                    // drop the gathered ops from the remaining sequence
+                    std::vector<int> rest;
+                    for (size_t j = idx; j < sops.size(); ++j)
+                    {
+                        bool picked = false;
+                        for (int b = 0; b < kStageBits; ++b)
+                            picked |= pick[b] == static_cast<int>(j);
+                        if (!picked)
+                            rest.push_back(sops[j]);
+                    }
+                    sops.resize(idx);
+                    sops.insert(sops.end(), rest.begin(), rest.end());
+                    continue;
+                }
             }
             const int oi = sops[idx++];
             const GateOp &op = q[pp.ops[oi]];

@@ -31,6 +31,8 @@ enum FKind : uint8_t
     F_DENSE1R = 7, // 2x2 with real entries (RY, H, real U3) on one stage bit
     F_NEG = 8,     // F_PHASE by -1 (Z, CZ): sign flips, no multiplies
     F_MULI = 9,    // F_PHASE by i (b1 = 0) or -i (b1 = 1) (S, Sdg): exchanges and sign flips
+    F_DENSE1X4 = 10,  // four uncontrolled 2x2 gates, one on each stage bit (entries 4b..4b+3 for bit b)
+    F_DENSE1RX4 = 11, // the same with real entries
 };
 
 // One gate of a pass. Conditions: (local index & lcmask) == lcval and
@@ -117,11 +119,12 @@ struct Segment
 };
 
 // Which queued op an FOp came from, and whether its two targets were
-// exchanged to put them in stage-bit order.
+// exchanged to put them in stage-bit order (four ops for the x4 kinds).
 struct FOpSource
 {
     int op;
     bool swapped;
+    int quad[4];    // F_DENSE1X4 / F_DENSE1RX4: the queued op on each stage bit
 };
 
 OpClass classify(const GateOp &op);
@@ -131,8 +134,11 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
 bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
                   std::vector<FOpSource> *src = nullptr);
 // Entries an FOp of this kind reads (4 dense 1-target, 16 dense 2-target, 1
-// phase, 4 diagonal, 0 permutations), written to m from the GateOp.
+// phase, 4 diagonal, 0 permutations), written to m from the GateOp. The x4
+// kinds take 16 entries from four ops: use quad_entries.
 int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m);
+int quad_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m);
+inline bool quad_kind(uint8_t kind) { return kind == F_DENSE1X4 || kind == F_DENSE1RX4; }
 // Entries a queued op will need in a pass (the same counts, from the GateOp).
 int op_entry_count(const GateOp &op);
 // Kernel parameters of a planned pass, cut in two (in order, recursively)

@@ -90,6 +90,34 @@ def test_long_diagonal_run_with_interleaved_commuting_gates(gpu_lib, oracle_lib)
     assert np.max(np.abs(got - ref)) <= 1e-12
 
 
+@pytest.mark.parametrize("n", [6, 11, 15])
+def test_single_qubit_layers_merge_across_blockers(gpu_lib, oracle_lib, n):
+    """Layers of uncontrolled one-target gates (merged four at a time into one
+    op of a stage) with CZ, CX and other gates between them: a gate may be
+    gathered past a blocker only when it commutes with it."""
+    rng = np.random.default_rng(n)
+    circ = []
+    for blk in range(10):
+        order = rng.permutation(n)
+        for q in order:
+            name = ["u3", "ry", "h", "sx", "rx", "x"][int(rng.integers(0, 6))]
+            npar = GATES[name][0]
+            circ.append((name, tuple(rng.uniform(-6, 6, size=npar)), (int(q),), (), ()))
+            if rng.random() < 0.25:
+                circ += C.random_circuit(n, 1, seed=int(rng.integers(1 << 30)), max_controls=1,
+                                         gates=["z", "x", "rz", "rzz", "u3", "swap"])
+    start = _random_state(n, 5)
+    got, _ = _run(gpu_lib, n, circ, fusion=FUSION_GREEDY, start=start)
+    ref, _ = _run(oracle_lib, n, circ, start=start)
+    assert np.max(np.abs(got - ref)) <= 1e-12
+    with qcs_b200.Batch(gpu_lib, 128) as batch:
+        batch.add_circuit(n, circ)
+        batch.run()
+        got_b = batch.statevector(0)
+    ref0, _ = _run(oracle_lib, n, circ)
+    assert np.max(np.abs(got_b - ref0)) <= 1e-12
+
+
 @pytest.mark.parametrize("mode", MODES)
 def test_twenty_qubit_layered_and_qft(gpu_lib, oracle_lib, mode):
     for circ in (C.layered_u3_cz(20, 6, seed=3), C.qft(20, seed=4)[0], C.layered_u3_cz_cx_toffoli(20, 4, seed=5)):
