@@ -534,6 +534,53 @@ __device__ __forceinline__ void phase_stage(V *sb, const uint32_t (&pos)[R], uin
         sb[pos[r]] = cmul(E[r], sb[pos[r]]);
 }
 
+// A phase run inside a register stage, on amplitudes already in registers:
+// the same terms as a phase stage, restricted to monomials of at most one
+// stage bit, so five accumulators suffice (E[0] for no stage bit, E[1 + b]
+// for stage bit b) and amplitude r gets E[0] * prod_{b in r} E[1 + b]. The
+// products are formed four slots at a time so that few stay live next to
+// the 16 amplitudes: 15 complex products to form the factors, 16 to apply.
+template <typename V, typename M>
+__device__ __forceinline__ void phase_inline(V (&a)[R], const FOp *terms, int nterms, uint32_t j0, uint64_t cbase,
+                                             const M &entry_at)
+{
+    V E0{1, 0}, E1{1, 0}, E2{1, 0}, E4{1, 0}, E8{1, 0};
+    for (int i = 0; i < nterms; ++i)
+    {
+        const FOp &t = terms[i];
+        if ((j0 & t.lcmask) != t.lcval || (cbase & t.gcmask) != t.gcval)
+            continue;
+        V d = cvt<V>(entry_at(t.moff));
+        if (t.b1)
+            d.y = -d.y;
+        switch (t.b0)
+        {
+        case 0: E0 = cmul(d, E0); break;
+        case 1: E1 = cmul(d, E1); break;
+        case 2: E2 = cmul(d, E2); break;
+        case 4: E4 = cmul(d, E4); break;
+        default: E8 = cmul(d, E8); break;
+        }
+    }
+    // slots r, r | 4, r | 8, r | 12 share the factor f(r) of their two low bits
+    V f = E0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+    {
+        if (r == 1)
+            f = cmul(E0, E1);
+        else if (r == 2)
+            f = cmul(E0, E2);
+        else if (r == 3)
+            f = cmul(cmul(E0, E1), E2);
+        const V g = cmul(f, E4);
+        a[r] = cmul(f, a[r]);
+        a[r | 4] = cmul(g, a[r | 4]);
+        a[r | 8] = cmul(cmul(f, E8), a[r | 8]);
+        a[r | 12] = cmul(cmul(g, E8), a[r | 12]);
+    }
+}
+
 // One CTA per chunk at a time; blockDim.x == 2^(k - kStageBits) <= 128, so
 // that three CTAs (12 warps, 3 x 64 KB of double-buffered chunks) share an SM.
 // BATCH: the work items are the chunks of many registers of the same size
@@ -674,6 +721,17 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
             for (int oi = S.op_begin; oi < S.op_end; ++oi)
             {
                 const FOp &op = p.ops[oi];
+                if (op.kind == F_PRUN)
+                {
+                    if (BATCH)
+                        phase_inline<V>(a, p.ops + oi + 1, op.lcmask, j0, cbase,
+                                        [&](int off) { return __ldg(entries + off); });
+                    else
+                        phase_inline<V>(a, p.ops + oi + 1, op.lcmask, j0, cbase,
+                                        [&](int off) { return p.entries[off]; });
+                    oi += op.lcmask;
+                    continue;
+                }
                 if ((cbase & op.gcmask) != op.gcval)
                     continue;
                 if (BATCH)
@@ -921,6 +979,23 @@ int phase_run_min()
     return v;
 }
 
+// Phase runs whose gates each involve at most one stage bit run inside the
+// register stage (F_PRUN) instead of in a phase stage of their own, saving
+// the stage's shared-memory round trip (tuning knob QCS_PHASE_INLINE, default
+// on; 0 keeps every run in phase stages).
+constexpr int kStageSlots = 1 << kStageBits;
+constexpr int kInlineRunMin = 3;          // weight of the ops an F_PRUN needs to pay for its 32 products
+constexpr int kInlineOtherBudget = 48;    // complex products per thread, about a stage round trip
+
+bool phase_inline_enabled()
+{
+    static const bool v = [] {
+        const char *e = std::getenv("QCS_PHASE_INLINE");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+
 int phase_weight(const GateOp &op)
 {
     if (op.na != 1)
@@ -1090,15 +1165,139 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
             S.op_begin = static_cast<uint16_t>(nops);
             return &S;
         };
+        // the stage bits a diagonal op's pattern (controls and targets) involves
+        auto pattern_stage_bits = [&](const GateOp &op) {
+            uint64_t cm = op.cmask;
+            for (int i = 0; i < op.nt; ++i)
+                cm |= 1ull << op.tq[i];
+            int c = 0;
+            for (int b = 0; b < n; ++b)
+                if (((cm >> b) & 1) && loc_of[b] >= 0 && ((bits >> loc_of[b]) & 1))
+                    ++c;
+            return c;
+        };
+        // the F_TERMs of a phase-run op: one per inclusion-exclusion member
+        auto emit_terms = [&](int qi) -> bool {
+            const GateOp &op = q[qi];
+            for (int a = 0; a < op.na; ++a)
+            {
+                uint64_t cm = op.cmask, cv = op.cval;
+                for (int i = 0; i < op.nt; ++i)
+                {
+                    cm |= 1ull << op.tq[i];
+                    if ((op.act[a] >> i) & 1)
+                        cv |= 1ull << op.tq[i];
+                }
+                uint32_t s1 = 0, s0 = 0, lcm = 0, lcv = 0;
+                uint64_t gcm = 0, gcv = 0;
+                for (int b = 0; b < n; ++b)
+                {
+                    if (!((cm >> b) & 1))
+                        continue;
+                    const bool v = (cv >> b) & 1;
+                    const int l = loc_of[b];
+                    if (l >= 0 && ((bits >> l) & 1))
+                        (v ? s1 : s0) |= 1u << pos_in_stage[l];
+                    else if (l >= 0)
+                    {
+                        lcm |= 1u << l;
+                        lcv |= v ? 1u << l : 0u;
+                    }
+                    else
+                    {
+                        gcm |= 1ull << b;
+                        gcv |= v ? 1ull << b : 0ull;
+                    }
+                }
+                for (uint32_t A = s0;; A = (A - 1) & s0)
+                {
+                    if (nops >= kFusedMaxOps || nentries + 1 > kFusedMaxEntries)
+                        return false;
+                    FOp &t = prm.ops[nops++];
+                    std::memset(&t, 0, sizeof(t));
+                    t.kind = F_TERM;
+                    t.b0 = static_cast<uint8_t>(s1 | A);
+                    t.b1 = static_cast<uint8_t>(__builtin_popcount(A) & 1);
+                    t.phys[0] = static_cast<uint8_t>(a);
+                    t.lcmask = lcm;
+                    t.lcval = lcv;
+                    t.gcmask = gcm;
+                    t.gcval = gcv;
+                    t.moff = static_cast<uint16_t>(nentries);
+                    fop_entries(op, t, false, prm.entries + nentries);
+                    ++nentries;
+                    if (src)
+                        src->push_back({qi, false});
+                    if (A == 0)
+                        break;
+                }
+            }
+            return true;
+        };
         FStage *cur = nullptr;
         std::vector<int> sops = cluster_diagonals(q, pp, stage_ops[si]);
         size_t idx = 0;
+        size_t singles_end = 0;   // ops [idx, singles_end) run one by one
         while (idx < sops.size())
         {
             size_t run_end = idx;
             int weight = 0;
-            while (run_end < sops.size() && phase_run_op(q[pp.ops[sops[run_end]]]))
+            while (idx >= singles_end && run_end < sops.size() && phase_run_op(q[pp.ops[sops[run_end]]]))
                 weight += phase_weight(q[pp.ops[sops[run_end++]]]);
+            // Ops of the run whose patterns hold at most one stage bit can run
+            // inside the register stage (F_PRUN: one complex product per term
+            // and thread, 32 per thread to apply); the others run one by one,
+            // which is cheap when their patterns hold several stage bits (a
+            // phase on 2^(4 - p) of the 16 slots). Only when those single ops
+            // would cost more than a stage's shared-memory round trip does
+            // the run become a phase stage.
+            if (weight >= phase_run_min() && phase_inline_enabled())
+            {
+                std::vector<int> lin, other;
+                int wlin = 0, other_cost = 0;
+                for (size_t ri = idx; ri < run_end; ++ri)
+                {
+                    const GateOp &op = q[pp.ops[sops[ri]]];
+                    const int sbc = pattern_stage_bits(op);
+                    if (sbc <= 1)
+                    {
+                        lin.push_back(sops[ri]);
+                        wlin += phase_weight(op);
+                    }
+                    else
+                    {
+                        other.push_back(sops[ri]);
+                        // complex products per thread as a single op
+                        other_cost += phase_weight(op) == 0 ? 1 : op.na == 1 ? (kStageSlots >> sbc) : kStageSlots;
+                    }
+                }
+                if (other_cost <= kInlineOtherBudget)
+                {
+                    if (wlin >= kInlineRunMin)
+                    {
+                        if (nops >= kFusedMaxOps)
+                            return false;
+                        if (cur == nullptr && (cur = open_stage(0)) == nullptr)
+                            return false;
+                        const int head = nops++;
+                        std::memset(&prm.ops[head], 0, sizeof(FOp));
+                        prm.ops[head].kind = F_PRUN;
+                        if (src)
+                            src->push_back({pp.ops[lin[0]], false});
+                        for (int oi : lin)
+                            if (!emit_terms(pp.ops[oi]))
+                                return false;
+                        prm.ops[head].lcmask = static_cast<uint32_t>(nops - head - 1);
+                        lin.clear();
+                    }
+                    // what is left of the run follows as single ops
+                    other.insert(other.end(), lin.begin(), lin.end());
+                    std::copy(other.begin(), other.end(), sops.begin() + idx);
+                    sops.erase(sops.begin() + idx + other.size(), sops.begin() + run_end);
+                    singles_end = idx + other.size();
+                    continue;
+                }
+            }
             if (weight >= phase_run_min())
             {
                 // a phase stage: one term per inclusion-exclusion member
@@ -1111,62 +1310,8 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                 if (ph == nullptr)
                     return false;
                 for (size_t ri = idx; ri < run_end; ++ri)
-                {
-                    const GateOp &op = q[pp.ops[sops[ri]]];
-                    for (int a = 0; a < op.na; ++a)
-                    {
-                        uint64_t cm = op.cmask, cv = op.cval;
-                        for (int i = 0; i < op.nt; ++i)
-                        {
-                            cm |= 1ull << op.tq[i];
-                            if ((op.act[a] >> i) & 1)
-                                cv |= 1ull << op.tq[i];
-                        }
-                        uint32_t s1 = 0, s0 = 0, lcm = 0, lcv = 0;
-                        uint64_t gcm = 0, gcv = 0;
-                        for (int b = 0; b < n; ++b)
-                        {
-                            if (!((cm >> b) & 1))
-                                continue;
-                            const bool v = (cv >> b) & 1;
-                            const int l = loc_of[b];
-                            if (l >= 0 && ((bits >> l) & 1))
-                                (v ? s1 : s0) |= 1u << pos_in_stage[l];
-                            else if (l >= 0)
-                            {
-                                lcm |= 1u << l;
-                                lcv |= v ? 1u << l : 0u;
-                            }
-                            else
-                            {
-                                gcm |= 1ull << b;
-                                gcv |= v ? 1ull << b : 0ull;
-                            }
-                        }
-                        for (uint32_t A = s0;; A = (A - 1) & s0)
-                        {
-                            if (nops >= kFusedMaxOps || nentries + 1 > kFusedMaxEntries)
-                                return false;
-                            FOp &t = prm.ops[nops++];
-                            std::memset(&t, 0, sizeof(t));
-                            t.kind = F_TERM;
-                            t.b0 = static_cast<uint8_t>(s1 | A);
-                            t.b1 = static_cast<uint8_t>(__builtin_popcount(A) & 1);
-                            t.phys[0] = static_cast<uint8_t>(a);
-                            t.lcmask = lcm;
-                            t.lcval = lcv;
-                            t.gcmask = gcm;
-                            t.gcval = gcv;
-                            t.moff = static_cast<uint16_t>(nentries);
-                            fop_entries(op, t, false, prm.entries + nentries);
-                            ++nentries;
-                            if (src)
-                                src->push_back({pp.ops[sops[ri]], false});
-                            if (A == 0)
-                                break;
-                        }
-                    }
-                }
+                    if (!emit_terms(pp.ops[sops[ri]]))
+                        return false;
                 ph->op_end = static_cast<uint16_t>(nops);
                 for (int t = ph->op_begin; t < nops; ++t)
                     ph->monomials |= static_cast<uint16_t>(1u << prm.ops[t].b0);

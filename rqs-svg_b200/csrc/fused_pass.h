@@ -33,6 +33,7 @@ enum FKind : uint8_t
     F_MULI = 9,    // F_PHASE by i (b1 = 0) or -i (b1 = 1) (S, Sdg): exchanges and sign flips
     F_DENSE1X4 = 10,  // four uncontrolled 2x2 gates, one on each stage bit (entries 4b..4b+3 for bit b)
     F_DENSE1RX4 = 11, // the same with real entries
+    F_PRUN = 12,      // a phase run inside a register stage: the next lcmask ops are its F_TERMs, each on at most one stage bit
 };
 
 // One gate of a pass. Conditions: (local index & lcmask) == lcval and
