@@ -534,17 +534,55 @@ __device__ __forceinline__ void phase_stage(V *sb, const uint32_t (&pos)[R], uin
         sb[pos[r]] = cmul(E[r], sb[pos[r]]);
 }
 
-// A phase run inside a register stage, on amplitudes already in registers:
-// the same terms as a phase stage, restricted to monomials of at most one
-// stage bit, so five accumulators suffice (E[0] for no stage bit, E[1 + b]
-// for stage bit b) and amplitude r gets E[0] * prod_{b in r} E[1 + b]. The
-// products are formed four slots at a time so that few stay live next to
-// the 16 amplitudes: 15 complex products to form the factors, 16 to apply.
+// A phase run inside a register stage (F_PRUN), on amplitudes already in
+// registers: the terms of a phase stage restricted to monomials of at most
+// one stage bit, so five factors suffice (E[0] on every slot, E[1 + b] on the
+// slots with stage bit b). Factors start from the run's tables: the thread's
+// entry of its thread tables and, per 8-bit group of the chunk index, the
+// chunk's entry of the group tables (both built on the host from the terms
+// whose conditions fall entirely on those bits); the other terms follow the
+// header and are multiplied in one by one. Each factor in use then
+// multiplies its slots directly: 16 products for E[0], 8 for a stage bit (a
+// QFT run: one stage-bit factor, 8 products per thread). Forming the 16 slot
+// factors first would take 31 products for any mix, but keeps more values
+// live next to the amplitudes, which made the kernel spill.
 template <typename V, typename M>
-__device__ __forceinline__ void phase_inline(V (&a)[R], const FOp *terms, int nterms, uint32_t j0, uint64_t cbase,
-                                             const M &entry_at)
+__device__ __forceinline__ void phase_inline(V (&a)[R], const FOp &head, const FOp *terms, uint32_t j0,
+                                             uint64_t cbase, uint64_t chunk, int tid, int T,
+                                             const double2 *tables, const M &entry_at)
 {
-    V E0{1, 0}, E1{1, 0}, E2{1, 0}, E4{1, 0}, E8{1, 0};
+    V E[kStageBits + 1];
+#pragma unroll
+    for (int e = 0; e <= kStageBits; ++e)
+        E[e] = V{1, 0};
+    const uint64_t packed = head.gcmask;
+    if (packed)
+    {
+        const double2 *tb = tables + head.lcval;
+#pragma unroll
+        for (int e = 0; e <= kStageBits; ++e)
+            if ((packed >> e) & 1)
+            {
+                E[e] = cvt<V>(__ldg(tb + tid));
+                tb += T;
+            }
+#pragma unroll
+        for (int g = 0; g < kMaxChunkGroups; ++g)
+        {
+            const uint32_t gm = static_cast<uint32_t>(packed >> (kChunkGroupBits * (g + 1))) & 31u;
+            if (gm == 0)
+                continue;
+            const uint32_t idx = static_cast<uint32_t>(chunk >> (kChunkGroupBits * g)) & ((1u << kChunkGroupBits) - 1);
+#pragma unroll
+            for (int e = 0; e <= kStageBits; ++e)
+                if ((gm >> e) & 1)
+                {
+                    E[e] = cmul(cvt<V>(__ldg(tb + idx)), E[e]);
+                    tb += 1 << kChunkGroupBits;
+                }
+        }
+    }
+    const int nterms = static_cast<int>(head.lcmask);
     for (int i = 0; i < nterms; ++i)
     {
         const FOp &t = terms[i];
@@ -555,30 +593,29 @@ __device__ __forceinline__ void phase_inline(V (&a)[R], const FOp *terms, int nt
             d.y = -d.y;
         switch (t.b0)
         {
-        case 0: E0 = cmul(d, E0); break;
-        case 1: E1 = cmul(d, E1); break;
-        case 2: E2 = cmul(d, E2); break;
-        case 4: E4 = cmul(d, E4); break;
-        default: E8 = cmul(d, E8); break;
+        case 0: E[0] = cmul(d, E[0]); break;
+        case 1: E[1] = cmul(d, E[1]); break;
+        case 2: E[2] = cmul(d, E[2]); break;
+        case 4: E[3] = cmul(d, E[3]); break;
+        default: E[4] = cmul(d, E[4]); break;
         }
     }
-    // slots r, r | 4, r | 8, r | 12 share the factor f(r) of their two low bits
-    V f = E0;
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
+    const uint32_t used = head.b0;
+    if (used & 1)
     {
-        if (r == 1)
-            f = cmul(E0, E1);
-        else if (r == 2)
-            f = cmul(E0, E2);
-        else if (r == 3)
-            f = cmul(cmul(E0, E1), E2);
-        const V g = cmul(f, E4);
-        a[r] = cmul(f, a[r]);
-        a[r | 4] = cmul(g, a[r | 4]);
-        a[r | 8] = cmul(cmul(f, E8), a[r | 8]);
-        a[r | 12] = cmul(cmul(g, E8), a[r | 12]);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            a[r] = cmul(E[0], a[r]);
     }
+#pragma unroll
+    for (int b = 0; b < kStageBits; ++b)
+        if ((used >> (1 + b)) & 1)
+        {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if ((r >> b) & 1)
+                    a[r] = cmul(E[1 + b], a[r]);
+        }
 }
 
 // One CTA per chunk at a time; blockDim.x == 2^(k - kStageBits) <= 128, so
@@ -724,10 +761,10 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
                 if (op.kind == F_PRUN)
                 {
                     if (BATCH)
-                        phase_inline<V>(a, p.ops + oi + 1, op.lcmask, j0, cbase,
+                        phase_inline<V>(a, op, p.ops + oi + 1, j0, cbase, c, tid, T, p.tables,
                                         [&](int off) { return __ldg(entries + off); });
                     else
-                        phase_inline<V>(a, p.ops + oi + 1, op.lcmask, j0, cbase,
+                        phase_inline<V>(a, op, p.ops + oi + 1, j0, cbase, c, tid, T, p.tables,
                                         [&](int off) { return p.entries[off]; });
                     oi += op.lcmask;
                     continue;
@@ -1107,10 +1144,33 @@ int quad_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m)
     return 16;
 }
 
+namespace
+{
+
+double2 cmul_host(double2 x, double2 y)
+{
+    return make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+}
+
+// One inclusion-exclusion member of a phase-run gate: the factor (entry a of
+// gate qi, conjugated when conj) on the slots whose stage bits include mono,
+// under a condition on the thread's other local bits and on the chunk.
+struct TermRec
+{
+    int qi;
+    int a;
+    uint8_t mono;
+    uint8_t conj;
+    uint32_t lcm, lcv;
+    uint64_t gcm, gcv;
+};
+
+constexpr size_t kPassTableBudget = size_t(1) << 16;   // table entries of one pass (1 MiB)
+
 // Fill the kernel parameters of a pass. Returns false when the pass does not
 // fit the parameter block limits.
-bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
-                  std::vector<FOpSource> *src)
+bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
+                       std::vector<FOpSource> *src, std::vector<double2> *tables)
 {
     std::memset(&prm, 0, sizeof(prm));
     prm.n = n;
@@ -1130,6 +1190,11 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
         }
     if (nl != k)
         throw std::runtime_error("internal: pass locality size mismatch");
+    // bit of the chunk index that holds each non-local qubit
+    int cpos[kMaxQubits];
+    for (int b = 0, c = 0; b < n; ++b)
+        cpos[b] = loc_of[b] >= 0 ? -1 : c++;
+    const size_t table_start = tables ? tables->size() : 0;
     if (pp.ops.size() > (size_t)kFusedMaxOps)
         return false;
 
@@ -1176,8 +1241,8 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                     ++c;
             return c;
         };
-        // the F_TERMs of a phase-run op: one per inclusion-exclusion member
-        auto emit_terms = [&](int qi) -> bool {
+        // the terms of a phase-run op: one per inclusion-exclusion member
+        auto term_records = [&](int qi, std::vector<TermRec> &out) {
             const GateOp &op = q[qi];
             for (int a = 0; a < op.na; ++a)
             {
@@ -1211,27 +1276,39 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                 }
                 for (uint32_t A = s0;; A = (A - 1) & s0)
                 {
-                    if (nops >= kFusedMaxOps || nentries + 1 > kFusedMaxEntries)
-                        return false;
-                    FOp &t = prm.ops[nops++];
-                    std::memset(&t, 0, sizeof(t));
-                    t.kind = F_TERM;
-                    t.b0 = static_cast<uint8_t>(s1 | A);
-                    t.b1 = static_cast<uint8_t>(__builtin_popcount(A) & 1);
-                    t.phys[0] = static_cast<uint8_t>(a);
-                    t.lcmask = lcm;
-                    t.lcval = lcv;
-                    t.gcmask = gcm;
-                    t.gcval = gcv;
-                    t.moff = static_cast<uint16_t>(nentries);
-                    fop_entries(op, t, false, prm.entries + nentries);
-                    ++nentries;
-                    if (src)
-                        src->push_back({qi, false});
+                    out.push_back(TermRec{qi, a, static_cast<uint8_t>(s1 | A),
+                                          static_cast<uint8_t>(__builtin_popcount(A) & 1), lcm, lcv, gcm, gcv});
                     if (A == 0)
                         break;
                 }
             }
+        };
+        auto push_term = [&](const TermRec &r) -> bool {
+            if (nops >= kFusedMaxOps || nentries + 1 > kFusedMaxEntries)
+                return false;
+            FOp &t = prm.ops[nops++];
+            std::memset(&t, 0, sizeof(t));
+            t.kind = F_TERM;
+            t.b0 = r.mono;
+            t.b1 = r.conj;
+            t.phys[0] = static_cast<uint8_t>(r.a);
+            t.lcmask = r.lcm;
+            t.lcval = r.lcv;
+            t.gcmask = r.gcm;
+            t.gcval = r.gcv;
+            t.moff = static_cast<uint16_t>(nentries);
+            fop_entries(q[r.qi], t, false, prm.entries + nentries);
+            ++nentries;
+            if (src)
+                src->push_back({r.qi, false});
+            return true;
+        };
+        auto emit_terms = [&](int qi) -> bool {
+            std::vector<TermRec> recs;
+            term_records(qi, recs);
+            for (const TermRec &r : recs)
+                if (!push_term(r))
+                    return false;
             return true;
         };
         FStage *cur = nullptr;
@@ -1281,13 +1358,117 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                             return false;
                         const int head = nops++;
                         std::memset(&prm.ops[head], 0, sizeof(FOp));
-                        prm.ops[head].kind = F_PRUN;
                         if (src)
                             src->push_back({pp.ops[lin[0]], false});
+                        std::vector<TermRec> recs;
                         for (int oi : lin)
-                            if (!emit_terms(pp.ops[oi]))
-                                return false;
-                        prm.ops[head].lcmask = static_cast<uint32_t>(nops - head - 1);
+                            term_records(pp.ops[oi], recs);
+                        uint64_t packed = 0;
+                        uint32_t table_off = 0, used = 0;
+                        std::vector<int> where(recs.size(), -1);   // -1 explicit, 0 thread table, 1 + g group g
+                        auto factor = [](uint8_t mono) { return mono == 0 ? 0 : 1 + __builtin_ctz(mono); };
+                        if (tables)
+                        {
+                            uint32_t lmask = 0, gmask[kMaxChunkGroups] = {0, 0, 0, 0};
+                            std::vector<uint32_t> ccm(recs.size(), 0), ccv(recs.size(), 0);
+                            for (size_t i = 0; i < recs.size(); ++i)
+                            {
+                                const TermRec &r = recs[i];
+                                const int e = factor(r.mono);
+                                if (r.gcm == 0)
+                                {
+                                    where[i] = 0;
+                                    lmask |= 1u << e;
+                                    continue;
+                                }
+                                if (r.lcm != 0)
+                                    continue;
+                                // chunk-index bits of the condition, all in one group?
+                                uint64_t cm = 0, cv = 0;
+                                for (int b = 0; b < n; ++b)
+                                    if ((r.gcm >> b) & 1)
+                                    {
+                                        cm |= 1ull << cpos[b];
+                                        cv |= ((r.gcv >> b) & 1) << cpos[b];
+                                    }
+                                const int g = __builtin_ctzll(cm) / kChunkGroupBits;
+                                if (g >= kMaxChunkGroups || (cm >> (g * kChunkGroupBits)) >> kChunkGroupBits)
+                                    continue;
+                                where[i] = 1 + g;
+                                gmask[g] |= 1u << e;
+                                ccm[i] = static_cast<uint32_t>(cm >> (g * kChunkGroupBits));
+                                ccv[i] = static_cast<uint32_t>(cv >> (g * kChunkGroupBits));
+                            }
+                            const size_t T = size_t(1) << (k - kStageBits);
+                            size_t entries = __builtin_popcount(lmask) * T;
+                            for (int g = 0; g < kMaxChunkGroups; ++g)
+                                entries += __builtin_popcount(gmask[g]) * (size_t(1) << kChunkGroupBits);
+                            if (tables->size() - table_start + entries > kPassTableBudget)
+                            {
+                                std::fill(where.begin(), where.end(), -1);
+                            }
+                            else
+                            {
+                                table_off = static_cast<uint32_t>(tables->size());
+                                auto entry = [&](const TermRec &r) {
+                                    const cplx m = q[r.qi].mat[r.a];
+                                    return make_double2(m.re, r.conj ? -m.im : m.im);
+                                };
+                                for (int e = 0; e <= kStageBits; ++e)
+                                {
+                                    if (!((lmask >> e) & 1))
+                                        continue;
+                                    for (size_t t = 0; t < T; ++t)
+                                    {
+                                        // local index of thread t's slot 0: zeros at the stage bits
+                                        uint32_t j0 = static_cast<uint32_t>(t);
+                                        for (int sb = 0; sb < kStageBits; ++sb)
+                                        {
+                                            const uint32_t lo = j0 & ((1u << sbits[sb]) - 1u);
+                                            j0 = lo | ((j0 ^ lo) << 1);
+                                        }
+                                        double2 v = make_double2(1.0, 0.0);
+                                        for (size_t i = 0; i < recs.size(); ++i)
+                                            if (where[i] == 0 && factor(recs[i].mono) == e &&
+                                                (j0 & recs[i].lcm) == recs[i].lcv)
+                                                v = cmul_host(entry(recs[i]), v);
+                                        tables->push_back(v);
+                                    }
+                                }
+                                for (int g = 0; g < kMaxChunkGroups; ++g)
+                                    for (int e = 0; e <= kStageBits; ++e)
+                                    {
+                                        if (!((gmask[g] >> e) & 1))
+                                            continue;
+                                        for (uint32_t c = 0; c < (1u << kChunkGroupBits); ++c)
+                                        {
+                                            double2 v = make_double2(1.0, 0.0);
+                                            for (size_t i = 0; i < recs.size(); ++i)
+                                                if (where[i] == 1 + g && factor(recs[i].mono) == e &&
+                                                    (c & ccm[i]) == ccv[i])
+                                                    v = cmul_host(entry(recs[i]), v);
+                                            tables->push_back(v);
+                                        }
+                                    }
+                                packed = lmask;
+                                for (int g = 0; g < kMaxChunkGroups; ++g)
+                                    packed |= static_cast<uint64_t>(gmask[g]) << (kChunkGroupBits * (g + 1));
+                                used = lmask | gmask[0] | gmask[1] | gmask[2] | gmask[3];
+                            }
+                        }
+                        for (size_t i = 0; i < recs.size(); ++i)
+                            if (where[i] < 0)
+                            {
+                                if (!push_term(recs[i]))
+                                    return false;
+                                used |= 1u << factor(recs[i].mono);
+                            }
+                        FOp &h = prm.ops[head];
+                        h.kind = F_PRUN;
+                        h.lcmask = static_cast<uint32_t>(nops - head - 1);
+                        h.lcval = table_off;
+                        h.gcmask = packed;
+                        h.b0 = static_cast<uint8_t>(used);
                         lin.clear();
                     }
                     // what is left of the run follows as single ops
@@ -1513,12 +1694,25 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
     return true;
 }
 
+} // namespace
+
+bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
+                  std::vector<FOpSource> *src, std::vector<double2> *tables)
+{
+    const size_t start = tables ? tables->size() : 0;
+    const bool ok = build_params_body(q, pp, n, k, prm, src, tables);
+    if (!ok && tables)
+        tables->resize(start);
+    return ok;
+}
+
 bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, std::vector<FPassParams> &params,
-                  std::vector<std::vector<FOpSource>> *srcs, std::vector<PlannedPass> *pieces)
+                  std::vector<std::vector<FOpSource>> *srcs, std::vector<PlannedPass> *pieces,
+                  std::vector<double2> *tables)
 {
     params.emplace_back();
     std::vector<FOpSource> src;
-    if (build_params(q, pp, n, pp.k, params.back(), srcs ? &src : nullptr))
+    if (build_params(q, pp, n, pp.k, params.back(), srcs ? &src : nullptr, tables))
     {
         if (srcs)
             srcs->push_back(std::move(src));
@@ -1533,7 +1727,7 @@ bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, st
     PlannedPass a = pp, b = pp;
     a.ops.assign(pp.ops.begin(), pp.ops.begin() + half);
     b.ops.assign(pp.ops.begin() + half, pp.ops.end());
-    return build_pieces(q, a, n, params, srcs, pieces) && build_pieces(q, b, n, params, srcs, pieces);
+    return build_pieces(q, a, n, params, srcs, pieces, tables) && build_pieces(q, b, n, params, srcs, pieces, tables);
 }
 
 namespace
@@ -1793,6 +1987,46 @@ FusedExecutor::~FusedExecutor()
         cudaEventDestroy(judge_a_);
     if (judge_b_)
         cudaEventDestroy(judge_b_);
+    if (tables_copied_)
+    {
+        cudaEventSynchronize(tables_copied_);
+        cudaEventDestroy(tables_copied_);
+    }
+    cudaFree(tables_dev_);
+    cudaFreeHost(tables_host_);
+}
+
+// Copy the flush's phase-run tables to the device, behind the previous
+// flush's passes on the stream (which may still read the device buffer; the
+// copy is ordered after them). The pinned staging buffer is reused once the
+// previous copy has completed. Returns null when there are no tables.
+const double2 *FusedExecutor::upload_tables()
+{
+    if (tables_.empty())
+        return nullptr;
+    const size_t count = tables_.size();
+    if (tables_copied_)
+        QCSB_CUDA(cudaEventSynchronize(tables_copied_));
+    else
+        QCSB_CUDA(cudaEventCreateWithFlags(&tables_copied_, cudaEventDisableTiming));
+    if (count > tables_cap_)
+    {
+        // the old device buffer may still be read by queued passes
+        QCSB_CUDA(cudaStreamSynchronize(stream_));
+        cudaFree(tables_dev_);
+        cudaFreeHost(tables_host_);
+        tables_dev_ = nullptr;
+        tables_host_ = nullptr;
+        tables_cap_ = 0;
+        const size_t cap = std::max(count + count / 2, size_t(1) << 16);
+        QCSB_CUDA(cudaMalloc(&tables_dev_, cap * sizeof(double2)));
+        QCSB_CUDA(cudaMallocHost(&tables_host_, cap * sizeof(double2)));
+        tables_cap_ = cap;
+    }
+    std::memcpy(tables_host_, tables_.data(), count * sizeof(double2));
+    QCSB_CUDA(cudaMemcpyAsync(tables_dev_, tables_host_, count * sizeof(double2), cudaMemcpyHostToDevice, stream_));
+    QCSB_CUDA(cudaEventRecord(tables_copied_, stream_));
+    return tables_dev_;
 }
 
 // Record the device time of the previous learned-mode flush in the judge.
@@ -1889,36 +2123,52 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         last_plan_learned = 0;
     }
 
+    // Build every pass of the flush first (host only), so that the phase-run
+    // tables of all passes go to the device in one copy; then launch in order.
+    // step >= 0: a pass (index into params), step < 0: plain op -1 - step.
     std::vector<FPassParams> params;
     std::vector<PlannedPass> pieces;
+    std::vector<long> steps;
+    tables_.clear();
     for (const Segment &s : segs)
     {
         if (!s.fused)
         {
-            launches += plain(ops[s.plain_op]);
+            steps.push_back(-1 - (long)s.plain_op);
             continue;
         }
-        params.clear();
-        pieces.clear();
-        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces))
+        const size_t before = params.size();
+        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces, &tables_))
         {
+            params.resize(before);
+            pieces.resize(before);
             for (int oi : s.pass.ops)
-                launches += plain(ops[oi]);
+                steps.push_back(-1 - (long)oi);
             continue;
         }
-        for (size_t i = 0; i < params.size(); ++i)
+        for (size_t i = before; i < params.size(); ++i)
+            steps.push_back((long)i);
+    }
+    const double2 *tables_dev = upload_tables();
+    for (long st : steps)
+    {
+        if (st < 0)
         {
-            if (timer.enabled)
-            {
-                const PassFeatures f = pass_features(ops, pieces[i], n);
-                timer.begin(stream_, KernelTimer::kFused, 2.0 * amp_bytes * std::ldexp(1.0, n), &f);
-            }
-            launches += c64 ? launch_fused_pass<float>(state, pieces[i].k, params[i], stream_)
-                             : launch_fused_pass<double>(state, pieces[i].k, params[i], stream_);
-            if (timer.enabled)
-                timer.end(stream_);
-            ++stats.fused_passes;
+            launches += plain(ops[-1 - st]);
+            continue;
         }
+        FPassParams &prm = params[st];
+        prm.tables = tables_dev;
+        if (timer.enabled)
+        {
+            const PassFeatures f = pass_features(ops, pieces[st], n);
+            timer.begin(stream_, KernelTimer::kFused, 2.0 * amp_bytes * std::ldexp(1.0, n), &f);
+        }
+        launches += c64 ? launch_fused_pass<float>(state, pieces[st].k, prm, stream_)
+                         : launch_fused_pass<double>(state, pieces[st].k, prm, stream_);
+        if (timer.enabled)
+            timer.end(stream_);
+        ++stats.fused_passes;
     }
     if (timed_flush)
         QCSB_CUDA(cudaEventRecord(judge_b_, stream_));

@@ -33,8 +33,24 @@ enum FKind : uint8_t
     F_MULI = 9,    // F_PHASE by i (b1 = 0) or -i (b1 = 1) (S, Sdg): exchanges and sign flips
     F_DENSE1X4 = 10,  // four uncontrolled 2x2 gates, one on each stage bit (entries 4b..4b+3 for bit b)
     F_DENSE1RX4 = 11, // the same with real entries
-    F_PRUN = 12,      // a phase run inside a register stage: the next lcmask ops are its F_TERMs, each on at most one stage bit
+    F_PRUN = 12,      // a phase run inside a register stage (fields below)
 };
+
+// F_PRUN: a run of diagonal gates, each on at most one stage bit, applied to
+// the amplitudes in registers through five factors E[0] (all slots) and
+// E[1 + b] (slots with stage bit b). Factors whose terms depend only on the
+// thread's other local bits come from per-thread tables; those whose terms
+// depend only on chunk bits inside one 8-bit group of the chunk index come
+// from per-group tables; the remaining terms follow the header as F_TERMs.
+//   lcmask: number of F_TERMs that follow
+//   lcval:  offset of the run's tables in FPassParams::tables
+//   gcmask: bits 0-4 which factors have a thread table (2^(k - 4) entries,
+//           indexed by thread); bits 8g+8 .. 8g+12 which have a table for
+//           chunk-index group g (256 entries, indexed by chunk bits 8g..8g+7);
+//           tables are stored in that order, factors ascending
+//   b0:     which factors can differ from 1
+constexpr int kChunkGroupBits = 8;
+constexpr int kMaxChunkGroups = 4;
 
 // One gate of a pass. Conditions: (local index & lcmask) == lcval and
 // (physical chunk bits & gcmask) == gcval. For F_PHASE the condition includes
@@ -92,6 +108,7 @@ struct FPassParams
     const double2 *mats;
     uint32_t mat_stride;
     int from_zero;               // registers start as |0..0>: build chunks instead of loading them
+    const double2 *tables;       // F_PRUN factor tables (device memory), null when no run has any
     FStage stages[kFusedMaxStages];
     FOp ops[kFusedMaxOps];
     double2 entries[kFusedMaxEntries];
@@ -132,8 +149,11 @@ OpClass classify(const GateOp &op);
 std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int low, int max_ops);
 // Fill the kernel parameters of a pass (false when it does not fit the
 // parameter block); src, when given, receives one FOpSource per FOp.
+// tables: where F_PRUN factor tables are appended (offsets in the ops are
+// absolute indices into it; the caller uploads it and sets prm.tables); null
+// keeps every term explicit, as batched passes need.
 bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
-                  std::vector<FOpSource> *src = nullptr);
+                  std::vector<FOpSource> *src = nullptr, std::vector<double2> *tables = nullptr);
 // Entries an FOp of this kind reads (4 dense 1-target, 16 dense 2-target, 1
 // phase, 4 diagonal, 0 permutations), written to m from the GateOp. The x4
 // kinds take 16 entries from four ops: use quad_entries.
@@ -144,9 +164,11 @@ inline bool quad_kind(uint8_t kind) { return kind == F_DENSE1X4 || kind == F_DEN
 int op_entry_count(const GateOp &op);
 // Kernel parameters of a planned pass, cut in two (in order, recursively)
 // while a piece does not fit one parameter block; every piece keeps the
-// pass's local qubits. False when a single op does not fit.
+// pass's local qubits. False when a single op does not fit. tables as for
+// build_params.
 bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, std::vector<FPassParams> &params,
-                  std::vector<std::vector<FOpSource>> *srcs = nullptr, std::vector<PlannedPass> *pieces = nullptr);
+                  std::vector<std::vector<FOpSource>> *srcs = nullptr, std::vector<PlannedPass> *pieces = nullptr,
+                  std::vector<double2> *tables = nullptr);
 int clamp_local_bits(int k, int n);
 int fused_min_qubits();
 

@@ -204,8 +204,16 @@ class FusedExecutor
         double learned_ms = -1.0;
     };
     void settle_judge();
+    const double2 *upload_tables();
 
     cudaStream_t stream_;
+    // phase-run tables of the current flush: built on the host, staged in
+    // pinned memory, copied to the device once per flush
+    std::vector<double2> tables_;
+    double2 *tables_host_ = nullptr;
+    double2 *tables_dev_ = nullptr;
+    size_t tables_cap_ = 0;
+    cudaEvent_t tables_copied_ = nullptr;
     int max_ops_ = 0;
     int local_bits_ = 0;
     CostModel *model_ = nullptr;
