@@ -242,7 +242,7 @@ void Batch::plan_group(Group &g, int k)
             if (off > 0xffffu)
                 throw std::runtime_error("batch: too many gate entries in one circuit");
             op.moff = static_cast<uint16_t>(off);
-            off += quad_kind(op.kind) ? quad_entries(g.shape, p.src[f], scratch)
+            off += layer_kind(op.kind) ? layer_entries(g.shape, p.src[f], scratch)
                                       : fop_entries(g.shape[p.src[f].op], op, p.src[f].swapped, scratch);
         }
     }
@@ -294,8 +294,8 @@ void Batch::fill_group_range(const Group &g, size_t first, size_t last)
             for (int f = 0; f < p.prm.nops; ++f)
             {
                 const FOp &op = p.prm.ops[f];
-                if (quad_kind(op.kind))
-                    quad_entries(ops, p.src[f], block + op.moff);
+                if (layer_kind(op.kind))
+                    layer_entries(ops, p.src[f], block + op.moff);
                 else
                     fop_entries(ops[p.src[f].op], op, p.src[f].swapped, block + op.moff);
             }

@@ -155,19 +155,30 @@ __device__ __forceinline__ void apply_dense1r(V (&a)[R], const FOp &op, const M 
     const S m10 = static_cast<S>(e[2].x), m11 = static_cast<S>(e[3].x);
     const bool tok = (j0 & op.lcmask) == op.lcval;
     const uint32_t cm = op.smask, cv = op.sval;
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-    {
-        if (r & (1 << B))
-            continue;
-        if (!tok || (cm != 0 && (r & cm) != cv))
-            continue;
+    auto pair = [&](int r) {
         const int r1 = r | (1 << B);
         const V x0 = a[r], x1 = a[r1];
         a[r].x = fma(m00, x0.x, m01 * x1.x);
         a[r].y = fma(m00, x0.y, m01 * x1.y);
         a[r1].x = fma(m11, x1.x, m10 * x0.x);
         a[r1].y = fma(m11, x1.y, m10 * x0.y);
+    };
+    if (cm == 0 && op.lcmask == 0)
+    {
+        // no condition: straight-line code without per-slot predicates
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (!(r & (1 << B)))
+                pair(r);
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+        if (r & (1 << B))
+            continue;
+        if (tok && (r & cm) == cv)
+            pair(r);
     }
 }
 
@@ -599,6 +610,12 @@ __device__ __forceinline__ void phase_inline(V (&a)[R], const FOp &head, const F
         case 4: E[3] = cmul(d, E[3]); break;
         default: E[4] = cmul(d, E[4]); break;
         }
+    }
+    if (head.b1)
+    {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            a[r] = cmul(cvt<V>(entry_at(head.moff + r)), a[r]);
     }
     const uint32_t used = head.b0;
     if (used & 1)
@@ -1137,11 +1154,19 @@ int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m)
     }
 }
 
-int quad_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m)
+int layer_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m)
 {
     for (int b = 0; b < kStageBits; ++b)
-        expand_dense(q[src.quad[b]], m + 4 * b);
-    return 16;
+    {
+        if (src.layer[b] >= 0)
+            expand_dense(q[src.layer[b]], m + 4 * b);
+        else
+        {
+            m[4 * b] = m[4 * b + 3] = make_double2(1.0, 0.0);
+            m[4 * b + 1] = m[4 * b + 2] = make_double2(0.0, 0.0);
+        }
+    }
+    return 4 * kStageBits;
 }
 
 namespace
@@ -1241,6 +1266,12 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     ++c;
             return c;
         };
+        auto pattern_bits = [&](const GateOp &op) {
+            uint64_t cm = op.cmask;
+            for (int i = 0; i < op.nt; ++i)
+                cm |= 1ull << op.tq[i];
+            return __builtin_popcountll(cm);
+        };
         // the terms of a phase-run op: one per inclusion-exclusion member
         auto term_records = [&](int qi, std::vector<TermRec> &out) {
             const GateOp &op = q[qi];
@@ -1330,7 +1361,11 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
             // the run become a phase stage.
             if (weight >= phase_run_min() && phase_inline_enabled())
             {
-                std::vector<int> lin, other;
+                // lin: at most one stage bit in the pattern; slot: the whole
+                // pattern on stage bits (a fixed factor per slot, folded into
+                // 16 per-slot entries; not in batched passes, whose entries
+                // are per register); other: single ops
+                std::vector<int> lin, slot, other;
                 int wlin = 0, other_cost = 0;
                 for (size_t ri = idx; ri < run_end; ++ri)
                 {
@@ -1341,6 +1376,8 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                         lin.push_back(sops[ri]);
                         wlin += phase_weight(op);
                     }
+                    else if (tables && sbc == pattern_bits(op))
+                        slot.push_back(sops[ri]);
                     else
                     {
                         other.push_back(sops[ri]);
@@ -1350,7 +1387,11 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 }
                 if (other_cost <= kInlineOtherBudget)
                 {
-                    if (wlin >= kInlineRunMin)
+                    const bool use_lin = wlin >= kInlineRunMin;
+                    const bool use_slot = slot.size() >= 2 || (use_lin && !slot.empty());
+                    if (!use_slot)
+                        other.insert(other.end(), slot.begin(), slot.end());
+                    if (use_lin || use_slot)
                     {
                         if (nops >= kFusedMaxOps)
                             return false;
@@ -1359,10 +1400,11 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                         const int head = nops++;
                         std::memset(&prm.ops[head], 0, sizeof(FOp));
                         if (src)
-                            src->push_back({pp.ops[lin[0]], false});
+                            src->push_back({pp.ops[use_lin ? lin[0] : slot[0]], false});
                         std::vector<TermRec> recs;
-                        for (int oi : lin)
-                            term_records(pp.ops[oi], recs);
+                        if (use_lin)
+                            for (int oi : lin)
+                                term_records(pp.ops[oi], recs);
                         uint64_t packed = 0;
                         uint32_t table_off = 0, used = 0;
                         std::vector<int> where(recs.size(), -1);   // -1 explicit, 0 thread table, 1 + g group g
@@ -1469,7 +1511,41 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                         h.lcval = table_off;
                         h.gcmask = packed;
                         h.b0 = static_cast<uint8_t>(used);
-                        lin.clear();
+                        if (use_slot)
+                        {
+                            if (nentries + kStageSlots > kFusedMaxEntries)
+                                return false;
+                            h.b1 = 1;
+                            h.moff = static_cast<uint16_t>(nentries);
+                            for (int r = 0; r < kStageSlots; ++r)
+                            {
+                                double2 v = make_double2(1.0, 0.0);
+                                for (int oi : slot)
+                                {
+                                    const GateOp &op = q[pp.ops[oi]];
+                                    for (int a = 0; a < op.na; ++a)
+                                    {
+                                        uint64_t cm = op.cmask, cv = op.cval;
+                                        for (int i = 0; i < op.nt; ++i)
+                                        {
+                                            cm |= 1ull << op.tq[i];
+                                            if ((op.act[a] >> i) & 1)
+                                                cv |= 1ull << op.tq[i];
+                                        }
+                                        bool match = true;
+                                        for (int b = 0; b < n && match; ++b)
+                                            if ((cm >> b) & 1)
+                                                match = ((r >> pos_in_stage[loc_of[b]]) & 1) == ((cv >> b) & 1);
+                                        if (match)
+                                            v = cmul_host(make_double2(op.mat[a].re, op.mat[a].im), v);
+                                    }
+                                }
+                                prm.entries[nentries + r] = v;
+                            }
+                            nentries += kStageSlots;
+                        }
+                        if (use_lin)
+                            lin.clear();
                     }
                     // what is left of the run follows as single ops
                     other.insert(other.end(), lin.begin(), lin.end());
@@ -1499,9 +1575,9 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 idx = run_end;
                 continue;
             }
-            // four uncontrolled 1-target dense gates, one per stage bit, run
-            // as one op: gather them from the ops ahead that commute with
-            // everything they are moved past (batched passes keep them apart)
+            // uncontrolled 1-target dense gates on distinct stage bits run as one
+            // F_DENSE1X4 / F_DENSE1RX4: gather them from the ops ahead that
+            // commute with everything they are moved past
             {
                 auto single = [&](const GateOp &g) {
                     if (g.diag || g.nt != 1 || g.cmask != 0 || g.na != 2 || is_x(g))
@@ -1521,8 +1597,8 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     {
                         // it moves before the skipped ops: it must commute with them
                         const OpClass cg = classify(g);
-                        for (size_t k : skipped)
-                            if (!commute(classify(q[pp.ops[sops[k]]]), cg))
+                        for (size_t sk : skipped)
+                            if (!commute(classify(q[pp.ops[sops[sk]]]), cg))
                             {
                                 take = false;
                                 break;
@@ -1536,29 +1612,35 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     else
                         skipped.push_back(j);
                     if (j == idx && !take)
-                        break;   // the run must start at the current op
+                        break;   // the group must start at the current op
                 }
-                if (seen == (1u << kStageBits) - 1)
+                bool all_real = true;
+                for (int b = 0; b < kStageBits; ++b)
+                    if (pick[b] >= 0 && !is_real(q[pp.ops[sops[pick[b]]]]))
+                        all_real = false;
+                // padded with identities on the missing bits: worth it from
+                // two real gates or three complex ones (an op dispatch costs
+                // about as much as a padded bit)
+                const int count = __builtin_popcount(seen);
+                if (count >= (all_real ? 2 : 3))
                 {
-                    if (nops >= kFusedMaxOps || nentries + 16 > kFusedMaxEntries)
+                    const int ne = 4 * kStageBits;
+                    if (nops >= kFusedMaxOps || nentries + ne > kFusedMaxEntries)
                         return false;
                     if (cur == nullptr && (cur = open_stage(0)) == nullptr)
                         return false;
                     FOp &f = prm.ops[nops++];
                     std::memset(&f, 0, sizeof(f));
-                    bool real = true;
-                    FOpSource qs{pp.ops[sops[pick[0]]], false, {0, 0, 0, 0}};
+                    FOpSource ls{pp.ops[sops[idx]], false, {-1, -1, -1, -1}};
                     for (int b = 0; b < kStageBits; ++b)
-                    {
-                        qs.quad[b] = pp.ops[sops[pick[b]]];
-                        real = real && is_real(q[qs.quad[b]]);
-                    }
-                    f.kind = real ? F_DENSE1RX4 : F_DENSE1X4;
+                        if (pick[b] >= 0)
+                            ls.layer[b] = pp.ops[sops[pick[b]]];
+                    f.kind = all_real ? F_DENSE1RX4 : F_DENSE1X4;
                     f.moff = static_cast<uint16_t>(nentries);
-                    quad_entries(q, qs, prm.entries + nentries);
-                    nentries += 16;
+                    layer_entries(q, ls, prm.entries + nentries);
+                    nentries += ne;
                     if (src)
-                        src->push_back(qs);
+                        src->push_back(ls);
                     // drop the gathered ops from the remaining sequence
                     std::vector<int> rest;
                     for (size_t j = idx; j < sops.size(); ++j)

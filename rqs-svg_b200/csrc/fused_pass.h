@@ -31,7 +31,8 @@ enum FKind : uint8_t
     F_DENSE1R = 7, // 2x2 with real entries (RY, H, real U3) on one stage bit
     F_NEG = 8,     // F_PHASE by -1 (Z, CZ): sign flips, no multiplies
     F_MULI = 9,    // F_PHASE by i (b1 = 0) or -i (b1 = 1) (S, Sdg): exchanges and sign flips
-    F_DENSE1X4 = 10,  // four uncontrolled 2x2 gates, one on each stage bit (entries 4b..4b+3 for bit b)
+    F_DENSE1X4 = 10,  // an uncontrolled 2x2 gate on each stage bit, in bit order (entries 4b..4b+3 for bit b;
+                      // identities on bits without a gate)
     F_DENSE1RX4 = 11, // the same with real entries
     F_PRUN = 12,      // a phase run inside a register stage (fields below)
 };
@@ -49,6 +50,8 @@ enum FKind : uint8_t
 //           chunk-index group g (256 entries, indexed by chunk bits 8g..8g+7);
 //           tables are stored in that order, factors ascending
 //   b0:     which factors can differ from 1
+//   b1:     1 when 16 per-slot factors (gates whose patterns lie entirely on
+//           the stage bits) start at moff
 constexpr int kChunkGroupBits = 8;
 constexpr int kMaxChunkGroups = 4;
 
@@ -142,7 +145,7 @@ struct FOpSource
 {
     int op;
     bool swapped;
-    int quad[4];    // F_DENSE1X4 / F_DENSE1RX4: the queued op on each stage bit
+    int layer[4];   // F_DENSE1X4 / F_DENSE1RX4: the queued op on each stage bit, -1 for none
 };
 
 OpClass classify(const GateOp &op);
@@ -156,10 +159,10 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
                   std::vector<FOpSource> *src = nullptr, std::vector<double2> *tables = nullptr);
 // Entries an FOp of this kind reads (4 dense 1-target, 16 dense 2-target, 1
 // phase, 4 diagonal, 0 permutations), written to m from the GateOp. The x4
-// kinds take 16 entries from four ops: use quad_entries.
+// kinds take 4 entries from each of their ops: use layer_entries.
 int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m);
-int quad_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m);
-inline bool quad_kind(uint8_t kind) { return kind == F_DENSE1X4 || kind == F_DENSE1RX4; }
+int layer_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m);
+inline bool layer_kind(uint8_t kind) { return kind == F_DENSE1X4 || kind == F_DENSE1RX4; }
 // Entries a queued op will need in a pass (the same counts, from the GateOp).
 int op_entry_count(const GateOp &op);
 // Kernel parameters of a planned pass, cut in two (in order, recursively)
