@@ -239,6 +239,8 @@ void Batch::plan_group(Group &g, int k)
         for (int f = 0; f < p.prm.nops; ++f)
         {
             FOp &op = p.prm.ops[f];
+            if (op.kind == F_SIGNT)
+                continue;   // moff holds the term's slot mask, no entries
             if (off > 0xffffu)
                 throw std::runtime_error("batch: too many gate entries in one circuit");
             op.moff = static_cast<uint16_t>(off);
@@ -294,6 +296,8 @@ void Batch::fill_group_range(const Group &g, size_t first, size_t last)
             for (int f = 0; f < p.prm.nops; ++f)
             {
                 const FOp &op = p.prm.ops[f];
+                if (op.kind == F_SIGNT)
+                    continue;
                 if (layer_kind(op.kind))
                     layer_entries(ops, p.src[f], block + op.moff);
                 else

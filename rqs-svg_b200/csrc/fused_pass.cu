@@ -323,6 +323,12 @@ __device__ __forceinline__ void apply_phase(V (&a)[R], const FOp &op, const M &m
 // Sign flips on the integer pipe (the FP64/FP32 pipes are the busy ones).
 __device__ __forceinline__ double flip(double x) { return __longlong_as_double(__double_as_longlong(x) ^ (1ll << 63)); }
 __device__ __forceinline__ float flip(float x) { return __int_as_float(__float_as_int(x) ^ (1 << 31)); }
+// sign bit XORed with bit 31 of s (s is 0 or 1 << 31)
+__device__ __forceinline__ double flip_by(double x, uint32_t s)
+{
+    return __hiloint2double(__double2hiint(x) ^ static_cast<int>(s), __double2loint(x));
+}
+__device__ __forceinline__ float flip_by(float x, uint32_t s) { return __uint_as_float(__float_as_uint(x) ^ s); }
 
 template <typename V>
 __device__ __forceinline__ void apply_neg(V (&a)[R], const FOp &op, uint32_t j0)
@@ -775,6 +781,28 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
             for (int oi = S.op_begin; oi < S.op_end; ++oi)
             {
                 const FOp &op = p.ops[oi];
+                if (op.kind == F_SIGNS)
+                {
+                    // XOR of the slot masks whose conditions hold, then one
+                    // sign-bit flip per slot on the integer pipe
+                    uint32_t neg = 0;
+                    const int nt = static_cast<int>(op.lcmask);
+                    for (int i = 1; i <= nt; ++i)
+                    {
+                        const FOp &t = p.ops[oi + i];
+                        if ((j0 & t.lcmask) == t.lcval && (cbase & t.gcmask) == t.gcval)
+                            neg ^= t.moff;
+                    }
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                    {
+                        const uint32_t s = ((neg >> r) & 1u) << 31;
+                        a[r].x = flip_by(a[r].x, s);
+                        a[r].y = flip_by(a[r].y, s);
+                    }
+                    oi += nt;
+                    continue;
+                }
                 if (op.kind == F_PRUN)
                 {
                     if (BATCH)
@@ -1038,7 +1066,7 @@ int phase_run_min()
 // the stage's shared-memory round trip (tuning knob QCS_PHASE_INLINE, default
 // on; 0 keeps every run in phase stages).
 constexpr int kStageSlots = 1 << kStageBits;
-constexpr int kInlineRunMin = 3;          // weight of the ops an F_PRUN needs to pay for its 32 products
+constexpr int kInlineRunMin = 2;          // gates an F_PRUN needs to beat single ops (about 200 instructions each)
 constexpr int kInlineOtherBudget = 48;    // complex products per thread, about a stage round trip
 
 bool phase_inline_enabled()
@@ -1058,6 +1086,12 @@ int phase_weight(const GateOp &op)
     const cplx e = op.mat[0];
     const bool clifford = (e.re == -1.0 && e.im == 0.0) || (e.re == 0.0 && (e.im == 1.0 || e.im == -1.0));
     return clifford ? 0 : 1;
+}
+
+// A phase of -1 on one pattern (Z, CZ, CCZ): runs as a sign flip.
+bool is_sign_op(const GateOp &op)
+{
+    return op.diag && op.na == 1 && op.mat[0].re == -1.0 && op.mat[0].im == 0.0;
 }
 
 bool phase_run_op(const GateOp &op)
@@ -1358,15 +1392,90 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
             // which is cheap when their patterns hold several stage bits (a
             // phase on 2^(4 - p) of the 16 slots). Only when those single ops
             // would cost more than a stage's shared-memory round trip does
-            // the run become a phase stage.
-            if (weight >= phase_run_min() && phase_inline_enabled())
+            // the run become a phase stage. Clifford phases (Z, CZ, S) join a
+            // run that has other phases (alone each is a predicated op of ~200
+            // instructions, in a run a table entry), but a run of Clifford
+            // phases alone stays single ops: sign flips and exchanges on the
+            // integer pipe, where the run would take FP64 products, the
+            // busier pipe on passes of dense gates (measured).
+            // -1 phases of the run (Z, CZ, CCZ) become one F_SIGNS; the rest of
+            // the run is looked at again without them
+            if (run_end > idx && phase_inline_enabled())
+            {
+                std::vector<int> signs, keep;
+                for (size_t ri = idx; ri < run_end; ++ri)
+                    (is_sign_op(q[pp.ops[sops[ri]]]) ? signs : keep).push_back(sops[ri]);
+                if (!signs.empty())
+                {
+                    if (nops + 1 + (int)signs.size() > kFusedMaxOps)
+                        return false;
+                    if (cur == nullptr && (cur = open_stage(0)) == nullptr)
+                        return false;
+                    FOp &h = prm.ops[nops++];
+                    std::memset(&h, 0, sizeof(h));
+                    h.kind = F_SIGNS;
+                    h.lcmask = static_cast<uint32_t>(signs.size());
+                    if (src)
+                        src->push_back({pp.ops[signs[0]], false});
+                    for (int oi : signs)
+                    {
+                        const GateOp &op = q[pp.ops[oi]];
+                        uint64_t cm = op.cmask, cv = op.cval;
+                        for (int i = 0; i < op.nt; ++i)
+                        {
+                            cm |= 1ull << op.tq[i];
+                            if ((op.act[0] >> i) & 1)
+                                cv |= 1ull << op.tq[i];
+                        }
+                        FOp &t = prm.ops[nops++];
+                        std::memset(&t, 0, sizeof(t));
+                        t.kind = F_SIGNT;
+                        uint32_t slots = 0;
+                        for (int r = 0; r < kStageSlots; ++r)
+                        {
+                            bool match = true;
+                            for (int b = 0; b < n && match; ++b)
+                                if (((cm >> b) & 1) && loc_of[b] >= 0 && ((bits >> loc_of[b]) & 1))
+                                    match = ((r >> pos_in_stage[loc_of[b]]) & 1) == ((cv >> b) & 1);
+                            if (match)
+                                slots |= 1u << r;
+                        }
+                        for (int b = 0; b < n; ++b)
+                        {
+                            if (!((cm >> b) & 1))
+                                continue;
+                            const int l = loc_of[b];
+                            const bool v = (cv >> b) & 1;
+                            if (l >= 0 && ((bits >> l) & 1))
+                                continue;
+                            if (l >= 0)
+                            {
+                                t.lcmask |= 1u << l;
+                                t.lcval |= v ? 1u << l : 0u;
+                            }
+                            else
+                            {
+                                t.gcmask |= 1ull << b;
+                                t.gcval |= v ? 1ull << b : 0ull;
+                            }
+                        }
+                        t.moff = static_cast<uint16_t>(slots);
+                        if (src)
+                            src->push_back({pp.ops[oi], false});
+                    }
+                    std::copy(keep.begin(), keep.end(), sops.begin() + idx);
+                    sops.erase(sops.begin() + idx + keep.size(), sops.begin() + run_end);
+                    continue;
+                }
+            }
+            if (run_end - idx >= static_cast<size_t>(kInlineRunMin) && weight > 0 && phase_inline_enabled())
             {
                 // lin: at most one stage bit in the pattern; slot: the whole
                 // pattern on stage bits (a fixed factor per slot, folded into
                 // 16 per-slot entries; not in batched passes, whose entries
                 // are per register); other: single ops
                 std::vector<int> lin, slot, other;
-                int wlin = 0, other_cost = 0;
+                int other_cost = 0, wlin = 0;
                 for (size_t ri = idx; ri < run_end; ++ri)
                 {
                     const GateOp &op = q[pp.ops[sops[ri]]];
@@ -1387,7 +1496,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 }
                 if (other_cost <= kInlineOtherBudget)
                 {
-                    const bool use_lin = wlin >= kInlineRunMin;
+                    const bool use_lin = lin.size() >= static_cast<size_t>(kInlineRunMin) && wlin > 0;
                     const bool use_slot = slot.size() >= 2 || (use_lin && !slot.empty());
                     if (!use_slot)
                         other.insert(other.end(), slot.begin(), slot.end());

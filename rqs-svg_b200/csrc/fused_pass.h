@@ -35,6 +35,8 @@ enum FKind : uint8_t
                       // identities on bits without a gate)
     F_DENSE1RX4 = 11, // the same with real entries
     F_PRUN = 12,      // a phase run inside a register stage (fields below)
+    F_SIGNS = 13,     // a run of -1 phases (Z, CZ, CCZ): the next lcmask ops are its F_SIGNT terms
+    F_SIGNT = 14,     // one -1 phase of an F_SIGNS: slots moff (16-bit mask) under the lc/gc condition
 };
 
 // F_PRUN: a run of diagonal gates, each on at most one stage bit, applied to
