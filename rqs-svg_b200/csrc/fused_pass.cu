@@ -2314,39 +2314,21 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         last_plan_learned = 0;
     }
 
-    // Build every pass of the flush first (host only), so that the phase-run
-    // tables of all passes go to the device in one copy; then launch in order.
+    // Passes launch as soon as they are built, so that the GPU runs while the
+    // host plans the rest, until the first pass that needs phase-run tables:
+    // from there on, passes are built first and launched after the tables of
+    // all of them have gone to the device in one copy (order is kept).
     // step >= 0: a pass (index into params), step < 0: plain op -1 - step.
     std::vector<FPassParams> params;
     std::vector<PlannedPass> pieces;
     std::vector<long> steps;
     tables_.clear();
-    for (const Segment &s : segs)
-    {
-        if (!s.fused)
-        {
-            steps.push_back(-1 - (long)s.plain_op);
-            continue;
-        }
-        const size_t before = params.size();
-        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces, &tables_))
-        {
-            params.resize(before);
-            pieces.resize(before);
-            for (int oi : s.pass.ops)
-                steps.push_back(-1 - (long)oi);
-            continue;
-        }
-        for (size_t i = before; i < params.size(); ++i)
-            steps.push_back((long)i);
-    }
-    const double2 *tables_dev = upload_tables();
-    for (long st : steps)
-    {
+    bool deferring = false;
+    auto launch_step = [&](long st, const double2 *tables_dev) {
         if (st < 0)
         {
             launches += plain(ops[-1 - st]);
-            continue;
+            return;
         }
         FPassParams &prm = params[st];
         prm.tables = tables_dev;
@@ -2360,6 +2342,38 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         if (timer.enabled)
             timer.end(stream_);
         ++stats.fused_passes;
+    };
+    auto add_step = [&](long st) {
+        if (deferring)
+            steps.push_back(st);
+        else
+            launch_step(st, nullptr);
+    };
+    for (const Segment &s : segs)
+    {
+        if (!s.fused)
+        {
+            add_step(-1 - (long)s.plain_op);
+            continue;
+        }
+        const size_t before = params.size();
+        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces, &tables_))
+        {
+            params.resize(before);
+            pieces.resize(before);
+            for (int oi : s.pass.ops)
+                add_step(-1 - (long)oi);
+            continue;
+        }
+        deferring = deferring || !tables_.empty();
+        for (size_t i = before; i < params.size(); ++i)
+            add_step((long)i);
+    }
+    if (!steps.empty())
+    {
+        const double2 *tables_dev = upload_tables();
+        for (long st : steps)
+            launch_step(st, tables_dev);
     }
     if (timed_flush)
         QCSB_CUDA(cudaEventRecord(judge_b_, stream_));
