@@ -1106,37 +1106,61 @@ bool phase_run_op(const GateOp &op)
     return true;
 }
 
-// Within one stage, move each diagonal op later past the non-diagonal ops it
-// commutes with, so that diagonal ops gather into runs (order among the
-// diagonal ops, and every non-commuting pair, is kept).
+// Within one stage, move diagonal ops later past the non-diagonal ops they
+// commute with, so that they gather into runs: when a held diagonal meets an
+// op it does not commute with, every held diagonal that this or a later op of
+// the stage blocks is placed there (keeping the runs whole, and the ops after
+// them together), and the ones nothing blocks sink to the end of the stage
+// (a QFT's phases to qubits outside the stage). Every non-commuting pair keeps
+// its order; diagonal ops commute with one another.
 std::vector<int> cluster_diagonals(const std::vector<GateOp> &q, const PlannedPass &pp, const std::vector<int> &ops)
 {
-    std::vector<int> out, held;
-    out.reserve(ops.size());
-    for (int oi : ops)
+    const size_t m = ops.size();
+    std::vector<OpClass> cls(m);
+    std::vector<bool> diag(m);
+    for (size_t i = 0; i < m; ++i)
     {
-        const GateOp &op = q[pp.ops[oi]];
-        if (phase_run_op(op))
+        cls[i] = classify(q[pp.ops[ops[i]]]);
+        diag[i] = phase_run_op(q[pp.ops[ops[i]]]);
+    }
+    // held diagonal h is blocked at or after position i by a non-diagonal op
+    auto blocked_from = [&](size_t h, size_t i) {
+        for (size_t j = i; j < m; ++j)
+            if (!diag[j] && !commute(cls[h], cls[j]))
+                return true;
+        return false;
+    };
+    std::vector<int> out;
+    std::vector<size_t> held;
+    out.reserve(m);
+    for (size_t i = 0; i < m; ++i)
+    {
+        if (diag[i])
         {
-            held.push_back(oi);
+            held.push_back(i);
             continue;
         }
-        const OpClass c = classify(op);
-        bool passes = true;
-        for (int h : held)
-            if (!commute(classify(q[pp.ops[h]]), c))
-            {
-                passes = false;
-                break;
-            }
-        if (!passes)
+        bool blocks = false;
+        for (size_t h : held)
+            blocks = blocks || !commute(cls[h], cls[i]);
+        if (blocks)
         {
-            out.insert(out.end(), held.begin(), held.end());
-            held.clear();
+            // every held diagonal that this or a later op blocks goes here, in
+            // one run; those that nothing later blocks sink to the stage's end
+            std::vector<size_t> still;
+            for (size_t h : held)
+            {
+                if (blocked_from(h, i))
+                    out.push_back(ops[h]);
+                else
+                    still.push_back(h);
+            }
+            held.swap(still);
         }
-        out.push_back(oi);
+        out.push_back(ops[i]);
     }
-    out.insert(out.end(), held.begin(), held.end());
+    for (size_t h : held)
+        out.push_back(ops[h]);
     return out;
 }
 
