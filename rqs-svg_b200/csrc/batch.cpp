@@ -244,7 +244,7 @@ void Batch::plan_group(Group &g, int k)
             if (off > 0xffffu)
                 throw std::runtime_error("batch: too many gate entries in one circuit");
             op.moff = static_cast<uint16_t>(off);
-            off += layer_kind(op.kind) ? layer_entries(g.shape, p.src[f], scratch)
+            off += layer_kind(op.kind) ? layer_entries(g.shape, p.src[f], op.kind, scratch)
                                       : fop_entries(g.shape[p.src[f].op], op, p.src[f].swapped, scratch);
         }
     }
@@ -299,7 +299,7 @@ void Batch::fill_group_range(const Group &g, size_t first, size_t last)
                 if (op.kind == F_SIGNT)
                     continue;
                 if (layer_kind(op.kind))
-                    layer_entries(ops, p.src[f], block + op.moff);
+                    layer_entries(ops, p.src[f], op.kind, block + op.moff);
                 else
                     fop_entries(ops[p.src[f].op], op, p.src[f].swapped, block + op.moff);
             }

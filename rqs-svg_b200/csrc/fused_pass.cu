@@ -229,6 +229,54 @@ __device__ __forceinline__ void apply_dense1x4(V (&a)[R], const M &e)
     }
 }
 
+// F_DENSE1X2 / F_DENSE1RX2: uncontrolled 2x2 gates on stage bits B0 < B1.
+template <typename V, int B0, int B1, typename M>
+__device__ __forceinline__ void apply_dense1x2(V (&a)[R], const M &e)
+{
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+    {
+        const int b = i ? B1 : B0;
+        const V m00 = cvt<V>(e[4 * i]), m01 = cvt<V>(e[4 * i + 1]);
+        const V m10 = cvt<V>(e[4 * i + 2]), m11 = cvt<V>(e[4 * i + 3]);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            if (r & (1 << b))
+                continue;
+            const int r1 = r | (1 << b);
+            const V x0 = a[r], x1 = a[r1];
+            a[r] = cmad2(m00, x0, m01, x1);
+            a[r1] = cmad2(m11, x1, m10, x0);
+        }
+    }
+}
+
+template <typename V, int B0, int B1, typename M>
+__device__ __forceinline__ void apply_dense1rx2(V (&a)[R], const M &e)
+{
+    typedef decltype(V::x) S;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+    {
+        const int b = i ? B1 : B0;
+        const S m00 = static_cast<S>(e[4 * i].x), m01 = static_cast<S>(e[4 * i + 1].x);
+        const S m10 = static_cast<S>(e[4 * i + 2].x), m11 = static_cast<S>(e[4 * i + 3].x);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+        {
+            if (r & (1 << b))
+                continue;
+            const int r1 = r | (1 << b);
+            const V x0 = a[r], x1 = a[r1];
+            a[r].x = fma(m00, x0.x, m01 * x1.x);
+            a[r].y = fma(m00, x0.y, m01 * x1.y);
+            a[r1].x = fma(m11, x1.x, m10 * x0.x);
+            a[r1].y = fma(m11, x1.y, m10 * x0.y);
+        }
+    }
+}
+
 template <typename V, int B>
 __device__ __forceinline__ void apply_swap1(V (&a)[R], const FOp &op, uint32_t j0)
 {
@@ -442,6 +490,29 @@ __device__ __forceinline__ void dispatch_dense2(V (&a)[R], const FOp &op, const 
     }
 }
 
+template <typename V, bool REAL, typename M>
+__device__ __forceinline__ void dispatch_x2(V (&a)[R], const FOp &op, const M &e)
+{
+#define QCSB_X2(b0, b1)                                                                                            \
+    case b0 * 4 + b1:                                                                                              \
+        if (REAL)                                                                                                  \
+            apply_dense1rx2<V, b0, b1>(a, e);                                                                      \
+        else                                                                                                       \
+            apply_dense1x2<V, b0, b1>(a, e);                                                                       \
+        break;
+    switch (op.b0 * 4 + op.b1)
+    {
+        QCSB_X2(0, 1) QCSB_X2(0, 2) QCSB_X2(0, 3) QCSB_X2(1, 2) QCSB_X2(1, 3)
+    default:
+        if (REAL)
+            apply_dense1rx2<V, 2, 3>(a, e);
+        else
+            apply_dense1x2<V, 2, 3>(a, e);
+        break;
+    }
+#undef QCSB_X2
+}
+
 template <typename V>
 __device__ __forceinline__ void dispatch_swap2(V (&a)[R], const FOp &op, uint32_t j0)
 {
@@ -467,6 +538,8 @@ __device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, u
     case F_MULI: apply_muli<V>(a, op, j0); break;
     case F_DENSE1X4: apply_dense1x4<V>(a, e); break;
     case F_DENSE1RX4: apply_dense1rx4<V>(a, e); break;
+    case F_DENSE1X2: dispatch_x2<V, false>(a, op, e); break;
+    case F_DENSE1RX2: dispatch_x2<V, true>(a, op, e); break;
     case F_SWAP1: dispatch_swap1<V>(a, op, j0); break;
     case F_DENSE2: dispatch_dense2<V>(a, op, e, j0); break;
     case F_SWAP2: dispatch_swap2<V>(a, op, j0); break;
@@ -1212,8 +1285,19 @@ int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m)
     }
 }
 
-int layer_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m)
+int layer_entries(const std::vector<GateOp> &q, const FOpSource &src, uint8_t kind, double2 *m)
 {
+    if (kind == F_DENSE1X2 || kind == F_DENSE1RX2)
+    {
+        int off = 0;
+        for (int b = 0; b < kStageBits; ++b)
+            if (src.layer[b] >= 0)
+            {
+                expand_dense(q[src.layer[b]], m + off);
+                off += 4;
+            }
+        return off;
+    }
     for (int b = 0; b < kStageBits; ++b)
     {
         if (src.layer[b] >= 0)
@@ -1751,13 +1835,14 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 for (int b = 0; b < kStageBits; ++b)
                     if (pick[b] >= 0 && !is_real(q[pp.ops[sops[pick[b]]]]))
                         all_real = false;
-                // padded with identities on the missing bits: worth it from
-                // two real gates or three complex ones (an op dispatch costs
-                // about as much as a padded bit)
+                // two complex gates: an x2 op; two real ones or three or four:
+                // an x4 op, padded with identities on the missing bits (an op
+                // dispatch costs about as much as a padded real bit; measured)
                 const int count = __builtin_popcount(seen);
-                if (count >= (all_real ? 2 : 3))
+                if (count >= 2)
                 {
-                    const int ne = 4 * kStageBits;
+                    const bool pair = count == 2 && !all_real;
+                    const int ne = pair ? 8 : 4 * kStageBits;
                     if (nops >= kFusedMaxOps || nentries + ne > kFusedMaxEntries)
                         return false;
                     if (cur == nullptr && (cur = open_stage(0)) == nullptr)
@@ -1768,9 +1853,18 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     for (int b = 0; b < kStageBits; ++b)
                         if (pick[b] >= 0)
                             ls.layer[b] = pp.ops[sops[pick[b]]];
-                    f.kind = all_real ? F_DENSE1RX4 : F_DENSE1X4;
+                    if (pair)
+                    {
+                        f.kind = all_real ? F_DENSE1RX2 : F_DENSE1X2;
+                        int nb = 0;
+                        for (int b = 0; b < kStageBits; ++b)
+                            if (pick[b] >= 0)
+                                (nb++ == 0 ? f.b0 : f.b1) = static_cast<uint8_t>(b);
+                    }
+                    else
+                        f.kind = all_real ? F_DENSE1RX4 : F_DENSE1X4;
                     f.moff = static_cast<uint16_t>(nentries);
-                    layer_entries(q, ls, prm.entries + nentries);
+                    layer_entries(q, ls, f.kind, prm.entries + nentries);
                     nentries += ne;
                     if (src)
                         src->push_back(ls);

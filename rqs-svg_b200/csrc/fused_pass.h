@@ -37,6 +37,8 @@ enum FKind : uint8_t
     F_PRUN = 12,      // a phase run inside a register stage (fields below)
     F_SIGNS = 13,     // a run of -1 phases (Z, CZ, CCZ): the next lcmask ops are its F_SIGNT terms
     F_SIGNT = 14,     // one -1 phase of an F_SIGNS: slots moff (16-bit mask) under the lc/gc condition
+    F_DENSE1X2 = 15,  // uncontrolled 2x2 gates on stage bits b0 < b1 (entries 0..3 for b0, 4..7 for b1)
+    F_DENSE1RX2 = 16, // the same with real entries
 };
 
 // F_PRUN: a run of diagonal gates, each on at most one stage bit, applied to
@@ -147,7 +149,7 @@ struct FOpSource
 {
     int op;
     bool swapped;
-    int layer[4];   // F_DENSE1X4 / F_DENSE1RX4: the queued op on each stage bit, -1 for none
+    int layer[4];   // x4 / x2 kinds: the queued op on each stage bit, -1 for none
 };
 
 OpClass classify(const GateOp &op);
@@ -163,8 +165,13 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
 // phase, 4 diagonal, 0 permutations), written to m from the GateOp. The x4
 // kinds take 4 entries from each of their ops: use layer_entries.
 int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m);
-int layer_entries(const std::vector<GateOp> &q, const FOpSource &src, double2 *m);
-inline bool layer_kind(uint8_t kind) { return kind == F_DENSE1X4 || kind == F_DENSE1RX4; }
+// x4 kinds: 4 entries per stage bit (identities where no gate); x2 kinds: 4
+// entries for each of the two bits present.
+int layer_entries(const std::vector<GateOp> &q, const FOpSource &src, uint8_t kind, double2 *m);
+inline bool layer_kind(uint8_t kind)
+{
+    return kind == F_DENSE1X4 || kind == F_DENSE1RX4 || kind == F_DENSE1X2 || kind == F_DENSE1RX2;
+}
 // Entries a queued op will need in a pass (the same counts, from the GateOp).
 int op_entry_count(const GateOp &op);
 // Kernel parameters of a planned pass, cut in two (in order, recursively)
