@@ -303,6 +303,8 @@ void Batch::fill_group_range(const Group &g, size_t first, size_t last)
                 else
                     fop_entries(ops[p.src[f].op], op, p.src[f].swapped, block + op.moff);
             }
+        if (amp_bytes_ == (int)sizeof(float2))
+            entries_to_float(block, g.stride);
     }
 }
 

@@ -50,6 +50,9 @@ template <>
 __device__ __forceinline__ double2 cvt<double2>(double2 m) { return m; }
 template <>
 __device__ __forceinline__ float2 cvt<float2>(double2 m) { return make_float2(static_cast<float>(m.x), static_cast<float>(m.y)); }
+// entries already stored in the amplitude type
+template <typename V>
+__device__ __forceinline__ V cvt(float2 m) { return m; }
 
 template <typename V>
 __device__ __forceinline__ V cmul(V m, V v)
@@ -97,17 +100,27 @@ constexpr int R = 1 << kStageBits;
 // the unconditional path.
 
 // Where an op's matrix entries come from: the pass parameters (one register)
-// or the register's block of the entry buffer (batched passes).
+// or the register's block of the entry buffer (batched passes). Entries are
+// stored in the amplitude type: complex64 passes hold float2 entries (the
+// host rounds them once), so the kernel neither converts nor loads 64-bit
+// values per use.
+template <typename V>
+__device__ __forceinline__ V pool_entry(const FPassParams &p, int i)
+{
+    return reinterpret_cast<const V *>(p.entries)[i];
+}
+template <typename V>
 struct PoolEntries
 {
     const FPassParams &p;
     uint32_t off;
-    __device__ __forceinline__ double2 operator[](int i) const { return p.entries[off + i]; }
+    __device__ __forceinline__ V operator[](int i) const { return pool_entry<V>(p, off + i); }
 };
+template <typename V>
 struct BufferEntries
 {
-    const double2 *m;
-    __device__ __forceinline__ double2 operator[](int i) const { return __ldg(m + i); }
+    const V *m;
+    __device__ __forceinline__ V operator[](int i) const { return __ldg(m + i); }
 };
 
 template <typename V, int B, typename M>
@@ -803,7 +816,7 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
         __syncthreads();
         const uint64_t cbase = chunk_base(c);
         const uint64_t reg = reg_of(c);
-        const double2 *entries = BATCH ? p.mats + reg * p.mat_stride : nullptr;
+        const V *entries = BATCH ? reinterpret_cast<const V *>(p.mats + reg * p.mat_stride) : nullptr;
 
         for (int st = 0; st < p.nstages; ++st)
         {
@@ -843,7 +856,7 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
                                    [&](int off) { return __ldg(entries + off); });
                 else
                     phase_stage<V>(sb, pos, j0, cbase, p.ops + S.op_begin, S.op_end - S.op_begin, S.monomials,
-                                   [&](int off) { return p.entries[off]; });
+                                   [&](int off) { return pool_entry<V>(p, off); });
                 __syncthreads();
                 continue;
             }
@@ -883,16 +896,16 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
                                         [&](int off) { return __ldg(entries + off); });
                     else
                         phase_inline<V>(a, op, p.ops + oi + 1, j0, cbase, c, tid, T, p.tables,
-                                        [&](int off) { return p.entries[off]; });
+                                        [&](int off) { return pool_entry<V>(p, off); });
                     oi += op.lcmask;
                     continue;
                 }
                 if ((cbase & op.gcmask) != op.gcval)
                     continue;
                 if (BATCH)
-                    apply_op<V>(a, op, BufferEntries{entries + op.moff}, j0, cbase);
+                    apply_op<V>(a, op, BufferEntries<V>{entries + op.moff}, j0, cbase);
                 else
-                    apply_op<V>(a, op, PoolEntries{p, op.moff}, j0, cbase);
+                    apply_op<V>(a, op, PoolEntries<V>{p, op.moff}, j0, cbase);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r)
@@ -2288,6 +2301,17 @@ uint64_t queue_signature(const std::vector<GateOp> &ops)
 
 int fused_min_qubits() { return kStageBits + 5; }
 
+void entries_to_float(double2 *entries, size_t count)
+{
+    // in place, front to back: float2 i ends where double2 i starts or earlier
+    float2 *f = reinterpret_cast<float2 *>(entries);
+    for (size_t i = 0; i < count; ++i)
+    {
+        const double2 d = entries[i];
+        f[i] = make_float2(static_cast<float>(d.x), static_cast<float>(d.y));
+    }
+}
+
 FusedExecutor::FusedExecutor(cudaStream_t stream) : stream_(stream) {}
 
 FusedExecutor::~FusedExecutor()
@@ -2484,6 +2508,9 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
             continue;
         }
         deferring = deferring || !tables_.empty();
+        if (c64)
+            for (size_t i = before; i < params.size(); ++i)
+                entries_to_float(params[i].entries, params[i].nentries);
         for (size_t i = before; i < params.size(); ++i)
             add_step((long)i);
     }

@@ -112,13 +112,13 @@ struct FPassParams
     // batched passes: registers of 2^n amplitudes stored back to back; work
     // item w is chunk w mod 2^(n-k) of register w >> (n-k); register r reads
     // its gate entries at mats + r * mat_stride
-    const double2 *mats;
+    const double2 *mats;         // complex64: each register's block holds float2 entries in its first half
     uint32_t mat_stride;
     int from_zero;               // registers start as |0..0>: build chunks instead of loading them
     const double2 *tables;       // F_PRUN factor tables (device memory), null when no run has any
     FStage stages[kFusedMaxStages];
     FOp ops[kFusedMaxOps];
-    double2 entries[kFusedMaxEntries];
+    double2 entries[kFusedMaxEntries];   // complex64 passes: float2 entries in the first half
 };
 static_assert(sizeof(FPassParams) <= 32764, "kernel parameter limit");
 
@@ -182,6 +182,9 @@ bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, st
                   std::vector<std::vector<FOpSource>> *srcs = nullptr, std::vector<PlannedPass> *pieces = nullptr,
                   std::vector<double2> *tables = nullptr);
 int clamp_local_bits(int k, int n);
+// Complex64 passes read their entries as float2: round count double2 entries
+// in place into the first half of the same memory.
+void entries_to_float(double2 *entries, size_t count);
 int fused_min_qubits();
 
 template <typename R>

@@ -65,6 +65,34 @@ def test_batch_matches_oracle(gpu_lib, oracle_lib, precision):
                 assert np.max(np.abs(zs[i] - _z_from_state(ref, n))) <= 1e-5, i
 
 
+@pytest.mark.parametrize("precision", [128, 64])
+def test_batch_phase_runs_and_sign_runs(gpu_lib, oracle_lib, precision):
+    """Batched passes with phase runs (QFT controlled phases: explicit terms,
+    since entries differ per register), runs of -1 phases (CZ, CCZ) with
+    controls on stage, thread and chunk qubits, and pairs / groups of
+    one-qubit gates, against the oracle."""
+    diag = ["z", "s", "t", "rz", "p", "rzz", "u1"]
+    circs = [(13, C.qft(13, seed=5)[0]), (14, C.qft(14, seed=6)[0])]
+    for seed, n in enumerate([12, 14]):
+        c = []
+        for blk in range(6):
+            c += C.random_circuit(n, 4, seed=300 + 10 * seed + blk, max_controls=1, gates=["u3", "h", "ry"])
+            c += C.random_circuit(n, 12, seed=400 + 10 * seed + blk, max_controls=2, gates=diag)
+        circs.append((n, c))
+    with qcs_b200.Batch(gpu_lib, precision) as b:
+        for n, circ in circs:
+            b.add_circuit(n, circ)
+        b.run()
+        for i, (n, circ) in enumerate(circs):
+            ref = _oracle_state(oracle_lib, n, circ)
+            got = b.statevector(i)
+            if precision == 128:
+                assert np.max(np.abs(got - ref)) <= 1e-12, i
+            else:
+                fid = abs(np.vdot(got, ref)) ** 2 / (np.vdot(got, got).real * np.vdot(ref, ref).real)
+                assert fid >= 1 - 1e-6, i
+
+
 def test_batch_parameter_updates(gpu_lib, oracle_lib):
     shapes = [(9, 2), (12, 3), (9, 2)]
     with qcs_b200.Batch(gpu_lib, 128) as b:
