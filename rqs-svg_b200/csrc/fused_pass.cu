@@ -123,6 +123,56 @@ struct BufferEntries
     __device__ __forceinline__ V operator[](int i) const { return __ldg(m + i); }
 };
 
+// A real 2x2 on one amplitude pair: each output component is a real
+// combination of the same component of the two inputs. Complex64 runs it on
+// the packed FP32 pipe (fma.rn.f32x2: both components per instruction), with
+// the same operation order and rounding as the scalar form.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+template <typename V>
+struct RealGate;
+
+template <>
+struct RealGate<double2>
+{
+    double m00, m01, m10, m11;
+    __device__ __forceinline__ RealGate(double a, double b, double c, double d) : m00(a), m01(b), m10(c), m11(d) {}
+    __device__ __forceinline__ void pair(double2 &y0, double2 &y1) const
+    {
+        const double2 x0 = y0, x1 = y1;
+        y0.x = fma(m00, x0.x, m01 * x1.x);
+        y0.y = fma(m00, x0.y, m01 * x1.y);
+        y1.x = fma(m11, x1.x, m10 * x0.x);
+        y1.y = fma(m11, x1.y, m10 * x0.y);
+    }
+};
+
+template <>
+struct RealGate<float2>
+{
+    unsigned long long c00, c01, c10, c11;   // each entry twice, packed
+    __device__ __forceinline__ RealGate(float a, float b, float c, float d)
+        : c00(pack2(a, a)), c01(pack2(b, b)), c10(pack2(c, c)), c11(pack2(d, d))
+    {
+    }
+    __device__ __forceinline__ void pair(float2 &y0, float2 &y1) const
+    {
+        const unsigned long long x0 = pack2(y0.x, y0.y), x1 = pack2(y1.x, y1.y);
+        unsigned long long t0, t1, r0, r1;
+        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t0) : "l"(c01), "l"(x1));
+        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t1) : "l"(c10), "l"(x0));
+        asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r0) : "l"(c00), "l"(x0), "l"(t0));
+        asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r1) : "l"(c11), "l"(x1), "l"(t1));
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(y0.x), "=f"(y0.y) : "l"(r0));
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(y1.x), "=f"(y1.y) : "l"(r1));
+    }
+};
+
 template <typename V, int B, typename M>
 __device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &e, uint32_t j0)
 {
@@ -168,14 +218,8 @@ __device__ __forceinline__ void apply_dense1r(V (&a)[R], const FOp &op, const M 
     const S m10 = static_cast<S>(e[2].x), m11 = static_cast<S>(e[3].x);
     const bool tok = (j0 & op.lcmask) == op.lcval;
     const uint32_t cm = op.smask, cv = op.sval;
-    auto pair = [&](int r) {
-        const int r1 = r | (1 << B);
-        const V x0 = a[r], x1 = a[r1];
-        a[r].x = fma(m00, x0.x, m01 * x1.x);
-        a[r].y = fma(m00, x0.y, m01 * x1.y);
-        a[r1].x = fma(m11, x1.x, m10 * x0.x);
-        a[r1].y = fma(m11, x1.y, m10 * x0.y);
-    };
+    const RealGate<V> g(m00, m01, m10, m11);
+    auto pair = [&](int r) { g.pair(a[r], a[r | (1 << B)]); };
     if (cm == 0 && op.lcmask == 0)
     {
         // no condition: straight-line code without per-slot predicates
@@ -206,17 +250,13 @@ __device__ __forceinline__ void apply_dense1rx4(V (&a)[R], const M &e)
     {
         const S m00 = static_cast<S>(e[4 * b].x), m01 = static_cast<S>(e[4 * b + 1].x);
         const S m10 = static_cast<S>(e[4 * b + 2].x), m11 = static_cast<S>(e[4 * b + 3].x);
+        const RealGate<V> g(m00, m01, m10, m11);
 #pragma unroll
         for (int r = 0; r < R; ++r)
         {
             if (r & (1 << b))
                 continue;
-            const int r1 = r | (1 << b);
-            const V x0 = a[r], x1 = a[r1];
-            a[r].x = fma(m00, x0.x, m01 * x1.x);
-            a[r].y = fma(m00, x0.y, m01 * x1.y);
-            a[r1].x = fma(m11, x1.x, m10 * x0.x);
-            a[r1].y = fma(m11, x1.y, m10 * x0.y);
+            g.pair(a[r], a[r | (1 << b)]);
         }
     }
 }
@@ -275,17 +315,13 @@ __device__ __forceinline__ void apply_dense1rx2(V (&a)[R], const M &e)
         const int b = i ? B1 : B0;
         const S m00 = static_cast<S>(e[4 * i].x), m01 = static_cast<S>(e[4 * i + 1].x);
         const S m10 = static_cast<S>(e[4 * i + 2].x), m11 = static_cast<S>(e[4 * i + 3].x);
+        const RealGate<V> g(m00, m01, m10, m11);
 #pragma unroll
         for (int r = 0; r < R; ++r)
         {
             if (r & (1 << b))
                 continue;
-            const int r1 = r | (1 << b);
-            const V x0 = a[r], x1 = a[r1];
-            a[r].x = fma(m00, x0.x, m01 * x1.x);
-            a[r].y = fma(m00, x0.y, m01 * x1.y);
-            a[r1].x = fma(m11, x1.x, m10 * x0.x);
-            a[r1].y = fma(m11, x1.y, m10 * x0.y);
+            g.pair(a[r], a[r | (1 << b)]);
         }
     }
 }
