@@ -173,10 +173,66 @@ struct RealGate<float2>
     }
 };
 
+// A complex 2x2 on one amplitude pair (y0, y1) <- (m00 y0 + m01 y1,
+// m10 y0 + m11 y1). Complex64 runs each output as one multiply and three
+// multiply-adds on the packed FP32 pipe: (re, im) += (m.re, m.re) * (x.re,
+// x.im) and (-m.im, m.im) * (x.im, x.re), in cmad2's order, so the results
+// are the same bit for bit.
+template <typename V>
+struct ComplexGate;
+
+template <>
+struct ComplexGate<double2>
+{
+    double2 m00, m01, m10, m11;
+    __device__ __forceinline__ ComplexGate(double2 a, double2 b, double2 c, double2 d) : m00(a), m01(b), m10(c), m11(d) {}
+    __device__ __forceinline__ void pair(double2 &y0, double2 &y1) const
+    {
+        const double2 x0 = y0, x1 = y1;
+        y0 = cmad2(m00, x0, m01, x1);
+        y1 = cmad2(m11, x1, m10, x0);
+    }
+};
+
+template <>
+struct ComplexGate<float2>
+{
+    // per entry: (re, re) and (-im, im), packed
+    unsigned long long r00, i00, r01, i01, r10, i10, r11, i11;
+    __device__ __forceinline__ ComplexGate(float2 a, float2 b, float2 c, float2 d)
+        : r00(pack2(a.x, a.x)), i00(pack2(-a.y, a.y)), r01(pack2(b.x, b.x)), i01(pack2(-b.y, b.y)),
+          r10(pack2(c.x, c.x)), i10(pack2(-c.y, c.y)), r11(pack2(d.x, d.x)), i11(pack2(-d.y, d.y))
+    {
+    }
+    // mr * v + mi * swap(v) + mr2 * w + mi2 * swap(w), in cmad2's order
+    static __device__ __forceinline__ unsigned long long mad(unsigned long long mr, unsigned long long mi,
+                                                             unsigned long long v, unsigned long long vs,
+                                                             unsigned long long mr2, unsigned long long mi2,
+                                                             unsigned long long w, unsigned long long ws)
+    {
+        unsigned long long t;
+        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(mi2), "l"(ws));
+        asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(t) : "l"(mr2), "l"(w));
+        asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(t) : "l"(mi), "l"(vs));
+        asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(t) : "l"(mr), "l"(v));
+        return t;
+    }
+    __device__ __forceinline__ void pair(float2 &y0, float2 &y1) const
+    {
+        const unsigned long long x0 = pack2(y0.x, y0.y), x0s = pack2(y0.y, y0.x);
+        const unsigned long long x1 = pack2(y1.x, y1.y), x1s = pack2(y1.y, y1.x);
+        const unsigned long long o0 = mad(r00, i00, x0, x0s, r01, i01, x1, x1s);
+        const unsigned long long o1 = mad(r11, i11, x1, x1s, r10, i10, x0, x0s);
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(y0.x), "=f"(y0.y) : "l"(o0));
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(y1.x), "=f"(y1.y) : "l"(o1));
+    }
+};
+
 template <typename V, int B, typename M>
 __device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &e, uint32_t j0)
 {
     const V m00 = cvt<V>(e[0]), m01 = cvt<V>(e[1]), m10 = cvt<V>(e[2]), m11 = cvt<V>(e[3]);
+    const ComplexGate<V> g(m00, m01, m10, m11);
     const bool tok = (j0 & op.lcmask) == op.lcval;
     const uint32_t cm = op.smask, cv = op.sval;
     if (cm == 0 && op.lcmask == 0)
@@ -186,10 +242,7 @@ __device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &
         {
             if (r & (1 << B))
                 continue;
-            const int r1 = r | (1 << B);
-            const V x0 = a[r], x1 = a[r1];
-            a[r] = cmad2(m00, x0, m01, x1);
-            a[r1] = cmad2(m11, x1, m10, x0);
+            g.pair(a[r], a[r | (1 << B)]);
         }
         return;
     }
@@ -200,10 +253,7 @@ __device__ __forceinline__ void apply_dense1(V (&a)[R], const FOp &op, const M &
             continue;
         if (tok && (r & cm) == cv)
         {
-            const int r1 = r | (1 << B);
-            const V x0 = a[r], x1 = a[r1];
-            a[r] = cmad2(m00, x0, m01, x1);
-            a[r1] = cmad2(m11, x1, m10, x0);
+            g.pair(a[r], a[r | (1 << B)]);
         }
     }
 }
@@ -269,15 +319,13 @@ __device__ __forceinline__ void apply_dense1x4(V (&a)[R], const M &e)
     {
         const V m00 = cvt<V>(e[4 * b]), m01 = cvt<V>(e[4 * b + 1]);
         const V m10 = cvt<V>(e[4 * b + 2]), m11 = cvt<V>(e[4 * b + 3]);
+        const ComplexGate<V> g(m00, m01, m10, m11);
 #pragma unroll
         for (int r = 0; r < R; ++r)
         {
             if (r & (1 << b))
                 continue;
-            const int r1 = r | (1 << b);
-            const V x0 = a[r], x1 = a[r1];
-            a[r] = cmad2(m00, x0, m01, x1);
-            a[r1] = cmad2(m11, x1, m10, x0);
+            g.pair(a[r], a[r | (1 << b)]);
         }
     }
 }
@@ -292,15 +340,13 @@ __device__ __forceinline__ void apply_dense1x2(V (&a)[R], const M &e)
         const int b = i ? B1 : B0;
         const V m00 = cvt<V>(e[4 * i]), m01 = cvt<V>(e[4 * i + 1]);
         const V m10 = cvt<V>(e[4 * i + 2]), m11 = cvt<V>(e[4 * i + 3]);
+        const ComplexGate<V> g(m00, m01, m10, m11);
 #pragma unroll
         for (int r = 0; r < R; ++r)
         {
             if (r & (1 << b))
                 continue;
-            const int r1 = r | (1 << b);
-            const V x0 = a[r], x1 = a[r1];
-            a[r] = cmad2(m00, x0, m01, x1);
-            a[r1] = cmad2(m11, x1, m10, x0);
+            g.pair(a[r], a[r | (1 << b)]);
         }
     }
 }
