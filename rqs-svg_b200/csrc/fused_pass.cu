@@ -330,7 +330,7 @@ __device__ __forceinline__ void apply_dense1x4(V (&a)[R], const M &e)
     }
 }
 
-// F_DENSE1X2 / F_DENSE1RX2: uncontrolled 2x2 gates on stage bits B0 < B1.
+// F_DENSE1X2: uncontrolled complex 2x2 gates on stage bits B0 < B1.
 template <typename V, int B0, int B1, typename M>
 __device__ __forceinline__ void apply_dense1x2(V (&a)[R], const M &e)
 {
@@ -341,27 +341,6 @@ __device__ __forceinline__ void apply_dense1x2(V (&a)[R], const M &e)
         const V m00 = cvt<V>(e[4 * i]), m01 = cvt<V>(e[4 * i + 1]);
         const V m10 = cvt<V>(e[4 * i + 2]), m11 = cvt<V>(e[4 * i + 3]);
         const ComplexGate<V> g(m00, m01, m10, m11);
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-        {
-            if (r & (1 << b))
-                continue;
-            g.pair(a[r], a[r | (1 << b)]);
-        }
-    }
-}
-
-template <typename V, int B0, int B1, typename M>
-__device__ __forceinline__ void apply_dense1rx2(V (&a)[R], const M &e)
-{
-    typedef decltype(V::x) S;
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-    {
-        const int b = i ? B1 : B0;
-        const S m00 = static_cast<S>(e[4 * i].x), m01 = static_cast<S>(e[4 * i + 1].x);
-        const S m10 = static_cast<S>(e[4 * i + 2].x), m11 = static_cast<S>(e[4 * i + 3].x);
-        const RealGate<V> g(m00, m01, m10, m11);
 #pragma unroll
         for (int r = 0; r < R; ++r)
         {
@@ -585,25 +564,15 @@ __device__ __forceinline__ void dispatch_dense2(V (&a)[R], const FOp &op, const 
     }
 }
 
-template <typename V, bool REAL, typename M>
+template <typename V, typename M>
 __device__ __forceinline__ void dispatch_x2(V (&a)[R], const FOp &op, const M &e)
 {
 #define QCSB_X2(b0, b1)                                                                                            \
-    case b0 * 4 + b1:                                                                                              \
-        if (REAL)                                                                                                  \
-            apply_dense1rx2<V, b0, b1>(a, e);                                                                      \
-        else                                                                                                       \
-            apply_dense1x2<V, b0, b1>(a, e);                                                                       \
-        break;
+    case b0 * 4 + b1: apply_dense1x2<V, b0, b1>(a, e); break;
     switch (op.b0 * 4 + op.b1)
     {
         QCSB_X2(0, 1) QCSB_X2(0, 2) QCSB_X2(0, 3) QCSB_X2(1, 2) QCSB_X2(1, 3)
-    default:
-        if (REAL)
-            apply_dense1rx2<V, 2, 3>(a, e);
-        else
-            apply_dense1x2<V, 2, 3>(a, e);
-        break;
+    default: apply_dense1x2<V, 2, 3>(a, e); break;
     }
 #undef QCSB_X2
 }
@@ -633,8 +602,7 @@ __device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, u
     case F_MULI: apply_muli<V>(a, op, j0); break;
     case F_DENSE1X4: apply_dense1x4<V>(a, e); break;
     case F_DENSE1RX4: apply_dense1rx4<V>(a, e); break;
-    case F_DENSE1X2: dispatch_x2<V, false>(a, op, e); break;
-    case F_DENSE1RX2: dispatch_x2<V, true>(a, op, e); break;
+    case F_DENSE1X2: dispatch_x2<V>(a, op, e); break;
     case F_SWAP1: dispatch_swap1<V>(a, op, j0); break;
     case F_DENSE2: dispatch_dense2<V>(a, op, e, j0); break;
     case F_SWAP2: dispatch_swap2<V>(a, op, j0); break;
@@ -1382,7 +1350,7 @@ int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m)
 
 int layer_entries(const std::vector<GateOp> &q, const FOpSource &src, uint8_t kind, double2 *m)
 {
-    if (kind == F_DENSE1X2 || kind == F_DENSE1RX2)
+    if (kind == F_DENSE1X2)
     {
         int off = 0;
         for (int b = 0; b < kStageBits; ++b)
@@ -1950,7 +1918,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                             ls.layer[b] = pp.ops[sops[pick[b]]];
                     if (pair)
                     {
-                        f.kind = all_real ? F_DENSE1RX2 : F_DENSE1X2;
+                        f.kind = F_DENSE1X2;
                         int nb = 0;
                         for (int b = 0; b < kStageBits; ++b)
                             if (pick[b] >= 0)

@@ -37,8 +37,7 @@ enum FKind : uint8_t
     F_PRUN = 12,      // a phase run inside a register stage (fields below)
     F_SIGNS = 13,     // a run of -1 phases (Z, CZ, CCZ): the next lcmask ops are its F_SIGNT terms
     F_SIGNT = 14,     // one -1 phase of an F_SIGNS: slots moff (16-bit mask) under the lc/gc condition
-    F_DENSE1X2 = 15,  // uncontrolled 2x2 gates on stage bits b0 < b1 (entries 0..3 for b0, 4..7 for b1)
-    F_DENSE1RX2 = 16, // the same with real entries
+    F_DENSE1X2 = 15,  // uncontrolled complex 2x2 gates on stage bits b0 < b1 (entries 0..3 for b0, 4..7 for b1)
 };
 
 // F_PRUN: a run of diagonal gates, each on at most one stage bit, applied to
@@ -170,7 +169,7 @@ int fop_entries(const GateOp &op, const FOp &f, bool swapped, double2 *m);
 int layer_entries(const std::vector<GateOp> &q, const FOpSource &src, uint8_t kind, double2 *m);
 inline bool layer_kind(uint8_t kind)
 {
-    return kind == F_DENSE1X4 || kind == F_DENSE1RX4 || kind == F_DENSE1X2 || kind == F_DENSE1RX2;
+    return kind == F_DENSE1X4 || kind == F_DENSE1RX4 || kind == F_DENSE1X2;
 }
 // Entries a queued op will need in a pass (the same counts, from the GateOp).
 int op_entry_count(const GateOp &op);
