@@ -452,20 +452,6 @@ __device__ __forceinline__ double flip_by(double x, uint32_t s)
 }
 __device__ __forceinline__ float flip_by(float x, uint32_t s) { return __uint_as_float(__float_as_uint(x) ^ s); }
 
-template <typename V>
-__device__ __forceinline__ void apply_neg(V (&a)[R], const FOp &op, uint32_t j0)
-{
-    const bool tok = (j0 & op.lcmask) == op.lcval;
-    const uint32_t cm = op.smask, cv = op.sval;
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-        if (tok && (r & cm) == cv)
-        {
-            a[r].x = flip(a[r].x);
-            a[r].y = flip(a[r].y);
-        }
-}
-
 // times i: (x, y) -> (-y, x); times -i: (x, y) -> (y, -x)
 template <typename V>
 __device__ __forceinline__ void apply_muli(V (&a)[R], const FOp &op, uint32_t j0)
@@ -598,7 +584,6 @@ __device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, u
     {
     case F_DENSE1: dispatch_dense1<V>(a, op, e, j0); break;
     case F_DENSE1R: dispatch_dense1r<V>(a, op, e, j0); break;
-    case F_NEG: apply_neg<V>(a, op, j0); break;
     case F_MULI: apply_muli<V>(a, op, j0); break;
     case F_DENSE1X4: apply_dense1x4<V>(a, e); break;
     case F_DENSE1RX4: apply_dense1rx4<V>(a, e); break;
@@ -611,86 +596,18 @@ __device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, u
     }
 }
 
-// A phase stage: a run of diagonal gates applied as one factor per
-// amplitude. Every diagonal gate multiplies the amplitudes whose bits match a
+// A phase run inside a register stage (F_PRUN), on amplitudes already in
+// registers. Every diagonal gate multiplies the amplitudes whose bits match a
 // pattern by a unit-modulus entry d. Split the pattern into the stage bits
-// (which pick one of the thread's 16 amplitudes r) and the rest (fixed for the
-// thread: its other local bits and the chunk). On the stage bits,
+// (which pick one of the thread's 16 amplitudes r) and the rest (fixed for
+// the thread: its other local bits and the chunk). On the stage bits,
 // [pattern matches r] expands by inclusion-exclusion into signed monomials
 // prod_{b in m} r_b, so d^[match] = prod over terms (d or conj d)^(monomial m
-// of r). The host emits one term (m, conjugate?, thread/chunk condition,
-// entry) per expansion member; the thread multiplies the terms that hold for
-// it into E[m], then amplitude r gets prod_{m subset of r} E[m] (a
-// subset-product transform, 32 complex products), whatever the number of
-// gates in the run.
-template <typename V, typename M>
-__device__ __forceinline__ void phase_stage(V *sb, const uint32_t (&pos)[R], uint32_t j0, uint64_t cbase,
-                                            const FOp *terms, int nterms, uint32_t monomials, const M &entry_at)
-{
-    V E[R];
-#pragma unroll
-    for (int m = 0; m < R; ++m)
-    {
-        E[m].x = 1;
-        E[m].y = 0;
-    }
-    for (int i = 0; i < nterms; ++i)
-    {
-        const FOp &t = terms[i];
-        if ((j0 & t.lcmask) != t.lcval || (cbase & t.gcmask) != t.gcval)
-            continue;
-        V d = cvt<V>(entry_at(t.moff));
-        if (t.b1)
-            d.y = -d.y;
-        switch (t.b0)
-        {
-#define QCSB_TERM(m)                                                                                               \
-    case m: E[m] = cmul(d, E[m]); break;
-            QCSB_TERM(0) QCSB_TERM(1) QCSB_TERM(2) QCSB_TERM(3) QCSB_TERM(4) QCSB_TERM(5) QCSB_TERM(6) QCSB_TERM(7)
-            QCSB_TERM(8) QCSB_TERM(9) QCSB_TERM(10) QCSB_TERM(11) QCSB_TERM(12) QCSB_TERM(13) QCSB_TERM(14)
-            QCSB_TERM(15)
-#undef QCSB_TERM
-        }
-    }
-    // monomials of at most one stage bit (a phase on one stage bit under a
-    // thread or chunk condition, the usual case): the product over subsets
-    // of r is a running product over r's bits, 15 complex products instead
-    // of the 32 of the general transform
-    constexpr uint32_t kLinear = 1u | (1u << 1) | (1u << 2) | (1u << 4) | (1u << 8);
-    if ((monomials & ~kLinear) == 0)
-    {
-        V single[kStageBits];
-#pragma unroll
-        for (int b = 0; b < kStageBits; ++b)
-        {
-            single[b] = E[1 << b];
-            E[1 << b] = cmul(E[0], single[b]);
-        }
-#pragma unroll
-        for (int r = 3; r < R; ++r)
-            if (r & (r - 1))
-                E[r] = cmul(E[r & (r - 1)], single[(r & 1) ? 0 : (r & 2) ? 1 : (r & 4) ? 2 : 3]);
-    }
-    else
-    {
-#pragma unroll
-        for (int b = 0; b < kStageBits; ++b)
-        {
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                if ((r >> b) & 1)
-                    E[r] = cmul(E[r ^ (1 << b)], E[r]);
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-        sb[pos[r]] = cmul(E[r], sb[pos[r]]);
-}
-
-// A phase run inside a register stage (F_PRUN), on amplitudes already in
-// registers: the terms of a phase stage restricted to monomials of at most
-// one stage bit, so five factors suffice (E[0] on every slot, E[1 + b] on the
-// slots with stage bit b). Factors start from the run's tables: the thread's
+// of r); the host emits one term (m, conjugate?, thread/chunk condition,
+// entry) per expansion member. A run holds only gates whose patterns have at
+// most one stage bit, so its monomials are 1 or r_b and five factors suffice
+// (E[0] on every slot, E[1 + b] on the slots with stage bit b); gates wholly
+// on the stage bits add 16 per-slot factors computed on the host. Factors start from the run's tables: the thread's
 // entry of its thread tables and, per 8-bit group of the chunk index, the
 // chunk's entry of the group tables (both built on the host from the terms
 // whose conditions fall entirely on those bits); the other terms follow the
@@ -895,21 +812,6 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
                         q ^= sbit[b];
                 return q;
             };
-            if (S.kind == 1)
-            {
-                uint32_t pos[R];
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    pos[r] = pos_of(r);
-                if (BATCH)
-                    phase_stage<V>(sb, pos, j0, cbase, p.ops + S.op_begin, S.op_end - S.op_begin, S.monomials,
-                                   [&](int off) { return __ldg(entries + off); });
-                else
-                    phase_stage<V>(sb, pos, j0, cbase, p.ops + S.op_begin, S.op_end - S.op_begin, S.monomials,
-                                   [&](int off) { return pool_entry<V>(p, off); });
-                __syncthreads();
-                continue;
-            }
             V a[R];
 #pragma unroll
             for (int r = 0; r < R; ++r)
@@ -1180,39 +1082,14 @@ void schedule_stages(const std::vector<GateOp> &q, const PlannedPass &pp, const 
     }
 }
 
-// Unitary diagonal gates on at most two targets join phase runs. A run is
-// applied as one phase stage when its weight reaches phase_run_min() (tuning
-// knob QCS_PHASE_RUN_MIN, default 6): a one-entry phase (CP, T, ...) weighs
-// 1, a diagonal with two or four entries (RZ, RZZ) 2, the ratio of their
-// costs as single ops; phases by -1 or +-i (Z, CZ, S) weigh 0, since alone
-// they are sign flips and exchanges. A phase stage has a fixed cost of about six
-// one-entry phases (the 16-way subset products), measured on B200.
-int phase_run_min()
-{
-    static const int v = [] {
-        const char *e = std::getenv("QCS_PHASE_RUN_MIN");
-        const int x = (e && e[0]) ? std::atoi(e) : 6;
-        return x >= 2 ? x : 2;
-    }();
-    return v;
-}
-
-// Phase runs whose gates each involve at most one stage bit run inside the
-// register stage (F_PRUN) instead of in a phase stage of their own, saving
-// the stage's shared-memory round trip (tuning knob QCS_PHASE_INLINE, default
-// on; 0 keeps every run in phase stages).
+// Unitary diagonal gates on at most two targets join phase runs, which run
+// inside the register stages: -1 phases as one F_SIGNS, gates on at most one
+// stage bit as one F_PRUN (table-fed factors), gates wholly on stage bits as
+// its per-slot factors, the rest one by one. A one-entry phase (CP, T, ...)
+// weighs 1, a diagonal with two or four entries (RZ, RZZ) 2; phases by -1 or
+// +-i (Z, CZ, S) weigh 0: an F_PRUN pays only with some weight in it.
 constexpr int kStageSlots = 1 << kStageBits;
 constexpr int kInlineRunMin = 2;          // gates an F_PRUN needs to beat single ops (about 200 instructions each)
-constexpr int kInlineOtherBudget = 48;    // complex products per thread, about a stage round trip
-
-bool phase_inline_enabled()
-{
-    static const bool v = [] {
-        const char *e = std::getenv("QCS_PHASE_INLINE");
-        return !(e && e[0] == '0');
-    }();
-    return v;
-}
 
 int phase_weight(const GateOp &op)
 {
@@ -1449,14 +1326,13 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 pos_in_stage[l] = nb;
                 sbits[nb++] = static_cast<uint8_t>(l);
             }
-        // the scheduled stage becomes register stages split by phase stages
-        auto open_stage = [&](uint8_t kind) -> FStage * {
+        // the scheduled stage becomes one register stage, opened at its first op
+        auto open_stage = [&]() -> FStage * {
             if (ns >= kFusedMaxStages)
                 return nullptr;
             FStage &S = prm.stages[ns++];
             std::memset(&S, 0, sizeof(S));
             std::memcpy(S.sbits, sbits, sizeof(sbits));
-            S.kind = kind;
             S.op_begin = static_cast<uint16_t>(nops);
             return &S;
         };
@@ -1539,14 +1415,6 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 src->push_back({r.qi, false});
             return true;
         };
-        auto emit_terms = [&](int qi) -> bool {
-            std::vector<TermRec> recs;
-            term_records(qi, recs);
-            for (const TermRec &r : recs)
-                if (!push_term(r))
-                    return false;
-            return true;
-        };
         FStage *cur = nullptr;
         std::vector<int> sops = cluster_diagonals(q, pp, stage_ops[si]);
         size_t idx = 0;
@@ -1557,21 +1425,18 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
             int weight = 0;
             while (idx >= singles_end && run_end < sops.size() && phase_run_op(q[pp.ops[sops[run_end]]]))
                 weight += phase_weight(q[pp.ops[sops[run_end++]]]);
-            // Ops of the run whose patterns hold at most one stage bit can run
-            // inside the register stage (F_PRUN: one complex product per term
-            // and thread, 32 per thread to apply); the others run one by one,
-            // which is cheap when their patterns hold several stage bits (a
-            // phase on 2^(4 - p) of the 16 slots). Only when those single ops
-            // would cost more than a stage's shared-memory round trip does
-            // the run become a phase stage. Clifford phases (Z, CZ, S) join a
-            // run that has other phases (alone each is a predicated op of ~200
-            // instructions, in a run a table entry), but a run of Clifford
-            // phases alone stays single ops: sign flips and exchanges on the
-            // integer pipe, where the run would take FP64 products, the
-            // busier pipe on passes of dense gates (measured).
+            // Ops of the run whose patterns hold at most one stage bit run as
+            // one F_PRUN (table entries or one complex product per term and
+            // thread, at most 48 per thread to apply), ops wholly on stage bits
+            // as its per-slot factors, the others one by one (a phase on
+            // 2^(4 - p) of the 16 slots). Clifford phases (S, Sdg) join a run
+            // that has other phases, but a run of them alone stays single ops
+            // (exchanges and sign flips on the integer pipe, where the run
+            // would take FP64 products, the busier pipe on passes of dense
+            // gates; measured).
             // -1 phases of the run (Z, CZ, CCZ) become one F_SIGNS; the rest of
             // the run is looked at again without them
-            if (run_end > idx && phase_inline_enabled())
+            if (run_end > idx)
             {
                 std::vector<int> signs, keep;
                 for (size_t ri = idx; ri < run_end; ++ri)
@@ -1580,7 +1445,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 {
                     if (nops + 1 + (int)signs.size() > kFusedMaxOps)
                         return false;
-                    if (cur == nullptr && (cur = open_stage(0)) == nullptr)
+                    if (cur == nullptr && (cur = open_stage()) == nullptr)
                         return false;
                     FOp &h = prm.ops[nops++];
                     std::memset(&h, 0, sizeof(h));
@@ -1639,14 +1504,14 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     continue;
                 }
             }
-            if (run_end - idx >= static_cast<size_t>(kInlineRunMin) && weight > 0 && phase_inline_enabled())
+            if (run_end - idx >= static_cast<size_t>(kInlineRunMin) && weight > 0)
             {
                 // lin: at most one stage bit in the pattern; slot: the whole
                 // pattern on stage bits (a fixed factor per slot, folded into
                 // 16 per-slot entries; not in batched passes, whose entries
                 // are per register); other: single ops
                 std::vector<int> lin, slot, other;
-                int other_cost = 0, wlin = 0;
+                int wlin = 0;
                 for (size_t ri = idx; ri < run_end; ++ri)
                 {
                     const GateOp &op = q[pp.ops[sops[ri]]];
@@ -1659,13 +1524,8 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     else if (tables && sbc == pattern_bits(op))
                         slot.push_back(sops[ri]);
                     else
-                    {
                         other.push_back(sops[ri]);
-                        // complex products per thread as a single op
-                        other_cost += phase_weight(op) == 0 ? 1 : op.na == 1 ? (kStageSlots >> sbc) : kStageSlots;
-                    }
                 }
-                if (other_cost <= kInlineOtherBudget)
                 {
                     const bool use_lin = lin.size() >= static_cast<size_t>(kInlineRunMin) && wlin > 0;
                     const bool use_slot = slot.size() >= 2 || (use_lin && !slot.empty());
@@ -1675,7 +1535,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     {
                         if (nops >= kFusedMaxOps)
                             return false;
-                        if (cur == nullptr && (cur = open_stage(0)) == nullptr)
+                        if (cur == nullptr && (cur = open_stage()) == nullptr)
                             return false;
                         const int head = nops++;
                         std::memset(&prm.ops[head], 0, sizeof(FOp));
@@ -1835,26 +1695,6 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     continue;
                 }
             }
-            if (weight >= phase_run_min())
-            {
-                // a phase stage: one term per inclusion-exclusion member
-                if (cur)
-                {
-                    cur->op_end = static_cast<uint16_t>(nops);
-                    cur = nullptr;
-                }
-                FStage *ph = open_stage(1);
-                if (ph == nullptr)
-                    return false;
-                for (size_t ri = idx; ri < run_end; ++ri)
-                    if (!emit_terms(pp.ops[sops[ri]]))
-                        return false;
-                ph->op_end = static_cast<uint16_t>(nops);
-                for (int t = ph->op_begin; t < nops; ++t)
-                    ph->monomials |= static_cast<uint16_t>(1u << prm.ops[t].b0);
-                idx = run_end;
-                continue;
-            }
             // uncontrolled 1-target dense gates on distinct stage bits run as one
             // F_DENSE1X4 / F_DENSE1RX4: gather them from the ops ahead that
             // commute with everything they are moved past
@@ -1908,7 +1748,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     const int ne = pair ? 8 : 4 * kStageBits;
                     if (nops >= kFusedMaxOps || nentries + ne > kFusedMaxEntries)
                         return false;
-                    if (cur == nullptr && (cur = open_stage(0)) == nullptr)
+                    if (cur == nullptr && (cur = open_stage()) == nullptr)
                         return false;
                     FOp &f = prm.ops[nops++];
                     std::memset(&f, 0, sizeof(f));
@@ -1950,7 +1790,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
             const GateOp &op = q[pp.ops[oi]];
             if (nops >= kFusedMaxOps)
                 return false;
-            if (cur == nullptr && (cur = open_stage(0)) == nullptr)
+            if (cur == nullptr && (cur = open_stage()) == nullptr)
                 return false;
             FOp &f = prm.ops[nops++];
             std::memset(&f, 0, sizeof(f));
@@ -1962,9 +1802,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 // one changed sub-index: a phase on the amplitudes whose
                 // control and target bits all match
                 const cplx e = op.mat[0];
-                if (e.re == -1.0 && e.im == 0.0)
-                    f.kind = F_NEG;
-                else if (e.re == 0.0 && (e.im == 1.0 || e.im == -1.0))
+                if (e.re == 0.0 && (e.im == 1.0 || e.im == -1.0))
                 {
                     f.kind = F_MULI;
                     f.b1 = e.im < 0.0 ? 1 : 0;

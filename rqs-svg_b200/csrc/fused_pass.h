@@ -27,9 +27,8 @@ enum FKind : uint8_t
     F_SWAP2 = 3,   // exchange sub-indices 01 and 10
     F_PHASE = 4,   // multiply by entry 0 where the condition bits match
     F_DIAG = 5,    // diagonal on one or two targets anywhere
-    F_TERM = 6,    // one factor of a phase stage (see fused_pass.cu)
+    F_TERM = 6,    // one term of an inline phase run (F_PRUN; see fused_pass.cu)
     F_DENSE1R = 7, // 2x2 with real entries (RY, H, real U3) on one stage bit
-    F_NEG = 8,     // F_PHASE by -1 (Z, CZ): sign flips, no multiplies
     F_MULI = 9,    // F_PHASE by i (b1 = 0) or -i (b1 = 1) (S, Sdg): exchanges and sign flips
     F_DENSE1X4 = 10,  // an uncontrolled 2x2 gate on each stage bit, in bit order (entries 4b..4b+3 for bit b;
                       // identities on bits without a gate)
@@ -82,18 +81,14 @@ struct FOp
 static_assert(sizeof(FOp) == 40, "FOp layout");
 
 // A stage applies ops [op_begin, op_end) on the amplitudes that differ in its
-// stage bits: a register stage (kind 0) runs the ops one by one on each
-// thread's 2^kStageBits amplitudes; a phase stage (kind 1) holds the F_TERM
-// factors of a run of diagonal gates.
+// stage bits: each thread loads its 2^kStageBits amplitudes into registers,
+// runs the ops one by one on them and stores them back.
 struct FStage
 {
     uint8_t sbits[kStageBits];   // local bit positions of the stage, ascending
     uint16_t op_begin, op_end;
-    uint8_t kind;
-    uint8_t pad;
-    uint16_t monomials;          // phase stages: bit m set when a term has monomial m
 };
-static_assert(sizeof(FStage) == 12, "FStage layout");
+static_assert(sizeof(FStage) == 8, "FStage layout");
 
 // Kernel parameters of one pass (passed as a __grid_constant__ block, under
 // the 32 KiB kernel parameter limit).
