@@ -120,6 +120,32 @@ def test_single_qubit_layers_merge_across_blockers(gpu_lib, oracle_lib, n):
     assert np.max(np.abs(got_b - ref0)) <= 1e-12
 
 
+@pytest.mark.parametrize("precision", [128, 64])
+def test_repeated_and_interleaved_runs_on_one_simulator(gpu_lib, oracle_lib, precision):
+    """One simulator runs the same circuit again, another circuit in between,
+    and the same gates with other parameters (the executor's tables and pass
+    parameters are rebuilt or reused across flushes): every result against
+    the oracle."""
+    n = 14
+    a = C.layered_u3_cz_cx_toffoli(n, 3, seed=11) + C.qft(n, seed=12)[0]
+    b = C.random_circuit(n, 120, seed=13, max_controls=2)
+    a2 = [(g[0], tuple(x + 0.25 for x in g[1]), g[2], g[3], g[4]) for g in a]   # same gates, other angles
+    refs = {}
+    for name, circ in (("a", a), ("b", b), ("a2", a2)):
+        with qcs_b200.Simulator(oracle_lib, n) as sim:
+            sim.run(circ)
+            refs[name] = sim.statevector()
+    with qcs_b200.Simulator(gpu_lib, n, fusion=FUSION_GREEDY, precision=precision) as sim:
+        for name, circ in (("a", a), ("a", a), ("b", b), ("a", a), ("a2", a2), ("a", a)):
+            sim.set_state("zero")
+            sim.run(circ)
+            got = sim.statevector()
+            if precision == 128:
+                assert np.max(np.abs(got - refs[name])) <= 1e-12, name
+            else:
+                assert qcs_b200.fidelity(got, refs[name]) >= 1 - 1e-6, name
+
+
 @pytest.mark.parametrize("mode", MODES)
 def test_twenty_qubit_layered_and_qft(gpu_lib, oracle_lib, mode):
     for circ in (C.layered_u3_cz(20, 6, seed=3), C.qft(20, seed=4)[0], C.layered_u3_cz_cx_toffoli(20, 4, seed=5)):
