@@ -535,21 +535,6 @@ __device__ __forceinline__ void dispatch_swap1(V (&a)[R], const FOp &op, uint32_
     }
 }
 
-// (b0, b1) with b0 < b1 encoded as b0 * 4 + b1
-template <typename V, typename M>
-__device__ __forceinline__ void dispatch_dense2(V (&a)[R], const FOp &op, const M &e, uint32_t j0)
-{
-    switch (op.b0 * 4 + op.b1)
-    {
-    case 1: apply_dense2<V, 0, 1>(a, op, e, j0); break;
-    case 2: apply_dense2<V, 0, 2>(a, op, e, j0); break;
-    case 3: apply_dense2<V, 0, 3>(a, op, e, j0); break;
-    case 6: apply_dense2<V, 1, 2>(a, op, e, j0); break;
-    case 7: apply_dense2<V, 1, 3>(a, op, e, j0); break;
-    default: apply_dense2<V, 2, 3>(a, op, e, j0); break;
-    }
-}
-
 template <typename V, typename M>
 __device__ __forceinline__ void dispatch_x2(V (&a)[R], const FOp &op, const M &e)
 {
@@ -563,25 +548,71 @@ __device__ __forceinline__ void dispatch_x2(V (&a)[R], const FOp &op, const M &e
 #undef QCSB_X2
 }
 
+// Where a stage's slots live in shared memory: slot s of this thread is at
+// p0 ^ (XOR of sbit[b] over the bits b of s).
 template <typename V>
-__device__ __forceinline__ void dispatch_swap2(V (&a)[R], const FOp &op, uint32_t j0)
+struct StageSlots
 {
-    switch (op.b0 * 4 + op.b1)
+    V *sb;
+    uint32_t p0;
+    uint32_t sbit[kStageBits];
+};
+
+// Two-target ops are compiled for slot bits (0, 1) only: for other stage bits
+// (b0, b1) register r holds slot perm(r) (bits b0, b1, then the other two
+// ascending) during the op, moved through the thread's own shared-memory
+// positions (no other thread reads them: no barrier), and back. The host
+// writes the op's stage-bit condition in that order.
+template <typename V, typename M>
+__device__ __forceinline__ void apply_two_target(V (&a)[R], const FOp &op, const M &e, uint32_t j0,
+                                                 const StageSlots<V> &ss)
+{
+    const bool move = op.b0 != 0 || op.b1 != 1;
+    const uint32_t rest = 15u & ~((1u << op.b0) | (1u << op.b1));
+    const uint32_t c0 = static_cast<uint32_t>(__ffs(rest) - 1), c1 = static_cast<uint32_t>(31 - __clz(rest));
+    auto sbit_of = [&](uint32_t b) {
+        return b == 0 ? ss.sbit[0] : b == 1 ? ss.sbit[1] : b == 2 ? ss.sbit[2] : ss.sbit[3];
+    };
+    const uint32_t q0 = sbit_of(op.b0), q1 = sbit_of(op.b1), q2 = sbit_of(c0), q3 = sbit_of(c1);
+    auto pos = [&](int r) {
+        return ss.p0 ^ ((r & 1) ? ss.sbit[0] : 0u) ^ ((r & 2) ? ss.sbit[1] : 0u) ^ ((r & 4) ? ss.sbit[2] : 0u) ^
+               ((r & 8) ? ss.sbit[3] : 0u);
+    };
+    auto pos_perm = [&](int r) {
+        return ss.p0 ^ ((r & 1) ? q0 : 0u) ^ ((r & 2) ? q1 : 0u) ^ ((r & 4) ? q2 : 0u) ^ ((r & 8) ? q3 : 0u);
+    };
+    if (move)
     {
-    case 1: apply_swap2<V, 0, 1>(a, op, j0); break;
-    case 2: apply_swap2<V, 0, 2>(a, op, j0); break;
-    case 3: apply_swap2<V, 0, 3>(a, op, j0); break;
-    case 6: apply_swap2<V, 1, 2>(a, op, j0); break;
-    case 7: apply_swap2<V, 1, 3>(a, op, j0); break;
-    default: apply_swap2<V, 2, 3>(a, op, j0); break;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            ss.sb[pos(r)] = a[r];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            a[r] = ss.sb[pos_perm(r)];
+    }
+    if (op.kind == F_SWAP2)
+        apply_swap2<V, 0, 1>(a, op, j0);
+    else
+        apply_dense2<V, 0, 1>(a, op, e, j0);
+    if (move)
+    {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            ss.sb[pos_perm(r)] = a[r];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            a[r] = ss.sb[pos(r)];
     }
 }
 
 template <typename V, typename M>
-__device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, uint32_t j0, uint64_t cbase)
+__device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, uint32_t j0, uint64_t cbase,
+                                         const StageSlots<V> &ss)
 {
     switch (op.kind)
     {
+    case F_DENSE2:
+    case F_SWAP2: apply_two_target<V>(a, op, e, j0, ss); break;
     case F_DENSE1: dispatch_dense1<V>(a, op, e, j0); break;
     case F_DENSE1R: dispatch_dense1r<V>(a, op, e, j0); break;
     case F_MULI: apply_muli<V>(a, op, j0); break;
@@ -589,8 +620,6 @@ __device__ __forceinline__ void apply_op(V (&a)[R], const FOp &op, const M &e, u
     case F_DENSE1RX4: apply_dense1rx4<V>(a, e); break;
     case F_DENSE1X2: dispatch_x2<V>(a, op, e); break;
     case F_SWAP1: dispatch_swap1<V>(a, op, j0); break;
-    case F_DENSE2: dispatch_dense2<V>(a, op, e, j0); break;
-    case F_SWAP2: dispatch_swap2<V>(a, op, j0); break;
     case F_PHASE: apply_phase<V>(a, op, e, j0); break;
     default: apply_diag<V>(a, op, e, j0, cbase); break;
     }
@@ -816,6 +845,7 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
 #pragma unroll
             for (int r = 0; r < R; ++r)
                 a[r] = sb[pos_of(r)];
+            const StageSlots<V> ss{sb, p0, {sbit[0], sbit[1], sbit[2], sbit[3]}};
             for (int oi = S.op_begin; oi < S.op_end; ++oi)
             {
                 const FOp &op = p.ops[oi];
@@ -855,9 +885,9 @@ __global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
                 if ((cbase & op.gcmask) != op.gcval)
                     continue;
                 if (BATCH)
-                    apply_op<V>(a, op, BufferEntries<V>{entries + op.moff}, j0, cbase);
+                    apply_op<V>(a, op, BufferEntries<V>{entries + op.moff}, j0, cbase, ss);
                 else
-                    apply_op<V>(a, op, PoolEntries<V>{p, op.moff}, j0, cbase);
+                    apply_op<V>(a, op, PoolEntries<V>{p, op.moff}, j0, cbase, ss);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r)
@@ -1894,6 +1924,16 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
             f.sval = static_cast<uint8_t>(sv);
             f.gcmask = gcm;
             f.gcval = gcv;
+            if (f.kind == F_DENSE2 || f.kind == F_SWAP2)
+            {
+                // the kernel runs it with slot bits b0, b1 moved to 0, 1 and the
+                // other two after them: its stage-bit condition in that order
+                const uint32_t rest = 15u & ~((1u << f.b0) | (1u << f.b1));
+                const int c0 = __builtin_ctz(rest), c1 = 31 - __builtin_clz(rest);
+                auto remap = [&](uint32_t m) { return (((m >> c0) & 1u) << 2) | (((m >> c1) & 1u) << 3); };
+                f.smask = static_cast<uint8_t>(remap(sm));
+                f.sval = static_cast<uint8_t>(remap(sv));
+            }
                 }
         if (cur)
             cur->op_end = static_cast<uint16_t>(nops);
