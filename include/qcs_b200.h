@@ -269,6 +269,36 @@ int qcs_b200_batch_get_statevector(qcs_b200_batch *batch, uint32_t index, double
 int qcs_b200_batch_get_info(qcs_b200_batch *batch, qcs_b200_batch_info *info);
 
 /*
+ * How the fused planner (greedy mode, 11 local qubits, 256 gates per pass)
+ * would run a gate list on a register of num_qubits, computed on the host
+ * without a GPU: for inspecting plans and testing the planner. This entry
+ * point has no counterpart in the reference library. Gates are given as in
+ * a batch (any number of targets the API allows); uncontrolled SWAPs only
+ * relabel qubits, as in the simulator's fused modes. kinds[] counts the ops
+ * of the passes by kind:
+ *    0 dense 2x2 (one gate)            1 X/CX exchange
+ *    2 dense 4x4 (two targets)         3 controlled SWAP exchange
+ *    4 phase                           5 diagonal on one or two targets
+ *    6 term of a phase run             7 real 2x2
+ *    9 phase by +-i                   10 four one-qubit gates (complex)
+ *   11 four one-qubit gates (real)    12 phase run (table-fed factors)
+ *   13 run of -1 phases               14 one -1 phase of such a run
+ *   15 two one-qubit gates (complex)
+ */
+#define QCS_B200_PLAN_KINDS 24
+typedef struct qcs_b200_plan_summary
+{
+    uint32_t passes;            /* fused passes */
+    uint32_t plain_gates;       /* gates left to the one-kernel-per-gate path */
+    uint32_t stages;            /* register stages over all passes */
+    uint32_t ops;               /* pass ops over all passes (terms included) */
+    uint32_t kinds[QCS_B200_PLAN_KINDS];
+    uint64_t table_entries;     /* complex entries of the phase-run factor tables */
+} qcs_b200_plan_summary;
+int qcs_b200_plan_summary_get(int num_qubits, const qcs_b200_gate *gates, uint64_t num_gates,
+                              qcs_b200_plan_summary *summary);
+
+/*
  * Allocation-free squared-norm sums of a complex128 state vector held in the
  * caller's device memory. This entry point has no counterpart in the
  * reference library.

@@ -801,6 +801,21 @@ extern "C" int qcs_b200_batch_add_circuit(qcs_b200_batch *batch, int num_qubits,
     });
 }
 
+namespace qcsb
+{
+void plan_summary(int n, const qcs_b200_gate *gates, uint64_t count, qcs_b200_plan_summary &out);
+}
+
+extern "C" int qcs_b200_plan_summary_get(int num_qubits, const qcs_b200_gate *gates, uint64_t num_gates,
+                                         qcs_b200_plan_summary *summary)
+{
+    return guarded([&] {
+        if (summary == nullptr)
+            throw std::runtime_error("plan_summary: summary must not be NULL");
+        qcsb::plan_summary(num_qubits, gates, num_gates, *summary);
+    });
+}
+
 extern "C" int qcs_b200_batch_set_parameters(qcs_b200_batch *batch, const double *params, uint64_t count)
 {
     return guarded([&] { batch_of(batch).set_parameters(params, count); });

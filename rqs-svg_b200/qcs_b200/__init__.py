@@ -85,6 +85,23 @@ class BatchGate(ctypes.Structure):
     ]
 
 
+PLAN_KINDS = 24
+PLAN_KIND_NAMES = {0: "dense1", 1: "x", 2: "dense2", 3: "cswap", 4: "phase", 5: "diag", 6: "term",
+                   7: "dense1_real", 9: "phase_i", 10: "group4", 11: "group4_real", 12: "phase_run",
+                   13: "sign_run", 14: "sign_term", 15: "group2"}
+
+
+class PlanSummary(ctypes.Structure):
+    _fields_ = [
+        ("passes", ctypes.c_uint32),
+        ("plain_gates", ctypes.c_uint32),
+        ("stages", ctypes.c_uint32),
+        ("ops", ctypes.c_uint32),
+        ("kinds", ctypes.c_uint32 * PLAN_KINDS),
+        ("table_entries", ctypes.c_uint64),
+    ]
+
+
 class BatchInfo(ctypes.Structure):
     _fields_ = [
         ("circuits", ctypes.c_uint32),
@@ -196,6 +213,8 @@ class Library:
             "qcs_b200_batch_expectation_z": [_P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
             "qcs_b200_batch_get_statevector": [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
             "qcs_b200_batch_get_info": [_P, ctypes.POINTER(BatchInfo)],
+            "qcs_b200_plan_summary_get": [ctypes.c_int, ctypes.POINTER(BatchGate), ctypes.c_uint64,
+                                          ctypes.POINTER(PlanSummary)],
         }
         for name, (np_, nt) in GATES.items():
             if name == "global_phase":
@@ -484,6 +503,18 @@ class CostModel:
         p = np.ascontiguousarray(params, dtype=np.float32)
         s = np.ascontiguousarray(scaling, dtype=np.float32)
         self.lib.call("qcs_b200_cost_model_set_params", self.h, _fptr(p), _fptr(s))
+
+
+def plan_summary(lib: "Library", num_qubits: int, circuit) -> dict:
+    """How the greedy fused planner would run a circuit (host only, no GPU):
+    passes, plain gates, stages, ops, ops by kind name, table entries."""
+    arr = Batch.encode(circuit)
+    out = PlanSummary()
+    lib.call("qcs_b200_plan_summary_get", num_qubits, arr.ctypes.data_as(ctypes.POINTER(BatchGate)),
+             ctypes.c_uint64(len(circuit)), ctypes.byref(out))
+    kinds = {name: int(out.kinds[i]) for i, name in PLAN_KIND_NAMES.items()}
+    return {"passes": out.passes, "plain_gates": out.plain_gates, "stages": out.stages, "ops": out.ops,
+            "kinds": kinds, "table_entries": int(out.table_entries)}
 
 
 def fidelity(a: np.ndarray, b: np.ndarray) -> float:
