@@ -1534,7 +1534,12 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     continue;
                 }
             }
-            if (run_end - idx >= static_cast<size_t>(kInlineRunMin) && weight > 0)
+            // (a run of one gate wholly on stage bits also goes in: 16 per-slot
+            // factors cost less than a predicated phase on all 16 slots)
+            const bool lone_slot_op = run_end - idx == 1 && tables != nullptr && weight > 0 &&
+                                      pattern_stage_bits(q[pp.ops[sops[idx]]]) == pattern_bits(q[pp.ops[sops[idx]]]) &&
+                                      pattern_bits(q[pp.ops[sops[idx]]]) >= 2;
+            if ((run_end - idx >= static_cast<size_t>(kInlineRunMin) || lone_slot_op) && weight > 0)
             {
                 // lin: at most one stage bit in the pattern; slot: the whole
                 // pattern on stage bits (a fixed factor per slot, folded into
@@ -1558,7 +1563,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 }
                 {
                     const bool use_lin = lin.size() >= static_cast<size_t>(kInlineRunMin) && wlin > 0;
-                    const bool use_slot = slot.size() >= 2 || (use_lin && !slot.empty());
+                    const bool use_slot = !slot.empty();
                     if (!use_slot)
                         other.insert(other.end(), slot.begin(), slot.end());
                     if (use_lin || use_slot)
