@@ -724,11 +724,13 @@ __device__ __forceinline__ void phase_inline(V (&a)[R], const FOp &head, const F
 }
 
 // One CTA per chunk at a time; blockDim.x == 2^(k - kStageBits) <= 128, so
-// that three CTAs (12 warps, 3 x 64 KB of double-buffered chunks) share an SM.
+// that three CTAs (12 warps, 3 x 64 KB of double-buffered chunks) share an SM
+// for complex128 (168 registers) and four for complex64 (128 registers; the
+// batched complex64 pass measured 8% faster at 128 than at 168).
 // BATCH: the work items are the chunks of many registers of the same size
 // and plan (see FPassParams), each with its own gate entries.
 template <typename Real, bool BATCH>
-__global__ void __launch_bounds__(128, (sizeof(Real) == 8 || BATCH) ? 3 : 4)
+__global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4)
     fused_pass_kernel(const __grid_constant__ FPassParams p)
 {
     typedef typename Cx<Real>::T V;
