@@ -413,6 +413,8 @@ def main():
     # end to end through the C ABI: host wall clock, host inputs (gate
     # parameters, sampler uniforms) in, results (<Z>, shots) out
     barrier(dist)
+    run_step(sim, circuit, shots=draws_shots)   # untimed warm-up of the host path
+    sim.synchronize()
     e2e = []
     for _ in range(args.steps):
         t0 = time.perf_counter()

@@ -150,7 +150,8 @@ uint32_t Batch::add_circuit(int n, const qcs_b200_gate *gates, uint32_t count)
         if (std::memchr(in.name, '\0', sizeof(in.name)) == nullptr)
             throw std::runtime_error(strformat("gate %u: name is not NUL-terminated", i));
         std::memcpy(g.name, in.name, sizeof(g.name));
-        g.np = gate_nparams(g.name);
+        g.id = gate_id(g.name);
+        g.np = gate_nparams(g.id);
         const int arity = gate_arity(g.name);
         if (arity > 2)
             throw std::runtime_error(strformat("gate %u (%s): batches take gates on at most two targets", i, g.name));
@@ -289,7 +290,7 @@ void Batch::fill_group_range(const Group &g, size_t first, size_t last)
         for (size_t i = 0; i < c.gates.size(); ++i)
         {
             const Gate &gt = c.gates[i];
-            ops[i] = op_like(g.shape[i], gate_matrix(gt.name, gt.params, gt.np));
+            ops[i] = op_like(g.shape[i], gate_matrix(gt.id, gt.params, gt.np));
         }
         double2 *block = mats_host_ + g.mats_off + (uint64_t)s * g.stride;
         for (const Pass &p : g.passes)
@@ -447,7 +448,7 @@ void Batch::build()
         uint64_t sig = mix(1469598103934665603ull, (uint64_t)c.n);
         for (const Gate &gt : c.gates)
         {
-            const GateMatrix gm = gate_matrix(gt.name, kProbe, gt.np);
+            const GateMatrix gm = gate_matrix(gt.id, kProbe, gt.np);
             const GateOp op = make_gate_op(gm, gt.tq, gt.cmask, gt.cval);
             sig = mix(sig, (uint64_t)op.nt | ((uint64_t)op.na << 8) | ((uint64_t)op.diag << 16));
             for (int i = 0; i < op.nt; ++i)

@@ -54,6 +54,7 @@ class Batch
     struct Gate
     {
         char name[16];
+        int id;      // gate table index (looked up once, at add_circuit)
         int np;
         double params[4];
         int tq[kMaxTargets];
