@@ -195,6 +195,9 @@ void Simulator::dispose()
     cudaFree(zsum_partials_);
     cudaFree(zsum_result_);
     cudaFree(staging_dev_);
+    cudaFree(sampler_dev_);
+    sampler_dev_ = nullptr;
+    sampler_bytes_ = 0;
     if (host_pinned_)
         cudaFreeHost(host_pinned_);
     if (staging_host_)
@@ -686,18 +689,27 @@ void Simulator::sample(uint32_t num_shots, uint64_t *out)
     std::uniform_real_distribution<double> dist(0.0, 1.0);
     for (size_t k = 0; k < nu; ++k)
         u[k] = dist(engine_);
-    double *tree = nullptr, *u_dev = nullptr;
-    uint64_t *bits_dev = nullptr;
-    QCSB_CUDA(cudaMallocAsync(&tree, tree_bytes, stream_));
-    QCSB_CUDA(cudaMallocAsync(&u_dev, sizeof(double) * std::max<size_t>(nu, 1), stream_));
-    QCSB_CUDA(cudaMallocAsync(&bits_dev, sizeof(uint64_t) * std::max<uint32_t>(num_shots, 1), stream_));
+    // one device buffer: tree, then uniforms, then outcomes (256-byte aligned)
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t u_off = up(tree_bytes), bits_off = u_off + up(sizeof(double) * std::max<size_t>(nu, 1));
+    const size_t need_dev = bits_off + up(sizeof(uint64_t) * std::max<uint32_t>(num_shots, 1));
+    if (need_dev > sampler_bytes_)
+    {
+        QCSB_CUDA(cudaStreamSynchronize(stream_));
+        cudaFree(sampler_dev_);
+        sampler_dev_ = nullptr;
+        sampler_bytes_ = 0;
+        QCSB_CUDA(cudaMalloc(&sampler_dev_, need_dev));
+        sampler_bytes_ = need_dev;
+    }
+    char *base = static_cast<char *>(sampler_dev_);
+    double *tree = reinterpret_cast<double *>(base);
+    double *u_dev = reinterpret_cast<double *>(base + u_off);
+    uint64_t *bits_dev = reinterpret_cast<uint64_t *>(base + bits_off);
     QCSB_CUDA(cudaMemcpyAsync(u_dev, u, sizeof(double) * nu, cudaMemcpyHostToDevice, stream_));
     stats.kernel_launches += QCSB_ON_STATE(launch_sampler, n_, perm_l2p_.data(), num_shots, u_dev, bits_dev, tree, split, stream_);
     QCSB_CUDA(cudaStreamSynchronize(stream_));   // the pinned buffer is reused below
     QCSB_CUDA(cudaMemcpyAsync(host_pinned_, bits_dev, sizeof(uint64_t) * num_shots, cudaMemcpyDeviceToHost, stream_));
-    QCSB_CUDA(cudaFreeAsync(tree, stream_));
-    QCSB_CUDA(cudaFreeAsync(u_dev, stream_));
-    QCSB_CUDA(cudaFreeAsync(bits_dev, stream_));
     QCSB_CUDA(cudaStreamSynchronize(stream_));
     std::memcpy(out, host_pinned_, sizeof(uint64_t) * num_shots);
 }

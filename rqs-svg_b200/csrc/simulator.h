@@ -172,6 +172,11 @@ class Simulator
     double2 *staging_dev_ = nullptr;
     double2 *staging_host_ = nullptr;
     uint64_t staging_count_ = 0;
+    // sampler: marginal tree, uniforms and outcomes, kept between calls and
+    // grown when a call needs more (per-call stream-ordered allocations made
+    // some calls stall for tenths of a second)
+    void *sampler_dev_ = nullptr;
+    size_t sampler_bytes_ = 0;
 };
 
 // Fused execution of a queue of gate operations (fused_pass.cu). Returns the
