@@ -1151,61 +1151,75 @@ bool phase_run_op(const GateOp &op)
     return true;
 }
 
-// Within one stage, move diagonal ops later past the non-diagonal ops they
-// commute with, so that they gather into runs: when a held diagonal meets an
-// op it does not commute with, every held diagonal that this or a later op of
-// the stage blocks is placed there (keeping the runs whole, and the ops after
-// them together), and the ones nothing blocks sink to the end of the stage
-// (a QFT's phases to qubits outside the stage). Every non-commuting pair keeps
-// its order; diagonal ops commute with one another.
+// Within one stage, gather the diagonal ops into as few runs as their order
+// allows. A diagonal may sit in any gap between the stage's other ops from
+// after the last earlier op it does not commute with to before the first later
+// one: an interval of gaps. The fewest gaps that meet every interval are
+// found greedily (by interval end), and each diagonal goes to the LATEST of
+// them inside its interval, so that runs sit between whole groups of gates
+// (the phases of split one-qubit gates before and after a layer) and those
+// that nothing later blocks sink to the end of the stage (a QFT's phases to
+// qubits outside the stage). Every non-commuting pair keeps its order;
+// diagonal ops commute with one another.
 std::vector<int> cluster_diagonals(const std::vector<GateOp> &q, const PlannedPass &pp, const std::vector<int> &ops)
 {
     const size_t m = ops.size();
     std::vector<OpClass> cls(m);
     std::vector<bool> diag(m);
+    std::vector<size_t> rank(m);   // non-diagonal ops before position i
+    size_t nd = 0;
     for (size_t i = 0; i < m; ++i)
     {
         cls[i] = classify(q[pp.ops[ops[i]]]);
         diag[i] = phase_run_op(q[pp.ops[ops[i]]]);
+        rank[i] = nd;
+        if (!diag[i])
+            ++nd;
     }
-    // held diagonal h is blocked at or after position i by a non-diagonal op
-    auto blocked_from = [&](size_t h, size_t i) {
-        for (size_t j = i; j < m; ++j)
-            if (!diag[j] && !commute(cls[h], cls[j]))
-                return true;
-        return false;
-    };
+    // gap g lies before the g-th non-diagonal op (g == nd: the stage's end)
+    std::vector<size_t> lo(m, 0), hi(m, nd);
+    std::vector<size_t> dg;
+    for (size_t i = 0; i < m; ++i)
+    {
+        if (!diag[i])
+            continue;
+        dg.push_back(i);
+        for (size_t j = i; j-- > 0;)
+            if (!diag[j] && !commute(cls[i], cls[j]))
+            {
+                lo[i] = rank[j] + 1;
+                break;
+            }
+        for (size_t j = i + 1; j < m; ++j)
+            if (!diag[j] && !commute(cls[i], cls[j]))
+            {
+                hi[i] = rank[j];
+                break;
+            }
+    }
+    std::vector<size_t> by_end = dg;
+    std::stable_sort(by_end.begin(), by_end.end(), [&](size_t a, size_t b) { return hi[a] < hi[b]; });
+    std::vector<size_t> points;   // ascending
+    for (size_t d : by_end)
+        if (points.empty() || points.back() < lo[d])
+            points.push_back(hi[d]);
+    std::vector<std::vector<int>> at(nd + 1);
+    for (size_t d : dg)
+    {
+        // the latest chosen gap inside [lo, hi]
+        const auto it = std::upper_bound(points.begin(), points.end(), hi[d]);
+        at[*(it - 1)].push_back(ops[d]);
+    }
     std::vector<int> out;
-    std::vector<size_t> held;
     out.reserve(m);
     for (size_t i = 0; i < m; ++i)
     {
         if (diag[i])
-        {
-            held.push_back(i);
             continue;
-        }
-        bool blocks = false;
-        for (size_t h : held)
-            blocks = blocks || !commute(cls[h], cls[i]);
-        if (blocks)
-        {
-            // every held diagonal that this or a later op blocks goes here, in
-            // one run; those that nothing later blocks sink to the stage's end
-            std::vector<size_t> still;
-            for (size_t h : held)
-            {
-                if (blocked_from(h, i))
-                    out.push_back(ops[h]);
-                else
-                    still.push_back(h);
-            }
-            held.swap(still);
-        }
+        out.insert(out.end(), at[rank[i]].begin(), at[rank[i]].end());
         out.push_back(ops[i]);
     }
-    for (size_t h : held)
-        out.push_back(ops[h]);
+    out.insert(out.end(), at[nd].begin(), at[nd].end());
     return out;
 }
 
