@@ -961,6 +961,83 @@ bool is_real(const GateOp &op)
     return true;
 }
 
+// Uncontrolled X gates move later in the queue, each until an op it cannot
+// pass, where it is placed (or until the end): an X on qubit q passes an op
+// that does not touch q; a diagonal op or a control on q with that bit of its
+// pattern flipped (X D X is D with the pattern bit flipped; likewise a
+// control's value); a controlled X on target q unchanged (X commutes with X);
+// and an uncontrolled 2x2 on q takes it in as a column swap (M X), where it
+// ends. Two X on one qubit cancel. Every change is exact (no arithmetic), and
+// X gates on scattered qubits (the basis-state input of a QFT) no longer hold
+// local bits of a pass that the gates after them need.
+std::vector<GateOp> defer_x(const std::vector<GateOp> &q)
+{
+    std::vector<GateOp> out;
+    out.reserve(q.size());
+    uint64_t pending = 0;
+    auto x_op = [](int t) {
+        GateOp x;
+        x.nt = 1;
+        x.tq[0] = t;
+        x.na = 2;
+        x.act[0] = 0;
+        x.act[1] = 1;
+        x.mat[0] = cplx{0.0, 0.0};
+        x.mat[1] = cplx{1.0, 0.0};
+        x.mat[2] = cplx{1.0, 0.0};
+        x.mat[3] = cplx{0.0, 0.0};
+        return x;
+    };
+    for (const GateOp &in : q)
+    {
+        if (is_x(in) && in.cmask == 0)
+        {
+            pending ^= 1ull << in.tq[0];
+            continue;
+        }
+        GateOp op = in;
+        op.cval ^= op.cmask & pending;
+        for (int i = 0; i < op.nt; ++i)
+        {
+            const int t = op.tq[i];
+            if (!((pending >> t) & 1))
+                continue;
+            if (op.diag)
+            {
+                for (int a = 0; a < op.na; ++a)
+                    op.act[a] ^= static_cast<uint8_t>(1u << i);
+                // keep the active sub-indices ascending, entries alongside
+                for (int a = 1; a < op.na; ++a)
+                    for (int b = a; b > 0 && op.act[b - 1] > op.act[b]; --b)
+                    {
+                        std::swap(op.act[b - 1], op.act[b]);
+                        std::swap(op.mat[b - 1], op.mat[b]);
+                    }
+            }
+            else if (is_x(op))
+            {
+                // a controlled X on target t commutes with X on t
+            }
+            else if (op.nt == 1 && op.cmask == 0 && op.na == 2 && op.act[0] == 0 && op.act[1] == 1)
+            {
+                std::swap(op.mat[0], op.mat[1]);
+                std::swap(op.mat[2], op.mat[3]);
+                pending &= ~(1ull << t);
+            }
+            else
+            {
+                out.push_back(x_op(t));
+                pending &= ~(1ull << t);
+            }
+        }
+        out.push_back(op);
+    }
+    for (int t = 0; t < 64; ++t)
+        if ((pending >> t) & 1)
+            out.push_back(x_op(t));
+    return out;
+}
+
 int op_entry_count(const GateOp &op)
 {
     if (op.diag)
@@ -2329,7 +2406,7 @@ void FusedExecutor::settle_judge()
     pending_learned_ = -1;
 }
 
-int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<GateOp> &ops, int mode,
+int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<GateOp> &queued, int mode,
                        qcs_b200_stats &stats, KernelTimer &timer)
 {
     const bool c64 = amp_bytes == (int)sizeof(float2);
@@ -2347,10 +2424,11 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
     // Small registers: a pass would not fill a warp; run gate by gate.
     if (n < fused_min_qubits())
     {
-        for (const GateOp &op : ops)
+        for (const GateOp &op : queued)
             launches += plain(op);
         return launches;
     }
+    const std::vector<GateOp> ops = defer_x(queued);
     const int k = choose_local_bits(n, local_bits_);
     const int low = std::min(kLowBits, k);
     const int max_ops = (max_ops_ > 0 && max_ops_ < kFusedMaxOps) ? max_ops_ : kFusedMaxOps;

@@ -147,6 +147,9 @@ struct FOpSource
 };
 
 OpClass classify(const GateOp &op);
+// The queue with uncontrolled X gates moved later (exact rewrites of the ops
+// they pass; see fused_pass.cu).
+std::vector<GateOp> defer_x(const std::vector<GateOp> &q);
 std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int low, int max_ops);
 // Fill the kernel parameters of a pass (false when it does not fit the
 // parameter block); src, when given, receives one FOpSource per FOp.

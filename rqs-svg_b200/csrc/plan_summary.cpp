@@ -76,6 +76,7 @@ void plan_summary(int n, const qcs_b200_gate *gates, uint64_t count, qcs_b200_pl
         out.plain_gates = static_cast<uint32_t>(queue.size());
         return;
     }
+    queue = defer_x(queue);
     const int k = clamp_local_bits(kDefaultLocal, n);
     const std::vector<Segment> segs = plan_greedy(queue, n, k, std::min(kLowBits, k), kFusedMaxOps);
     std::vector<double2> tables;

@@ -120,6 +120,38 @@ def test_single_qubit_layers_merge_across_blockers(gpu_lib, oracle_lib, n):
     assert np.max(np.abs(got_b - ref0)) <= 1e-12
 
 
+@pytest.mark.parametrize("n", [9, 12, 15])
+def test_deferred_x_gates_match_oracle(gpu_lib, oracle_lib, n):
+    """Uncontrolled X gates move later in the fused queue: past diagonal gates
+    and controls (their pattern bits flipped), past controlled X on their
+    target, into the next uncontrolled one-qubit gate on their qubit (a column
+    swap), or up to a gate they cannot pass; measurements in between."""
+    rng = np.random.default_rng(77 + n)
+    circ = []
+    kinds = [["p", "rz", "rzz", "z", "t", "s", "global_phase"], ["x", "y"], ["h", "u3", "ry", "sx"],
+             ["rxx", "iswap", "swap", "ecr", "u3", "x"]]
+    for blk in range(16):
+        for q in rng.choice(n, size=int(rng.integers(1, n)), replace=False):
+            circ.append(("x", (), (int(q),), (), ()))
+        gates = kinds[blk % len(kinds)]
+        circ += C.random_circuit(n, int(rng.integers(1, 14)), seed=3000 + 17 * n + blk, max_controls=3, gates=gates)
+        if blk % 5 == 4:
+            circ.append(("measure", (blk % n,), (int(rng.integers(0, n)),), (), ()))
+    start = _random_state(n, 11)
+    # complex64 without the measurements (an outcome may differ at a near tie)
+    for precision, tol, gates in ((128, TOL, circ), (64, 2e-5, [g for g in circ if g[0] != "measure"])):
+        with qcs_b200.Simulator(gpu_lib, n, n, seed=5, fusion=FUSION_GREEDY, precision=precision) as sim:
+            sim.set_statevector(start)
+            sim.run(gates)
+            got, bits = sim.statevector(), sim.clbits_string()
+        with qcs_b200.Simulator(oracle_lib, n, n, seed=5) as sim:
+            sim.set_statevector(start)
+            sim.run(gates)
+            ref, ref_bits = sim.statevector(), sim.clbits_string()
+        assert bits == ref_bits, precision
+        assert np.max(np.abs(got - ref)) <= tol, precision
+
+
 @pytest.mark.parametrize("precision", [128, 64])
 def test_repeated_and_interleaved_runs_on_one_simulator(gpu_lib, oracle_lib, precision):
     """One simulator runs the same circuit again, another circuit in between,

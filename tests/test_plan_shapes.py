@@ -34,6 +34,26 @@ def test_qft_runs_are_table_fed_inside_two_stages_per_pass(gpu_lib):
     assert s["ops"] <= 20 * s["passes"]
 
 
+def test_basis_input_x_gates_move_into_the_qft(gpu_lib):
+    # the QFT of a basis state: the input's X gates pass the controlled phases
+    # (pattern bits flipped) and end in each qubit's H (a column swap), so the
+    # plan is the one of the QFT alone: no X op, no pass for the input
+    n = 33
+    circ, x = C.qft(n, seed=1)
+    assert bin(x).count("1") > 8
+    s = _summary(gpu_lib, n, circ)
+    bare = _summary(gpu_lib, n, [g for g in circ if g[0] != "x"])
+    assert s["kinds"]["x"] == 0
+    assert s["passes"] == bare["passes"] <= 4
+    assert s["stages"] == bare["stages"]
+    # an X that meets a gate it cannot pass (a controlled U3 on its qubit)
+    # is placed right before it; one with nothing after it ends the queue
+    circ = [("x", (), (3,), (), ()), ("p", (0.3,), (3,), (), (5,)), ("u3", (0.1, 0.2, 0.3), (3,), (), (7,)),
+            ("x", (), (9,), (), ()), ("x", (), (4,), (), ()), ("x", (), (4,), (), ())]
+    s = _summary(gpu_lib, 12, circ)
+    assert s["kinds"]["x"] == 2
+
+
 def test_layered_circuit_groups_one_qubit_gates_and_runs_signs(gpu_lib):
     n = 20
     s = _summary(gpu_lib, n, C.layered_u3_cz_cx_toffoli(n, 8, seed=2))
