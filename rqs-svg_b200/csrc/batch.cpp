@@ -102,9 +102,9 @@ Batch::~Batch()
 
 void Batch::release_device()
 {
-    if (exec_)
-        cudaGraphExecDestroy(exec_);
-    exec_ = nullptr;
+    for (cudaGraphExec_t e : execs_)
+        cudaGraphExecDestroy(e);
+    execs_.clear();
     cudaFree(arena_);
     cudaFree(mats_dev_);
     cudaFree(zitems_dev_);
@@ -202,12 +202,9 @@ void Batch::set_parameters(const double *params, uint64_t count)
         for (Gate &g : c.gates)
             for (int j = 0; j < g.np; ++j)
                 g.params[j] = params[i++];
-    if (built_)
-    {
-        // the previous run's graph may still be copying the entries
-        QCSB_CUDA(cudaStreamSynchronize(stream_));
-        fill_entries();
-    }
+    // the entries are filled by the next run, group by group, while the GPU
+    // runs the groups before
+    dirty_ = built_;
 }
 
 void Batch::plan_group(Group &g, int k)
@@ -376,11 +373,18 @@ void Batch::enqueue_passes(const Group &g, cudaStream_t s, int *launches)
     }
 }
 
-void Batch::enqueue_run(cudaStream_t s, int *launches)
+void Batch::enqueue_group(int gi, cudaStream_t s, int *launches)
 {
-    QCSB_CUDA(cudaMemcpyAsync(mats_dev_, mats_host_, sizeof(double2) * mats_count_, cudaMemcpyHostToDevice, s));
-    for (const Group &g : groups_)
-        enqueue_passes(g, s, launches);
+    const Group &g = groups_[gi];
+    const size_t count = (size_t)g.stride * g.members.size();
+    if (count > 0)
+        QCSB_CUDA(cudaMemcpyAsync(mats_dev_ + g.mats_off, mats_host_ + g.mats_off, sizeof(double2) * count,
+                                  cudaMemcpyHostToDevice, s));
+    enqueue_passes(g, s, launches);
+}
+
+void Batch::enqueue_results(cudaStream_t s, int *launches)
+{
     *launches += amp_bytes_ == 8
                      ? launch_batch_zsums<float>(arena_, zitems_dev_, num_zitems_, zregs_dev_,
                                                  (uint32_t)circuits_.size(), zpartials_dev_, zout_dev_, s)
@@ -531,13 +535,26 @@ void Batch::build()
     layout_entries();
     fill_entries();
 
-    // capture the run
+    // capture the run: a graph per group, then the results
     int launches = 0;
+    for (int gi = 0; gi <= (int)groups_.size(); ++gi)
+        execs_.push_back(capture(gi, &launches));
+    launches_per_run_ = (uint32_t)launches;
+    built_ = true;
+    dirty_ = false;
+}
+
+// Graph of group gi (gi == number of groups: the results).
+cudaGraphExec_t Batch::capture(int gi, int *launches)
+{
     cudaGraph_t graph = nullptr;
     QCSB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
     try
     {
-        enqueue_run(stream_, &launches);
+        if (gi < (int)groups_.size())
+            enqueue_group(gi, stream_, launches);
+        else
+            enqueue_results(stream_, launches);
     }
     catch (...)
     {
@@ -547,19 +564,33 @@ void Batch::build()
         throw;
     }
     QCSB_CUDA(cudaStreamEndCapture(stream_, &graph));
-    const cudaError_t err = cudaGraphInstantiate(&exec_, graph, 0);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     QCSB_CUDA(err);
-    launches_per_run_ = (uint32_t)launches;
-    built_ = true;
+    return exec;
 }
 
 void Batch::run()
 {
     if (!built_)
         build();
-    QCSB_CUDA(cudaEventRecord(ev0_, stream_));
-    QCSB_CUDA(cudaGraphLaunch(exec_, stream_));
+    // new parameters: each group's entries are filled on the host while the
+    // GPU runs the groups launched before it (the copies of a group read only
+    // its own part of the pinned entry buffer)
+    const bool fill = dirty_;
+    for (size_t gi = 0; gi < groups_.size(); ++gi)
+    {
+        if (fill)
+            fill_entries((int)gi);
+        if (gi == 0)
+            QCSB_CUDA(cudaEventRecord(ev0_, stream_));
+        QCSB_CUDA(cudaGraphLaunch(execs_[gi], stream_));
+    }
+    if (groups_.empty())
+        QCSB_CUDA(cudaEventRecord(ev0_, stream_));
+    QCSB_CUDA(cudaGraphLaunch(execs_.back(), stream_));
+    dirty_ = false;
     QCSB_CUDA(cudaEventRecord(ev1_, stream_));
     QCSB_CUDA(cudaStreamSynchronize(stream_));
     float ms = 0.0f;

@@ -93,7 +93,9 @@ class Batch
     void fill_entries(int only_group = -1);
     void fill_group_range(const Group &g, size_t first, size_t last);
     void enqueue_passes(const Group &g, cudaStream_t s, int *launches);
-    void enqueue_run(cudaStream_t s, int *launches);
+    void enqueue_group(int gi, cudaStream_t s, int *launches);
+    void enqueue_results(cudaStream_t s, int *launches);
+    cudaGraphExec_t capture(int gi, int *launches);
     void tune();
     void release_device();
 
@@ -103,6 +105,7 @@ class Batch
     uint64_t num_params_ = 0;
     bool built_ = false;
     bool ran_ = false;
+    bool dirty_ = false;   // parameters set since the entries were last filled
 
     cudaStream_t stream_ = nullptr;
     void *arena_ = nullptr;
@@ -114,7 +117,9 @@ class Batch
     uint32_t num_zitems_ = 0;
     double *zpartials_dev_ = nullptr, *zout_dev_ = nullptr, *zout_host_ = nullptr;
     uint64_t zout_count_ = 0;
-    cudaGraphExec_t exec_ = nullptr;
+    // one graph per group (its entries in, its passes) and one for the
+    // results (<Z> of every register, out to the host)
+    std::vector<cudaGraphExec_t> execs_;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     uint32_t launches_per_run_ = 0;
     double last_ms_ = 0.0;
