@@ -535,7 +535,11 @@ void Batch::build()
     layout_entries();
     fill_entries();
 
-    // capture the run: a graph per group, then the results
+    // capture the run: a graph per group, then the results (after dropping
+    // those of a build that stopped part way)
+    for (cudaGraphExec_t e : execs_)
+        cudaGraphExecDestroy(e);
+    execs_.clear();
     int launches = 0;
     for (int gi = 0; gi <= (int)groups_.size(); ++gi)
         execs_.push_back(capture(gi, &launches));
