@@ -101,3 +101,14 @@ def test_bad_gates_are_rejected(gpu_lib):
         _summary(gpu_lib, 4, [("h", (), (7,), (), ())])
     with pytest.raises(qcs_b200.QCSError):
         _summary(gpu_lib, 4, [("nosuchgate", (), (0,), (), ())])
+
+
+def test_measured_workloads_keep_their_pass_counts(gpu_lib):
+    # the pass counts behind the measured numbers (one read and write of the
+    # register per pass): a planner change that adds passes shows here first
+    s = _summary(gpu_lib, 30, C.layered_u3_cz_cx_toffoli(30, 40, seed=1))
+    assert s["plain_gates"] == 0 and s["passes"] <= 65
+    s = _summary(gpu_lib, 30, C.u3_random_matching(30, 60, seed=1))
+    assert s["plain_gates"] == 0 and s["passes"] <= 110
+    s = _summary(gpu_lib, 33, C.qft(33, seed=1)[0])
+    assert s["plain_gates"] == 0 and s["passes"] <= 4
