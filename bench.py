@@ -23,8 +23,9 @@ replica ("replicas only": the path has no exchange step) and value is the
 slowest rank's time divided by N (seconds per circuit for the whole job).
 
 Arms:
-  default             this library (fused greedy passes; --fusion plain for the
-                      one-kernel-per-gate path)
+  default             this library (fused passes under the learned planner and
+                      its judge; --fusion greedy for the greedy planner alone,
+                      --fusion plain for the one-kernel-per-gate path)
   --impl reference    the reference library built from its sources for
                       sm_100a (oracle/_ref/libqcs_ref.so) on the same GPU, same
                       circuit, through its C API; it has no <Z> or sampler, so
@@ -109,7 +110,10 @@ def parse_args():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="layered",
                     help="layered: U3 + CZ/CX + Toffoli layers with <Z> and shots (default); "
                          "matching: U3 + CX on random matchings; qft: QFT of a random basis state")
-    ap.add_argument("--fusion", choices=["plain", "greedy", "learned"], default="greedy")
+    ap.add_argument("--fusion", choices=["plain", "greedy", "learned"], default="learned",
+                    help="learned (default): the cost model is trained on pass timings recorded on smaller "
+                         "registers, its plan and the greedy plan are both timed during warm-up and the faster "
+                         "one runs; greedy: fused passes cut greedily; plain: one kernel per gate")
     ap.add_argument("--precision", type=int, choices=[128, 64], default=None,
                     help="amplitude bits (default 128; 64 for hea_batch)")
     ap.add_argument("--qubits", type=int, default=30)
@@ -509,7 +513,12 @@ def main():
                    "parallelism": f"replicas x{WORLD}",
                    "l2": f"state ({bpa << n >> 20} MiB) larger than L2; no flush" if (bpa << n) > (126 << 20)
                    else "state fits L2; no flush"},
-        "hbm_gbs_algorithmic": alg_bytes / sec_per_step / 1e9,
+        # bytes the step's kernels read and write (each fused pass the whole
+        # register once, each plain gate its changed amplitudes) per second
+        "hbm_gbs": (ktimes["fused_bytes"] + ktimes["plain_bytes"]) / args.steps / sec_per_step / 1e9,
+        # not an HBM rate: the bytes the one-kernel-per-gate path would move
+        # for this circuit, divided by the fused step time
+        "effective_gbs_plain_bytes": alg_bytes / sec_per_step / 1e9,
         "e2e": {"value": e2e_total / args.steps / WORLD, "unit": "s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(stats["kernel_launches"] / args.steps),
@@ -577,6 +586,13 @@ def main_batch(args, dist):
     barrier(dist)
     clk = clocks.stop(0)
     info = b.info()
+    # accuracy: one more run with the circuits' own parameters, <Z_q> of
+    # every 64th circuit against the CPU oracle (which also times them for
+    # the CPU baseline)
+    b.set_parameters(np.concatenate([np.asarray([v for _, p, *_ in c for v in p], dtype=np.float64)
+                                     for c in circs]))
+    b.run()
+    z_batch = b.expectation_z()
     b.close()
     agg = aggregate_replica_times(dist, dev, WORLD)
     sec = agg["sec_per_step"]
@@ -585,9 +601,13 @@ def main_batch(args, dist):
     achieved = info["pass_bytes"] / sec / 1e9
     nparams = info["parameters"]
     alg = sum(C.algorithmic_bytes(c, w, precision // 8) for w, c in zip(widths, circs))
-    cpu = None
+    cpu, accuracy = None, None
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_batch(widths, circs)
+        cpu, z_oracle = cpu_baseline_batch(widths, circs, with_z=True)
+        errs = [float(np.max(np.abs(z_batch[i] - z))) for i, z in z_oracle.items()]
+        accuracy = {"check": f"<Z_q> of every 64th circuit ({len(errs)} circuits, all qubits) vs the CPU "
+                             f"oracle (complex128), the circuits' own parameters",
+                    "max_abs_err": max(errs), "tolerance": 1e-5 if precision == 64 else 1e-12}
     line = {
         "metric": f"batch wall s ({len(circs)} HEA circuits)",
         "value": agg["value"], "unit": "s", "n_gpus": WORLD, "steps": args.steps, "warmup": args.warmup,
@@ -598,7 +618,9 @@ def main_batch(args, dist):
                    "amplitudes": info["amplitudes"], "parallelism": f"replicas x{WORLD}",
                    "l2": f"registers ({info['amplitudes'] * precision // 8 >> 20} MiB) larger than L2; no flush"},
         "circuits_per_s": len(circs) / sec,
-        "hbm_gbs_algorithmic": alg / sec / 1e9,
+        "hbm_gbs": achieved,
+        # not an HBM rate: the per-gate path's bytes over the batch step time
+        "effective_gbs_plain_bytes": alg / sec / 1e9,
         "e2e": {"value": e2e_total / args.steps / WORLD, "unit": "s", "h2d_bytes_per_step": nparams * 8,
                 "d2h_bytes_per_step": sum(widths) * 8},
         "gpu_launches": info["launches_per_run"],
@@ -610,6 +632,7 @@ def main_batch(args, dist):
         "batch": {"groups": info["groups"], "passes": info["passes"], "pass_bytes": info["pass_bytes"],
                   "setup_s": setup_s, "step_s": dev},
         "cpu_baseline": cpu,
+        "accuracy": accuracy,
         "clocks": clk,
     }
     if RANK == 0:
@@ -618,24 +641,28 @@ def main_batch(args, dist):
         dist.destroy_process_group()
 
 
-def cpu_baseline_batch(widths, circs, stride=64):
+def cpu_baseline_batch(widths, circs, stride=64, with_z=False):
     """The CPU oracle on every 64th circuit of the batch (complex128),
-    scaled by 64."""
+    scaled by 64; with_z also returns each sampled circuit's <Z_q>."""
     oracle_so = REPO / "oracle" / "liboracle_qcs.so"
     if not oracle_so.exists():
-        return None
+        return (None, {}) if with_z else None
     lib = qcs_b200.Library(oracle_so)
     t0 = time.perf_counter()
     count = 0
+    zs = {}
     for i in range(0, len(circs), stride):
         with qcs_b200.Simulator(lib, widths[i]) as sim:
             sim.run(circs[i])
             sim.statevector()
+            if with_z:
+                zs[i] = sim.expectation_z()[0]
         count += 1
     dt = time.perf_counter() - t0
-    return {"value": dt * len(circs) / count, "unit": "s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"every {stride}th circuit ({count} circuits) on the CPU oracle (complex128), {dt:.1f} s, "
-                      f"scaled by {stride}"}
+    cpu = {"value": dt * len(circs) / count, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+           "sample": f"every {stride}th circuit ({count} circuits) on the CPU oracle (complex128), {dt:.1f} s, "
+                     f"scaled by {stride}"}
+    return (cpu, zs) if with_z else cpu
 
 
 def run_reference_batch(args, dist, widths, circs, depth, workload, stride=16):

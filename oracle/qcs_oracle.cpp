@@ -33,7 +33,7 @@
 //
 // Parity pinning: the reference ships no tests or golden vectors. This oracle
 // is pinned against outputs of the reference library itself, built from its
-// own sources for sm_100a (oracle/ref/Makefile) and run on a B200; the
+// own sources for sm_100a (the `ref` target of oracle/Makefile) and run on a B200; the
 // fixtures and the script that generated them are in tests/golden/.
 
 #include "qcs.h"

@@ -442,6 +442,13 @@ void Batch::build()
 {
     if (circuits_.empty())
         throw std::runtime_error("run: the batch has no circuits");
+    // A build that threw part way (a gate that fits no pass, too little
+    // memory) leaves its buffers and graphs behind; a rebuild starts from
+    // nothing so that retries do not leak device or pinned memory.
+    if (stream_)
+        QCSB_CUDA(cudaStreamSynchronize(stream_));
+    release_device();
+    mats_count_ = 0;
     groups_.clear();
     // group by structure
     for (uint32_t ci = 0; ci < circuits_.size(); ++ci)

@@ -157,3 +157,52 @@ def test_batch_of_identity_circuits(gpu_lib):
         z = b.expectation_z()
         assert np.all(z[0] == 1.0)
         assert z[1][3] == -1.0 and np.all(np.delete(z[1], 3) == 1.0)
+
+
+def test_batch_failed_build_releases_memory(gpu_lib):
+    """A build that stops part way (here: a circuit whose gate entries exceed
+    one register's entry block, found after the register arena is allocated)
+    must not leak that arena when run() is retried."""
+    import torch
+
+    big = 24   # a 256 MiB complex128 register makes a leaked arena visible
+    too_many = [("u3", (0.1 * i, 0.2, 0.3), (i % 9,), (), ()) for i in range(17000)]
+    with qcs_b200.Batch(gpu_lib, 128) as b:
+        b.add_circuit(big, [("h", (), (0,), (), ())])
+        b.add_circuit(9, too_many)
+        with pytest.raises(qcs_b200.QCSError, match="too many gate entries"):
+            b.run()
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        for _ in range(3):
+            with pytest.raises(qcs_b200.QCSError, match="too many gate entries"):
+                b.run()
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+    assert free_before - free_after < (64 << 20), (free_before, free_after)
+
+
+@pytest.mark.parametrize("precision", [128, 64])
+def test_batch_multi_chunk_registers(gpu_lib, oracle_lib, precision):
+    """The batch workload's widest registers (15-20 qubits, depth 8: 16 to
+    512 chunks per register in the batched pass), including two circuits of
+    one structure, against the oracle: states, and <Z_q> of every qubit."""
+    widths = [15, 16, 17, 18, 19, 20, 17]
+    circs = [(w, C.hea_circuit(w, 8, seed=500 + i)) for i, w in enumerate(widths)]
+    with qcs_b200.Batch(gpu_lib, precision) as b:
+        for n, circ in circs:
+            b.add_circuit(n, circ)
+        b.run()
+        zs = b.expectation_z()
+        assert b.info()["groups"] == len(circs) - 1
+        for i, (n, circ) in enumerate(circs):
+            ref = _oracle_state(oracle_lib, n, circ)
+            got = b.statevector(i)
+            zref = _z_from_state(ref, n)
+            if precision == 128:
+                assert np.max(np.abs(got - ref)) <= 1e-12, i
+                assert np.max(np.abs(zs[i] - zref)) <= 1e-12, i
+            else:
+                fid = abs(np.vdot(got, ref)) ** 2 / (np.vdot(got, got).real * np.vdot(ref, ref).real)
+                assert fid >= 1 - 1e-6, (i, fid)
+                assert np.max(np.abs(zs[i] - zref)) <= 1e-5, i
