@@ -114,6 +114,9 @@ def parse_args():
                     help="learned (default): the cost model is trained on pass timings recorded on smaller "
                          "registers, its plan and the greedy plan are both timed during warm-up and the faster "
                          "one runs; greedy: fused passes cut greedily; plain: one kernel per gate")
+    ap.add_argument("--tensor", choices=["never", "auto", "always"], default="auto",
+                    help="tensor passes (complex128 stages as 16x16 matrices on the FP64 tensor cores): "
+                         "auto (default) where the estimated FP64 work is lower")
     ap.add_argument("--precision", type=int, choices=[128, 64], default=None,
                     help="amplitude bits (default 128; 64 for hea_batch)")
     ap.add_argument("--qubits", type=int, default=30)
@@ -374,6 +377,8 @@ def main():
     fusion = {"plain": qcs_b200.FUSION_PLAIN, "greedy": qcs_b200.FUSION_GREEDY,
               "learned": qcs_b200.FUSION_LEARNED}[args.fusion]
     sim = qcs_b200.Simulator(lib, n, seed=1234 + RANK, fusion=fusion, precision=args.precision)
+    sim.set_tensor_passes({"never": qcs_b200.TENSOR_NEVER, "auto": qcs_b200.TENSOR_AUTO,
+                           "always": qcs_b200.TENSOR_ALWAYS}[args.tensor])
     model, training, judge = None, None, None
     if fusion == qcs_b200.FUSION_LEARNED:
         model, training = train_planner(lib, args)
@@ -409,7 +414,8 @@ def main():
     sec_per_step = agg["sec_per_step"]
     passes = None
     if len(pass_ms):
-        passes = {"per_step": len(pass_ms) / args.steps, "median_ms": float(np.median(pass_ms)),
+        passes = {"per_step": len(pass_ms) / args.steps, "tensor_per_step": stats["tensor_passes"] / args.steps,
+                  "median_ms": float(np.median(pass_ms)),
                   "max_ms": float(np.max(pass_ms)), "arith_ops_per_pass": float(np.mean(pass_feats[:, 1])),
                   "light_ops_per_pass": float(np.mean(pass_feats[:, 2])),
                   "hbm_floor_ms": 2 * bpa * (1 << n) / (hbm_peak()[0] * 1e9) * 1e3}
@@ -509,7 +515,8 @@ def main():
         "dtype": "c128 (f64)" if args.precision == 128 else "c64 (f32 gates, f64 reductions)",
         "data": "synthetic (seeded circuit)",
         "config": {"workload": workload, "qubits": n, "depth": depth, "gates": len(circuit),
-                   "shots": SHOTS if draws_shots else 0, "fusion": args.fusion, "precision": args.precision,
+                   "shots": SHOTS if draws_shots else 0, "fusion": args.fusion, "tensor_passes": args.tensor,
+                   "precision": args.precision,
                    "parallelism": f"replicas x{WORLD}",
                    "l2": f"state ({bpa << n >> 20} MiB) larger than L2; no flush" if (bpa << n) > (126 << 20)
                    else "state fits L2; no flush"},

@@ -129,6 +129,7 @@ typedef struct qcs_b200_stats
     uint64_t fused_passes;
     uint64_t plain_gate_kernels;
     double algorithmic_bytes;
+    uint64_t tensor_passes;       /* fused passes run as tensor passes (a subset of fused_passes) */
 } qcs_b200_stats;
 
 int qcs_simulator_get_stats(const qcs_simulator *sim, qcs_b200_stats *stats);
@@ -161,6 +162,21 @@ int qcs_simulator_get_kernel_times(qcs_simulator *sim, qcs_b200_kernel_times *ti
  * timings for the cost model.
  */
 int qcs_simulator_set_planner_options(qcs_simulator *sim, int max_gates_per_pass, int local_qubits);
+
+/*
+ * Tensor passes (complex128 registers): a fused pass whose stages depend on
+ * few bits outside themselves can run every stage as dense 16 x 16 matrices
+ * on the FP64 tensor cores instead of gate by gate. mode 0: never; 1 (the
+ * default): when the estimated FP64 work is lower; 2: whenever the pass
+ * allows it. Results agree with the other paths to the rounding of the
+ * matrix products (they replace the reference's per-pair 2x2 products,
+ * src/qcs.cu:1139-1174, by products of whole stages).
+ */
+#define QCS_TENSOR_NEVER 0
+#define QCS_TENSOR_AUTO 1
+#define QCS_TENSOR_ALWAYS 2
+int qcs_simulator_set_tensor_passes(qcs_simulator *sim, int mode);
+int qcs_simulator_get_tensor_passes(const qcs_simulator *sim, int *mode);
 
 /*
  * Pass timings recorded while kernel timing is enabled: for each fused pass
@@ -294,6 +310,10 @@ typedef struct qcs_b200_plan_summary
     uint32_t ops;               /* pass ops over all passes (terms included) */
     uint32_t kinds[QCS_B200_PLAN_KINDS];
     uint64_t table_entries;     /* complex entries of the phase-run factor tables */
+    uint32_t tensor_passes;     /* passes a complex128 register runs as tensor passes (automatic choice) */
+    uint32_t tensor_eligible;   /* passes whose stages allow a tensor pass */
+    uint32_t tensor_matrices;   /* stage matrices over the tensor passes */
+    uint32_t reserved;
 } qcs_b200_plan_summary;
 int qcs_b200_plan_summary_get(int num_qubits, const qcs_b200_gate *gates, uint64_t num_gates,
                               qcs_b200_plan_summary *summary);

@@ -590,6 +590,15 @@ extern "C" int qcs_simulator_set_planner_options(qcs_simulator *sim, int max_gat
     return guarded([&] { core(sim).set_planner_options(max_gates_per_pass, local_qubits); });
 }
 
+extern "C" int qcs_simulator_set_tensor_passes(qcs_simulator *sim, int mode)
+{
+    return guarded([&] { core(sim).set_tensor_mode(mode); });
+}
+extern "C" int qcs_simulator_get_tensor_passes(const qcs_simulator *sim, int *mode)
+{
+    return guarded([&] { write_result(mode, core(sim).tensor_mode()); });
+}
+
 extern "C" int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *milliseconds,
                                               uint32_t capacity, uint32_t *count)
 {

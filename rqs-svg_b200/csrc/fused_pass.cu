@@ -92,6 +92,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 constexpr int R = 1 << kStageBits;
 
+
 // Gate application on a thread's 2^kStageBits amplitudes a[r] (r = the values
 // of the stage's local bits; j0 = the thread's local index with the stage
 // bits zero). A condition splits into the other local bits (checked once
@@ -906,7 +907,132 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4)
     }
 }
 
+// The matrices of a tensor pass: thread (matrix, col) applies the ops of the
+// matrix's stage, exactly as the register stage above applies them, to the
+// unit vector of input slot col, with the stage's condition bits set as the
+// matrix index says and every other bit outside the stage zero (no op of the
+// stage depends on those). The resulting column is written as the B
+// fragments of the tensor pass's m16n8k8 products: B[u][nu] for input slot
+// u (tensor layout) and output column nu = 8i + g, i.e. output slot
+// 4i + (g >> 1), real part for even g and imaginary part for odd g; lane
+// 4g + t of fragment 4j + i holds (B[8j + t][8i + g], B[8j + t + 4][8i + g]).
+template <typename Real>
+__global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant__ FPassParams p,
+                                                          const __grid_constant__ TBuildParams tb)
+{
+    typedef typename Cx<Real>::T V;
+    __shared__ V scratch[64][R];
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t mat = gid >> kStageBits;
+    const int col = static_cast<int>(gid & (R - 1));
+    if (mat >= tb.nmats)
+        return;
+    int st = 0;
+    while (st + 1 < tb.nstages && tb.stages[st + 1].woff <= mat)
+        ++st;
+    const TStage &S = tb.stages[st];
+    const FStage &FS = p.stages[st];
+    const uint32_t v = mat - S.woff;
+    const int k = p.k;
+    uint32_t j0 = 0;
+    for (int i = 0; i < S.nlc; ++i)
+        if ((v >> i) & 1)
+            j0 |= 1u << S.gpos[kStageBits + i];
+    uint64_t local = 0;
+    for (int i = 0; i < k; ++i)
+        local |= p.qbit[i];
+    uint64_t cbase = 0, chunk = 0;
+    for (int i = 0; i < S.ngc; ++i)
+        if ((v >> (S.nlc + i)) & 1)
+        {
+            const int q = S.gq[i];
+            cbase |= 1ull << q;
+            chunk |= 1ull << (q - __popcll(local & ((1ull << q) - 1)));
+        }
+    // the register pass's thread index of this group: j0 without the stage bits
+    uint32_t tidx = 0;
+    for (int l = 0, pos = 0; l < k; ++l)
+    {
+        if (l == FS.sbits[0] || l == FS.sbits[1] || l == FS.sbits[2] || l == FS.sbits[3])
+            continue;
+        if ((j0 >> l) & 1)
+            tidx |= 1u << pos;
+        ++pos;
+    }
+    // slot u of the tensor layout is slot reg(u) of the register layout
+    auto reg = [&](int u) {
+        int r = 0;
+#pragma unroll
+        for (int b = 0; b < kStageBits; ++b)
+            if ((u >> b) & 1)
+                r |= 1 << ((S.perm >> (2 * b)) & 3);
+        return r;
+    };
+    const int r0 = reg(col);
+    V a[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        a[r] = r == r0 ? V{1, 0} : V{0, 0};
+    const StageSlots<V> ss{scratch[threadIdx.x], 0u, {1u, 2u, 4u, 8u}};
+    const int T = 1 << (k - kStageBits);
+    for (int oi = FS.op_begin; oi < FS.op_end; ++oi)
+    {
+        const FOp &op = p.ops[oi];
+        if (op.kind == F_SIGNS)
+        {
+            uint32_t neg = 0;
+            const int nt = static_cast<int>(op.lcmask);
+            for (int i = 1; i <= nt; ++i)
+            {
+                const FOp &t = p.ops[oi + i];
+                if ((j0 & t.lcmask) == t.lcval && (cbase & t.gcmask) == t.gcval)
+                    neg ^= t.moff;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+            {
+                const uint32_t sgn = ((neg >> r) & 1u) << 31;
+                a[r].x = flip_by(a[r].x, sgn);
+                a[r].y = flip_by(a[r].y, sgn);
+            }
+            oi += nt;
+            continue;
+        }
+        if (op.kind == F_PRUN)
+        {
+            phase_inline<V>(a, op, p.ops + oi + 1, j0, cbase, chunk, static_cast<int>(tidx), T, p.tables,
+                            [&](int off) { return pool_entry<V>(p, off); });
+            oi += op.lcmask;
+            continue;
+        }
+        if ((cbase & op.gcmask) != op.gcval)
+            continue;
+        apply_op<V>(a, op, PoolEntries<V>{p, op.moff}, j0, cbase, ss);
+    }
+    const int j = col >> 3, b = (col >> 2) & 1, t = col & 3;
+    Real *out = reinterpret_cast<Real *>(tb.out) + static_cast<size_t>(mat) * kTensorFragments * 64;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int g = 0; g < 8; ++g)
+        {
+            const V y = a[reg(4 * i + (g >> 1))];
+            out[((j * 4 + i) * 32 + g * 4 + t) * 2 + b] = (g & 1) ? y.y : y.x;
+        }
+}
+
 } // namespace
+
+template <typename R>
+int launch_stage_matrices(const FPassParams &prm, const TBuildParams &tb, cudaStream_t stream)
+{
+    const unsigned threads = 64;
+    const unsigned blocks = static_cast<unsigned>((static_cast<uint64_t>(tb.nmats) * (1u << kStageBits) + threads - 1) / threads);
+    stage_matrix_kernel<R><<<blocks, threads, 0, stream>>>(prm, tb);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+template int launch_stage_matrices<double>(const FPassParams &, const TBuildParams &, cudaStream_t);
 
 // ------------------------------------------------------------ planning
 
@@ -1400,7 +1526,7 @@ constexpr size_t kPassTableBudget = size_t(1) << 16;   // table entries of one p
 // Fill the kernel parameters of a pass. Returns false when the pass does not
 // fit the parameter block limits.
 bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
-                       std::vector<FOpSource> *src, std::vector<double2> *tables)
+                       std::vector<FOpSource> *src, std::vector<double2> *tables, std::vector<StageCond> *conds)
 {
     std::memset(&prm, 0, sizeof(prm));
     prm.n = n;
@@ -1449,6 +1575,25 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                 pos_in_stage[l] = nb;
                 sbits[nb++] = static_cast<uint8_t>(l);
             }
+        // the bits outside the stage that its ops depend on
+        StageCond cond;
+        for (int oi : stage_ops[si])
+        {
+            const GateOp &op = q[pp.ops[oi]];
+            uint64_t pattern = op.cmask;
+            for (int i = 0; i < op.nt; ++i)
+                pattern |= 1ull << op.tq[i];
+            for (int b = 0; b < n; ++b)
+            {
+                if (!((pattern >> b) & 1))
+                    continue;
+                const int l = loc_of[b];
+                if (l < 0)
+                    cond.gmask |= 1ull << b;
+                else if (!((bits >> l) & 1))
+                    cond.lmask |= 1u << l;
+            }
+        }
         // the scheduled stage becomes one register stage, opened at its first op
         auto open_stage = [&]() -> FStage * {
             if (ns >= kFusedMaxStages)
@@ -1457,6 +1602,8 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
             std::memset(&S, 0, sizeof(S));
             std::memcpy(S.sbits, sbits, sizeof(sbits));
             S.op_begin = static_cast<uint16_t>(nops);
+            if (conds)
+                conds->push_back(cond);
             return &S;
         };
         // the stage bits a diagonal op's pattern (controls and targets) involves
@@ -2045,10 +2192,12 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
 } // namespace
 
 bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
-                  std::vector<FOpSource> *src, std::vector<double2> *tables)
+                  std::vector<FOpSource> *src, std::vector<double2> *tables, std::vector<StageCond> *conds)
 {
     const size_t start = tables ? tables->size() : 0;
-    const bool ok = build_params_body(q, pp, n, k, prm, src, tables);
+    if (conds)
+        conds->clear();
+    const bool ok = build_params_body(q, pp, n, k, prm, src, tables, conds);
     if (!ok && tables)
         tables->resize(start);
     return ok;
@@ -2056,16 +2205,19 @@ bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, in
 
 bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, std::vector<FPassParams> &params,
                   std::vector<std::vector<FOpSource>> *srcs, std::vector<PlannedPass> *pieces,
-                  std::vector<double2> *tables)
+                  std::vector<double2> *tables, std::vector<std::vector<StageCond>> *conds)
 {
     params.emplace_back();
     std::vector<FOpSource> src;
-    if (build_params(q, pp, n, pp.k, params.back(), srcs ? &src : nullptr, tables))
+    std::vector<StageCond> cond;
+    if (build_params(q, pp, n, pp.k, params.back(), srcs ? &src : nullptr, tables, conds ? &cond : nullptr))
     {
         if (srcs)
             srcs->push_back(std::move(src));
         if (pieces)
             pieces->push_back(pp);
+        if (conds)
+            conds->push_back(std::move(cond));
         return true;
     }
     params.pop_back();
@@ -2075,7 +2227,8 @@ bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, st
     PlannedPass a = pp, b = pp;
     a.ops.assign(pp.ops.begin(), pp.ops.begin() + half);
     b.ops.assign(pp.ops.begin() + half, pp.ops.end());
-    return build_pieces(q, a, n, params, srcs, pieces, tables) && build_pieces(q, b, n, params, srcs, pieces, tables);
+    return build_pieces(q, a, n, params, srcs, pieces, tables, conds) &&
+           build_pieces(q, b, n, params, srcs, pieces, tables, conds);
 }
 
 namespace
@@ -2353,6 +2506,7 @@ FusedExecutor::~FusedExecutor()
     }
     cudaFree(tables_dev_);
     cudaFreeHost(tables_host_);
+    cudaFree(mats_dev_);
 }
 
 // Copy the flush's phase-run tables to the device, behind the previous
@@ -2490,6 +2644,11 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
     // step >= 0: a pass (index into params), step < 0: plain op -1 - step.
     std::vector<FPassParams> params;
     std::vector<PlannedPass> pieces;
+    std::vector<std::vector<StageCond>> conds;
+    // per pass: index into tparams/tbuild when it runs as a tensor pass, else -1
+    std::vector<int> tensor_of;
+    std::vector<TPassParams> tparams;
+    std::vector<TBuildParams> tbuild;
     std::vector<long> steps;
     tables_.clear();
     bool deferring = false;
@@ -2506,8 +2665,34 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
             const PassFeatures f = pass_features(ops, pieces[st], n);
             timer.begin(stream_, KernelTimer::kFused, 2.0 * amp_bytes * std::ldexp(1.0, n), &f);
         }
-        launches += c64 ? launch_fused_pass<float>(state, pieces[st].k, prm, stream_)
-                         : launch_fused_pass<double>(state, pieces[st].k, prm, stream_);
+        if (tensor_of[st] >= 0)
+        {
+            TPassParams &tp = tparams[tensor_of[st]];
+            TBuildParams &tb = tbuild[tensor_of[st]];
+            if (tb.nmats > mats_cap_)
+            {
+                // the old buffer may still be read by queued passes
+                QCSB_CUDA(cudaStreamSynchronize(stream_));
+                cudaFree(mats_dev_);
+                mats_dev_ = nullptr;
+                mats_cap_ = 0;
+                const size_t cap = std::max<size_t>(tb.nmats, 256);
+                QCSB_CUDA(cudaMalloc(&mats_dev_, cap * kTensorFragments * 32 * sizeof(double2)));
+                mats_cap_ = cap;
+            }
+            prm.state = state;
+            tb.out = mats_dev_;
+            tp.mats = mats_dev_;
+            tp.state = state;
+            launches += launch_stage_matrices<double>(prm, tb, stream_);
+            launches += launch_tensor_pass<double>(tp, stream_);
+            ++stats.tensor_passes;
+        }
+        else
+        {
+            launches += c64 ? launch_fused_pass<float>(state, pieces[st].k, prm, stream_)
+                             : launch_fused_pass<double>(state, pieces[st].k, prm, stream_);
+        }
         if (timer.enabled)
             timer.end(stream_);
         ++stats.fused_passes;
@@ -2526,15 +2711,34 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
             continue;
         }
         const size_t before = params.size();
-        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces, &tables_))
+        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces, &tables_, &conds))
         {
             params.resize(before);
             pieces.resize(before);
+            conds.resize(before);
             for (int oi : s.pass.ops)
                 add_step(-1 - (long)oi);
             continue;
         }
         deferring = deferring || !tables_.empty();
+        for (size_t i = before; i < params.size(); ++i)
+        {
+            tensor_of.push_back(-1);
+            if (c64 || tensor_mode_ == 0)
+                continue;
+            tparams.emplace_back();
+            tbuild.emplace_back();
+            if (make_tensor_params(params[i], conds[i], tparams.back(), tbuild.back()) &&
+                (tensor_mode_ == 2 || tensor_pass_cost(tparams.back()) < register_pass_cost(params[i])))
+            {
+                tensor_of.back() = static_cast<int>(tparams.size()) - 1;
+            }
+            else
+            {
+                tparams.pop_back();
+                tbuild.pop_back();
+            }
+        }
         if (c64)
             for (size_t i = before; i < params.size(); ++i)
                 entries_to_float(params[i].entries, params[i].nentries);

@@ -116,6 +116,83 @@ struct FPassParams
 };
 static_assert(sizeof(FPassParams) <= 32764, "kernel parameter limit");
 
+// The bits outside a stage that its ops depend on (controls, and the
+// targets of diagonal ops, that are not stage bits): local positions and
+// physical qubits of the chunk index. A tensor pass (tensor_pass.cu) applies
+// the stage as one matrix per assignment of these bits.
+struct StageCond
+{
+    uint32_t lmask = 0;   // local positions (bit l: local qubit l of the pass)
+    uint64_t gmask = 0;   // physical qubits that are not local
+};
+
+// ---------------------------------------------------------------- tensor passes
+// A tensor pass runs the stages of a planned pass as dense 16 x 16 complex
+// matrices on the tensor cores (tensor_pass.cu). Each stage's ops depend on
+// its 4 stage bits and on a few bits outside the stage (StageCond); the
+// stage becomes one matrix per assignment of those condition bits, built on
+// the GPU from the pass's ops (stage_matrix_kernel) and applied to every
+// 16-amplitude group of the stage by warp-level MMAs.
+constexpr int kTensorLocal = 11;       // local qubits of a tensor pass (2^11-amplitude chunks)
+constexpr int kTensorTileBits = 3;     // group bits that pick a warp's tiles: local condition bits go there
+constexpr int kTensorMaxCond = 8;      // condition bits of a stage: at most 2^8 matrices
+constexpr int kTensorMaxMats = 4096;   // matrices of one pass
+// Per matrix: the B fragments of the m16n8k8 products, 8 fragments x 32
+// lanes x (b0, b1), 4 KiB for complex128.
+constexpr int kTensorFragments = 8;
+
+struct TStage
+{
+    uint8_t sbits[kStageBits];   // local positions of slot bits 0..3
+    uint8_t gpos[7];             // local positions of group bits 0..6 (bits 4..6 pick the tile)
+    uint8_t nlc;                 // local condition bits: gpos[4 .. 4 + nlc)
+    uint8_t ngc;                 // chunk condition bits: physical qubits gq[0 .. ngc)
+    uint8_t gq[kTensorMaxCond];
+    uint8_t perm;                // slot bit b of the tensor layout is bit (perm >> 2b) & 3 of the register layout
+    uint8_t pad[2];
+    uint32_t woff;               // first matrix of the stage
+};
+static_assert(sizeof(TStage) == 28, "TStage layout");
+
+// The matrices of a pass: one per (stage, assignment of its condition bits);
+// matrix woff + v of a stage has local condition bit i equal to bit i of v
+// and chunk condition bit i equal to bit nlc + i of v.
+struct TBuildParams
+{
+    int nstages;
+    uint32_t nmats;
+    double2 *out;                // nmats x kTensorFragments x 32 lanes x double2
+    TStage stages[kFusedMaxStages];
+};
+
+struct TPassParams
+{
+    void *state;
+    const double2 *mats;
+    int n;
+    int from_zero;
+    uint64_t chunks;
+    uint64_t qmasks[kMaxLocal];
+    uint64_t qbit[kMaxLocal];
+    int nstages;
+    TStage stages[kFusedMaxStages];
+};
+
+// Tensor-pass layout of a built pass: false when a stage depends on more
+// condition bits than a tensor pass handles (or k is not kTensorLocal).
+bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, TPassParams &tp,
+                        TBuildParams &tb);
+// FP64 work per amplitude of a pass on the register path and on the tensor
+// path (both in multiply-adds, scaled by the measured efficiency of each).
+double register_pass_cost(const FPassParams &prm);
+double tensor_pass_cost(const TPassParams &tp);
+// Builds the pass's matrices (stage_matrix_kernel) and runs the pass;
+// returns the number of kernels launched.
+template <typename R>
+int launch_stage_matrices(const FPassParams &prm, const TBuildParams &tb, cudaStream_t stream);
+template <typename R>
+int launch_tensor_pass(const TPassParams &tp, cudaStream_t stream);
+
 struct OpClass
 {
     bool fusable;
@@ -156,8 +233,10 @@ std::vector<Segment> plan_greedy(const std::vector<GateOp> &q, int n, int k, int
 // tables: where F_PRUN factor tables are appended (offsets in the ops are
 // absolute indices into it; the caller uploads it and sets prm.tables); null
 // keeps every term explicit, as batched passes need.
+// conds, when given, receives one StageCond per stage of prm.
 bool build_params(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int k, FPassParams &prm,
-                  std::vector<FOpSource> *src = nullptr, std::vector<double2> *tables = nullptr);
+                  std::vector<FOpSource> *src = nullptr, std::vector<double2> *tables = nullptr,
+                  std::vector<StageCond> *conds = nullptr);
 // Entries an FOp of this kind reads (4 dense 1-target, 16 dense 2-target, 1
 // phase, 4 diagonal, 0 permutations), written to m from the GateOp. The x4
 // kinds take 4 entries from each of their ops: use layer_entries.
@@ -177,7 +256,7 @@ int op_entry_count(const GateOp &op);
 // build_params.
 bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, std::vector<FPassParams> &params,
                   std::vector<std::vector<FOpSource>> *srcs = nullptr, std::vector<PlannedPass> *pieces = nullptr,
-                  std::vector<double2> *tables = nullptr);
+                  std::vector<double2> *tables = nullptr, std::vector<std::vector<StageCond>> *conds = nullptr);
 int clamp_local_bits(int k, int n);
 // Complex64 passes read their entries as float2: round count double2 entries
 // in place into the first half of the same memory.

@@ -16,7 +16,8 @@ static_assert(F_DENSE1 == 0 && F_SWAP1 == 1 && F_DENSE2 == 2 && F_SWAP2 == 3 && 
                   F_TERM == 6 && F_DENSE1R == 7 && F_MULI == 9 && F_DENSE1X4 == 10 && F_DENSE1RX4 == 11 &&
                   F_PRUN == 12 && F_SIGNS == 13 && F_SIGNT == 14 && F_DENSE1X2 == 15,
               "op kinds as documented in qcs_b200.h");
-static_assert(sizeof(qcs_b200_plan_summary) == 4 * 4 + 4 * QCS_B200_PLAN_KINDS + 8, "qcs_b200_plan_summary layout");
+static_assert(sizeof(qcs_b200_plan_summary) == 4 * 4 + 4 * QCS_B200_PLAN_KINDS + 8 + 4 * 4,
+              "qcs_b200_plan_summary layout");
 
 void plan_summary(int n, const qcs_b200_gate *gates, uint64_t count, qcs_b200_plan_summary &out)
 {
@@ -88,13 +89,26 @@ void plan_summary(int n, const qcs_b200_gate *gates, uint64_t count, qcs_b200_pl
             continue;
         }
         std::vector<FPassParams> params;
-        if (!build_pieces(queue, s.pass, n, params, nullptr, nullptr, &tables))
+        std::vector<std::vector<StageCond>> conds;
+        if (!build_pieces(queue, s.pass, n, params, nullptr, nullptr, &tables, &conds))
         {
             out.plain_gates += static_cast<uint32_t>(s.pass.ops.size());
             continue;
         }
-        for (const FPassParams &p : params)
+        for (size_t pi = 0; pi < params.size(); ++pi)
         {
+            const FPassParams &p = params[pi];
+            TPassParams tp;
+            TBuildParams tb;
+            if (make_tensor_params(p, conds[pi], tp, tb))
+            {
+                ++out.tensor_eligible;
+                if (tensor_pass_cost(tp) < register_pass_cost(p))
+                {
+                    ++out.tensor_passes;
+                    out.tensor_matrices += tb.nmats;
+                }
+            }
             ++out.passes;
             out.stages += static_cast<uint32_t>(p.nstages);
             out.ops += static_cast<uint32_t>(p.nops);

@@ -151,6 +151,7 @@ void Simulator::allocate_memory()
     QCSB_CUDA(cudaMallocHost(&host_pinned_, host_pinned_bytes_));
     fused_ = new FusedExecutor(stream_);
     fused_->set_options(opt_max_ops_, opt_local_bits_);
+    fused_->set_tensor_mode(opt_tensor_);
     fused_->set_cost_model(model_);
     set_zero_state();
 }
@@ -165,6 +166,17 @@ void Simulator::set_planner_options(int max_ops, int local_bits)
     opt_local_bits_ = local_bits;
     if (fused_)
         fused_->set_options(max_ops, local_bits);
+}
+
+void Simulator::set_tensor_mode(int mode)
+{
+    if (mode < 0 || mode > 2)
+        throw std::runtime_error(strformat("tensor pass mode %d is not 0 (never), 1 (auto) or 2 (always)", mode));
+    if (allocated())
+        flush();
+    opt_tensor_ = mode;
+    if (fused_)
+        fused_->set_tensor_mode(mode);
 }
 
 void Simulator::set_cost_model(CostModel *model)

@@ -117,6 +117,8 @@ class Simulator
     void synchronize();
 
     void set_planner_options(int max_ops, int local_bits);
+    void set_tensor_mode(int mode);
+    int tensor_mode() const { return opt_tensor_; }
     void set_cost_model(CostModel *model);
     FusedExecutor *fused_executor() { return fused_; }
 
@@ -159,7 +161,7 @@ class Simulator
     size_t pending_gates_ = 0;   // queued ops other than deferred collapses
     FusedExecutor *fused_ = nullptr;
     CostModel *model_ = nullptr;
-    int opt_max_ops_ = 0, opt_local_bits_ = 0;
+    int opt_max_ops_ = 0, opt_local_bits_ = 0, opt_tensor_ = 1;
 
     // scratch: reduction partials and results, pinned host mirror,
     // chunk staging for logical-order transfers, sampler tree
@@ -196,6 +198,9 @@ class FusedExecutor
         local_bits_ = local_bits;
     }
     void set_cost_model(CostModel *model) { model_ = model; }
+    // Tensor passes (tensor_pass.cu): 0 never, 1 where the cost estimate
+    // favours them (default), 2 wherever a pass's stages allow them.
+    void set_tensor_mode(int mode) { tensor_mode_ = mode; }
 
     // Which planner ran the last flush in learned mode (1 = learned,
     // 0 = greedy) and the device times the judge holds for that queue.
@@ -221,6 +226,11 @@ class FusedExecutor
     cudaEvent_t tables_copied_ = nullptr;
     int max_ops_ = 0;
     int local_bits_ = 0;
+    int tensor_mode_ = 1;
+    // matrices of the tensor pass being run: every pass's builder writes
+    // them right before the pass reads them, in stream order
+    double2 *mats_dev_ = nullptr;
+    size_t mats_cap_ = 0;   // matrices
     CostModel *model_ = nullptr;
     // "measured device time is the judge": per queue signature, the device
     // time of a flush under each planner; once both are known the faster one

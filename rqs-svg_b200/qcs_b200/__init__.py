@@ -45,6 +45,7 @@ GATES = {
 }
 
 FUSION_PLAIN, FUSION_GREEDY, FUSION_LEARNED = 0, 1, 2
+TENSOR_NEVER, TENSOR_AUTO, TENSOR_ALWAYS = 0, 1, 2
 
 
 class QCSError(RuntimeError):
@@ -59,6 +60,7 @@ class Stats(ctypes.Structure):
         ("fused_passes", ctypes.c_uint64),
         ("plain_gate_kernels", ctypes.c_uint64),
         ("algorithmic_bytes", ctypes.c_double),
+        ("tensor_passes", ctypes.c_uint64),
     ]
 
 
@@ -99,6 +101,10 @@ class PlanSummary(ctypes.Structure):
         ("ops", ctypes.c_uint32),
         ("kinds", ctypes.c_uint32 * PLAN_KINDS),
         ("table_entries", ctypes.c_uint64),
+        ("tensor_passes", ctypes.c_uint32),
+        ("tensor_eligible", ctypes.c_uint32),
+        ("tensor_matrices", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -187,6 +193,8 @@ class Library:
             "qcs_simulator_get_kernel_times": [_P, ctypes.POINTER(KernelTimes)],
             "qcs_b200_zsums_noalloc": [_P, ctypes.c_int, _P, _P],
             "qcs_simulator_set_planner_options": [_P, ctypes.c_int, ctypes.c_int],
+            "qcs_simulator_set_tensor_passes": [_P, ctypes.c_int],
+            "qcs_simulator_get_tensor_passes": [_P, ctypes.POINTER(ctypes.c_int)],
             "qcs_simulator_set_precision": [_P, ctypes.c_int],
             "qcs_simulator_get_precision": [_P, ctypes.POINTER(ctypes.c_int)],
             "qcs_simulator_get_pass_records": [_P, _FP, _FP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)],
@@ -436,6 +444,10 @@ class Simulator:
     def set_planner_options(self, max_gates_per_pass: int = 0, local_qubits: int = 0):
         self.lib.call("qcs_simulator_set_planner_options", self.h, max_gates_per_pass, local_qubits)
 
+    def set_tensor_passes(self, mode: int):
+        """0: never, 1: where cheaper (default), 2: wherever a pass allows."""
+        self.lib.call("qcs_simulator_set_tensor_passes", self.h, mode)
+
     def pass_records(self, capacity: int = 1 << 20):
         feats = np.zeros((capacity, 4), dtype=np.float32)
         ms = np.zeros(capacity, dtype=np.float32)
@@ -514,7 +526,8 @@ def plan_summary(lib: "Library", num_qubits: int, circuit) -> dict:
              ctypes.c_uint64(len(circuit)), ctypes.byref(out))
     kinds = {name: int(out.kinds[i]) for i, name in PLAN_KIND_NAMES.items()}
     return {"passes": out.passes, "plain_gates": out.plain_gates, "stages": out.stages, "ops": out.ops,
-            "kinds": kinds, "table_entries": int(out.table_entries)}
+            "kinds": kinds, "table_entries": int(out.table_entries), "tensor_passes": out.tensor_passes,
+            "tensor_eligible": out.tensor_eligible, "tensor_matrices": out.tensor_matrices}
 
 
 def fidelity(a: np.ndarray, b: np.ndarray) -> float:

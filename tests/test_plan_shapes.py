@@ -112,3 +112,20 @@ def test_measured_workloads_keep_their_pass_counts(gpu_lib):
     assert s["plain_gates"] == 0 and s["passes"] <= 110
     s = _summary(gpu_lib, 33, C.qft(33, seed=1)[0])
     assert s["plain_gates"] == 0 and s["passes"] <= 4
+
+
+def test_tensor_pass_choice(gpu_lib):
+    # the layered and matching workloads run almost every pass on the FP64
+    # tensor cores; the QFT's phase runs reach too many qubits outside their
+    # stages (one matrix per assignment of at most 8 of them) and stay on the
+    # register path
+    s = _summary(gpu_lib, 30, C.layered_u3_cz_cx_toffoli(30, 40, seed=1))
+    assert s["tensor_eligible"] == s["passes"] and s["tensor_passes"] >= s["passes"] - 2
+    assert s["tensor_matrices"] <= 4096 * s["tensor_passes"]
+    s = _summary(gpu_lib, 30, C.u3_random_matching(30, 60, seed=1))
+    assert s["tensor_passes"] >= 0.8 * s["passes"]
+    s = _summary(gpu_lib, 33, C.qft(33, seed=1)[0])
+    assert s["tensor_passes"] == 0
+    # passes with fewer than 11 local qubits have no tensor form
+    s = _summary(gpu_lib, 10, C.layered_u3_cz(10, 8, seed=1))
+    assert s["tensor_eligible"] == 0

@@ -1,0 +1,126 @@
+"""Tensor passes (stages as 16 x 16 matrices on the FP64 tensor cores)
+against the oracle: forced wherever a pass allows them (QCS_TENSOR_ALWAYS),
+on registers of 12-24 qubits, with every gate kind of at most two targets,
+controls on stage, local and chunk qubits, diagonal runs, mid-circuit
+measurements (their collapse rides along as a zeroing diagonal), mappings
+and state preparations. Tolerance: complex128 amplitudes to 1e-12, clbits
+exactly."""
+
+import numpy as np
+import pytest
+
+import qcs_b200
+from qcs_b200 import GATES, FUSION_GREEDY, TENSOR_ALWAYS, TENSOR_AUTO, TENSOR_NEVER
+from qcs_b200 import circuits as C
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+TWO_TARGET = sorted(g for g, (_, nt) in GATES.items() if nt <= 2)
+
+
+def _run(lib, n, circ, tensor=None, seed=1, start=None, mapping=None):
+    with qcs_b200.Simulator(lib, n, n, seed=seed, mapping=mapping,
+                            fusion=FUSION_GREEDY if tensor is not None else None) as sim:
+        if tensor is not None:
+            sim.set_tensor_passes(tensor)
+        if start is not None:
+            sim.set_statevector(start)
+        sim.run(circ)
+        state = sim.statevector()   # flushes the queue
+        stats = sim.stats() if tensor is not None else None
+        return state, sim.clbits_string(), stats
+
+
+def _random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+@pytest.mark.parametrize("n", [12, 16, 20])
+def test_layered_circuits(gpu_lib, oracle_lib, n):
+    for circ in (C.layered_u3_cz_cx_toffoli(n, 6, seed=n), C.u3_random_matching(n, 6, seed=n + 1),
+                 C.layered_u3_cz(n, 6, seed=n + 2)):
+        got, _, stats = _run(gpu_lib, n, circ, tensor=TENSOR_ALWAYS)
+        ref, _, _ = _run(oracle_lib, n, circ)
+        assert stats["tensor_passes"] > 0
+        assert np.max(np.abs(got - ref)) <= TOL
+        assert qcs_b200.fidelity(got, ref) >= 1 - 1e-12
+
+
+@pytest.mark.parametrize("n", [12, 14, 17])
+def test_every_two_target_gate_kind_with_controls(gpu_lib, oracle_lib, n):
+    start = _random_state(n, n)
+    for i, name in enumerate(TWO_TARGET):
+        circ = C.random_circuit(n, 40, seed=n * 977 + i, max_controls=2, gates=[name, "u3", "h"])
+        got, _, _ = _run(gpu_lib, n, circ, tensor=TENSOR_ALWAYS, start=start)
+        ref, _, _ = _run(oracle_lib, n, circ, start=start)
+        assert np.max(np.abs(got - ref)) <= TOL, name
+
+
+@pytest.mark.parametrize("n", [12, 16, 19])
+def test_mixed_random_circuits(gpu_lib, oracle_lib, n):
+    circ = C.random_circuit(n, 300, seed=5000 + n, max_controls=3, gates=TWO_TARGET)
+    start = _random_state(n, 3)
+    got, _, stats = _run(gpu_lib, n, circ, tensor=TENSOR_ALWAYS, start=start)
+    ref, _, _ = _run(oracle_lib, n, circ, start=start)
+    assert np.max(np.abs(got - ref)) <= TOL
+    # the same queue without tensor passes
+    plain, _, stats0 = _run(gpu_lib, n, circ, tensor=TENSOR_NEVER, start=start)
+    assert stats0["tensor_passes"] == 0
+    assert np.max(np.abs(got - plain)) <= TOL
+
+
+@pytest.mark.parametrize("n", [12, 15])
+def test_measurements_and_resets(gpu_lib, oracle_lib, n):
+    circ = [("h", (), (q,), (), ()) for q in range(n)]
+    circ += C.random_circuit(n, 150, seed=70 + n, max_controls=2, gates=TWO_TARGET, measure_prob=0.08)
+    circ += C.layered_u3_cz(n, 3, seed=n)
+    circ += [("measure", (q,), (q,), (), ()) for q in range(0, n, 2)]
+    circ += C.layered_u3_cz_cx_toffoli(n, 2, seed=n)
+    for seed in (11, 12):
+        got, gbits, _ = _run(gpu_lib, n, circ, tensor=TENSOR_ALWAYS, seed=seed)
+        ref, rbits, _ = _run(oracle_lib, n, circ, seed=seed)
+        assert gbits == rbits
+        assert np.max(np.abs(got - ref)) <= TOL
+
+
+def test_mapping_and_qft(gpu_lib, oracle_lib):
+    n = 16
+    mapping = list(np.random.default_rng(3).permutation(n))
+    circ = C.layered_u3_cz_cx_toffoli(n, 5, seed=9) + C.qft(n, seed=2)[0]
+    got, _, _ = _run(gpu_lib, n, circ, tensor=TENSOR_ALWAYS, mapping=mapping)
+    ref, _, _ = _run(oracle_lib, n, circ, mapping=mapping)
+    assert np.max(np.abs(got - ref)) <= TOL
+
+
+def test_twenty_four_qubits_automatic_choice(gpu_lib, oracle_lib):
+    n = 24
+    circ = C.layered_u3_cz_cx_toffoli(n, 4, seed=21)
+    got, _, stats = _run(gpu_lib, n, circ, tensor=TENSOR_AUTO)
+    ref, _, _ = _run(oracle_lib, n, circ)
+    assert stats["tensor_passes"] > 0
+    assert np.max(np.abs(got - ref)) <= TOL
+    assert qcs_b200.fidelity(got, ref) >= 1 - 1e-12
+
+
+def test_repeated_runs_reuse_matrix_buffer(gpu_lib, oracle_lib):
+    """Flushes of different sizes on one simulator (the matrix buffer grows
+    between passes) and the |0..0> start of a fresh register."""
+    n = 14
+    circs = [C.layered_u3_cz(n, 2, seed=1), C.u3_random_matching(n, 12, seed=2), C.layered_u3_cz(n, 1, seed=3)]
+    with qcs_b200.Simulator(gpu_lib, n, fusion=FUSION_GREEDY) as sim:
+        sim.set_tensor_passes(TENSOR_ALWAYS)
+        for circ in circs + circs[::-1]:
+            sim.set_state("zero")
+            sim.run(circ)
+            got = sim.statevector()
+            ref, _, _ = _run(oracle_lib, n, circ)
+            assert np.max(np.abs(got - ref)) <= TOL
+
+
+def test_tensor_mode_argument_checks(gpu_lib):
+    with qcs_b200.Simulator(gpu_lib, 12) as sim:
+        with pytest.raises(qcs_b200.QCSError, match="tensor pass mode"):
+            sim.set_tensor_passes(3)
