@@ -911,11 +911,12 @@ __global__ void __launch_bounds__(128, sizeof(Real) == 8 ? 3 : 4)
 // matrix's stage, exactly as the register stage above applies them, to the
 // unit vector of input slot col, with the stage's condition bits set as the
 // matrix index says and every other bit outside the stage zero (no op of the
-// stage depends on those). The resulting column is written as the B
-// fragments of the tensor pass's m16n8k8 products: B[u][nu] for input slot
-// u (tensor layout) and output column nu = 8i + g, i.e. output slot
-// 4i + (g >> 1), real part for even g and imaginary part for odd g; lane
-// 4g + t of fragment 4j + i holds (B[8j + t][8i + g], B[8j + t + 4][8i + g]).
+// stage depends on those). The resulting column M[.][col] is written as the
+// B fragments of the tensor pass's m16n8k8 products, for the real part Mr,
+// the imaginary part Mi and Mr + Mi: B[u][nu] = M[s(nu)][u] for input slot u
+// (tensor layout) and output column nu = 8i + 2t' + e of n-tile i, output
+// slot s(nu) = 8i + t' + 4e; lane 4g + t of fragment 4 * part + 2j + i
+// holds (B[8j + t][8i + g], B[8j + t + 4][8i + g]).
 template <typename Real>
 __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant__ FPassParams p,
                                                           const __grid_constant__ TBuildParams tb)
@@ -1010,14 +1011,45 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
         apply_op<V>(a, op, PoolEntries<V>{p, op.moff}, j0, cbase, ss);
     }
     const int j = col >> 3, b = (col >> 2) & 1, t = col & 3;
+    if (tb.tf32)
+    {
+        // TF32 high part and the TF32 rounding of the remainder, per entry
+        auto split = [](double v, uint32_t &hi, uint32_t &lo) {
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(static_cast<float>(v)));
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(static_cast<float>(v - __uint_as_float(hi))));
+        };
+        uint32_t *out = reinterpret_cast<uint32_t *>(tb.out) + static_cast<size_t>(mat) * kTensorFragments * 128;
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int g = 0; g < 8; ++g)
+            {
+                const V y = a[reg(8 * i + (g >> 1) + 4 * (g & 1))];
+                const double parts[3] = {y.x, y.y, y.x + y.y};
+                const int lane = g * 4 + t;
+#pragma unroll
+                for (int part = 0; part < 3; ++part)
+                {
+                    uint32_t hi, lo;
+                    split(parts[part], hi, lo);
+                    uint32_t *f = out + ((part * 4 + j * 2 + i) * 32 + lane) * 4;
+                    f[b] = hi;
+                    f[2 + b] = lo;
+                }
+            }
+        return;
+    }
     Real *out = reinterpret_cast<Real *>(tb.out) + static_cast<size_t>(mat) * kTensorFragments * 64;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int g = 0; g < 8; ++g)
         {
-            const V y = a[reg(4 * i + (g >> 1))];
-            out[((j * 4 + i) * 32 + g * 4 + t) * 2 + b] = (g & 1) ? y.y : y.x;
+            const V y = a[reg(8 * i + (g >> 1) + 4 * (g & 1))];
+            const int lane = g * 4 + t;
+            out[((0 * 4 + j * 2 + i) * 32 + lane) * 2 + b] = y.x;
+            out[((1 * 4 + j * 2 + i) * 32 + lane) * 2 + b] = y.y;
+            out[((2 * 4 + j * 2 + i) * 32 + lane) * 2 + b] = y.x + y.y;
         }
 }
 
@@ -2685,7 +2717,7 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
             tp.mats = mats_dev_;
             tp.state = state;
             launches += launch_stage_matrices<double>(prm, tb, stream_);
-            launches += launch_tensor_pass<double>(tp, stream_);
+            launches += c64 ? launch_tensor_pass<float>(tp, stream_) : launch_tensor_pass<double>(tp, stream_);
             ++stats.tensor_passes;
         }
         else
@@ -2724,24 +2756,27 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         for (size_t i = before; i < params.size(); ++i)
         {
             tensor_of.push_back(-1);
-            if (c64 || tensor_mode_ == 0)
-                continue;
-            tparams.emplace_back();
-            tbuild.emplace_back();
-            if (make_tensor_params(params[i], conds[i], tparams.back(), tbuild.back()) &&
-                (tensor_mode_ == 2 || tensor_pass_cost(tparams.back()) < register_pass_cost(params[i])))
+            if (tensor_mode_ != 0)
             {
-                tensor_of.back() = static_cast<int>(tparams.size()) - 1;
+                tparams.emplace_back();
+                tbuild.emplace_back();
+                if (make_tensor_params(params[i], conds[i], amp_bytes, tparams.back(), tbuild.back()) &&
+                    (tensor_mode_ == 2 ||
+                     tensor_pass_cost(tparams.back(), amp_bytes) < register_pass_cost(params[i], amp_bytes)))
+                {
+                    tensor_of.back() = static_cast<int>(tparams.size()) - 1;
+                }
+                else
+                {
+                    tparams.pop_back();
+                    tbuild.pop_back();
+                }
             }
-            else
-            {
-                tparams.pop_back();
-                tbuild.pop_back();
-            }
-        }
-        if (c64)
-            for (size_t i = before; i < params.size(); ++i)
+            // complex64 register passes read their entries as float2; tensor
+            // passes build their matrices from the double2 entries
+            if (c64 && tensor_of.back() < 0)
                 entries_to_float(params[i].entries, params[i].nentries);
+        }
         for (size_t i = before; i < params.size(); ++i)
             add_step((long)i);
     }

@@ -137,9 +137,11 @@ constexpr int kTensorLocal = 11;       // local qubits of a tensor pass (2^11-am
 constexpr int kTensorTileBits = 3;     // group bits that pick a warp's tiles: local condition bits go there
 constexpr int kTensorMaxCond = 8;      // condition bits of a stage: at most 2^8 matrices
 constexpr int kTensorMaxMats = 4096;   // matrices of one pass
-// Per matrix: the B fragments of the m16n8k8 products, 8 fragments x 32
-// lanes x (b0, b1), 4 KiB for complex128.
-constexpr int kTensorFragments = 8;
+// Per matrix: the B fragments of the m16n8k8 products, 12 fragments (real
+// part, imaginary part, their sum; x 2 k-steps x 2 n-tiles) x 32 lanes x
+// 16 bytes: (b0, b1) in FP64 for complex128, (b0, b1) TF32 high parts and
+// (b0, b1) TF32 low parts for complex64; 6 KiB either way.
+constexpr int kTensorFragments = 12;
 
 struct TStage
 {
@@ -161,7 +163,8 @@ struct TBuildParams
 {
     int nstages;
     uint32_t nmats;
-    double2 *out;                // nmats x kTensorFragments x 32 lanes x double2
+    int tf32;                    // fragments as TF32 high/low parts (complex64 passes)
+    double2 *out;                // nmats x kTensorFragments x 32 lanes x 16 bytes
     TStage stages[kFusedMaxStages];
 };
 
@@ -176,16 +179,21 @@ struct TPassParams
     uint64_t qbit[kMaxLocal];
     int nstages;
     TStage stages[kFusedMaxStages];
+    // per stage: shared-memory offsets (swizzled) of group bits 0..6 and
+    // slot bits 0..3
+    uint16_t swz[kFusedMaxStages][12];
 };
 
-// Tensor-pass layout of a built pass: false when a stage depends on more
-// condition bits than a tensor pass handles (or k is not kTensorLocal).
-bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, TPassParams &tp,
+// Tensor-pass layout of a built pass (amp_bytes 16: complex128, 8:
+// complex64): false when a stage depends on more condition bits than a
+// tensor pass handles (or k is not kTensorLocal). The matrices are built
+// from prm's entries in FP64 (complex64 passes keep them as double2).
+bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, int amp_bytes, TPassParams &tp,
                         TBuildParams &tb);
-// FP64 work per amplitude of a pass on the register path and on the tensor
-// path (both in multiply-adds, scaled by the measured efficiency of each).
-double register_pass_cost(const FPassParams &prm);
-double tensor_pass_cost(const TPassParams &tp);
+// Estimated time of a pass on the register path and on the tensor path, in
+// one unit (multiply-adds per amplitude at the register path's FP64 rate).
+double register_pass_cost(const FPassParams &prm, int amp_bytes);
+double tensor_pass_cost(const TPassParams &tp, int amp_bytes);
 // Builds the pass's matrices (stage_matrix_kernel) and runs the pass;
 // returns the number of kernels launched.
 template <typename R>

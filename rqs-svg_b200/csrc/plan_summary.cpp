@@ -100,10 +100,10 @@ void plan_summary(int n, const qcs_b200_gate *gates, uint64_t count, qcs_b200_pl
             const FPassParams &p = params[pi];
             TPassParams tp;
             TBuildParams tb;
-            if (make_tensor_params(p, conds[pi], tp, tb))
+            if (make_tensor_params(p, conds[pi], 16, tp, tb))
             {
                 ++out.tensor_eligible;
-                if (tensor_pass_cost(tp) < register_pass_cost(p))
+                if (tensor_pass_cost(tp, 16) < register_pass_cost(p, 16))
                 {
                     ++out.tensor_passes;
                     out.tensor_matrices += tb.nmats;

@@ -1,5 +1,7 @@
 // Tensor passes: the stages of a fused pass as dense 16 x 16 complex
-// matrices on the FP64 tensor cores (mma.sync m16n8k8, DMMA).
+// matrices on the tensor cores (mma.sync m16n8k8): FP64 (DMMA) for
+// complex128 registers, TF32 with a three-term split and FP32 accumulation
+// for complex64 registers.
 //
 // A fused pass (fused_pass.cu) stages a 2^11-amplitude chunk in shared memory
 // and runs its gates in stages of 4 local "stage bits". On the register path
@@ -8,23 +10,32 @@
 // product as one 16 x 16 matrix M to every 16-amplitude group of the chunk.
 // Gates of the stage that depend on bits outside it (controls, diagonal
 // targets) make M depend on those bits; the stage then has one matrix per
-// assignment of its condition bits (at most 2^8), all built on the GPU from
-// the pass's ops before the pass (stage_matrix_kernel).
+// assignment of its condition bits (at most 2^8), all built on the GPU in
+// FP64 from the pass's ops before the pass (stage_matrix_kernel).
 //
 // Product layout. A warp takes 16 groups (rows r) at a time: y_r = M x_r for
-// all 16 rows is D = A B with A (16 x 16 per component) the rows' input
-// amplitudes and B[u][nu] = Re or Im of M[u'][u] (nu = output slot u' and
-// component). With R = Re(x) B and S = Im(x) B (eight m16n8k8 products each,
-// K = 16 input slots, N = 32 output columns), Re y = R_re - S_im and
-// Im y = R_im + S_re. Lane (g, t) of the warp (g = lane / 4, t = lane % 4)
-// holds rows g and g + 8 at input slots t, t + 4, t + 8, t + 12 for the A
-// fragments, and the accumulators give it the same rows at output slots
-// 4i + t for n-tiles i: it loads and stores the same 8 shared-memory
-// positions, so the stage runs in place without extra barriers.
+// all 16 rows, with M = Mr + i Mi, in three real products (Gauss):
+// T1 = Mr Re(x), T2 = Mi Im(x), T3 = (Mr + Mi)(Re x + Im x), then
+// Re y = T1 - T2 and Im y = T3 - T1 - T2: twelve m16n8k8 products per 16
+// rows (K = 16 input slots in two k-steps, N = 16 output slots in two
+// n-tiles) instead of the sixteen of the four-product form. Lane (g, t) of
+// the warp (g = lane / 4, t = lane % 4) holds rows g and g + 8 at input
+// slots t, t + 4, t + 8, t + 12 for the A fragments; output column
+// nu = 8i + 2t + e of n-tile i stands for output slot 8i + t + 4e, so the
+// accumulators give the lane the same four slots of the same rows: it loads
+// and stores the same 8 shared-memory positions, and the stage runs in place
+// without barriers between the warp's tiles.
 //
-// FP64 work: 64 multiply-adds per amplitude and stage (the register path:
-// 8 per complex 2x2 gate), at the FP64 tensor rate, which on B200 equals the
-// FMA rate, but with one instruction per 1024 multiply-adds instead of 32.
+// complex128: 48 FP64 multiply-adds per amplitude and stage on the tensor
+// pipe plus 4 additions (the register path: 8 multiply-adds per complex 2x2
+// gate), at the FP64 tensor rate, which on B200 equals the FMA rate, but
+// with one instruction per 1024 multiply-adds instead of 32.
+//
+// complex64: every operand is split into a TF32 high part and the TF32
+// rounding of the remainder; each product is a_lo b_hi + a_hi b_lo +
+// a_hi b_hi (the lo x lo term, 2^-22 relative, is dropped) accumulated in
+// FP32, about FP32's own accuracy, at the TF32 tensor rate (7.5x the FP64
+// rate on B200).
 
 #include "fused_pass.h"
 
@@ -36,36 +47,96 @@ namespace qcsb
 namespace
 {
 
-__device__ __forceinline__ int swz2(int j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7); }
-
-__device__ __forceinline__ void cp_async16(double2 *smem, const double2 *gmem)
-{
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// D += A B for one m16n8k8 FP64 tile (A 16 x 8 row-major fragments a0..a3,
-// B 8 x 8 fragments b0, b1, D 16 x 8 fragments d0..d3).
-__device__ __forceinline__ void dmma(double (&d)[4], double a0, double a1, double a2, double a3, double b0, double b1)
-{
-    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-                 "{%0,%1,%2,%3};\n"
-                 : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-                 : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
-}
-
 constexpr int kThreads = 1 << (kTensorLocal - kStageBits);   // 128: 4 warps, two 16-group tiles each
 constexpr int kSlots = 1 << kStageBits;
 constexpr int kChunk = 1 << kTensorLocal;
 
+// Shared-memory swizzles (linear over GF(2)): 16-byte amplitudes fold 3
+// index bits into the 3 bits that pick a 16-byte bank group, 8-byte
+// amplitudes fold 4.
+__host__ __device__ __forceinline__ int swz16(int j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7); }
+__host__ __device__ __forceinline__ int swz8(int j) { return j ^ (((j >> 4) ^ (j >> 8)) & 15); }
+
+template <typename Real>
+struct Tensor;
+
+template <>
+struct Tensor<double>
+{
+    typedef double2 V;
+    typedef double2 Frag;   // (b0, b1)
+    static __device__ __forceinline__ int swz(int j) { return swz16(j); }
+    static __device__ __forceinline__ void cp_async(V *smem, const V *gmem)
+    {
+        const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    }
+    // D += A B, m16n8k8 FP64: a0 = A[g][t], a1 = A[g + 8][t], a2 = A[g][t + 4],
+    // a3 = A[g + 8][t + 4]; b0 = B[t][g], b1 = B[t + 4][g]; d0 = D[g][2t],
+    // d1 = D[g][2t + 1], d2 = D[g + 8][2t], d3 = D[g + 8][2t + 1]
+    static __device__ __forceinline__ void mma(double (&d)[4], double a0, double a1, double a2, double a3,
+                                               const Frag &b)
+    {
+        asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+            : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b.x), "d"(b.y));
+    }
+};
+
+__device__ __forceinline__ uint32_t to_tf32(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+template <>
+struct Tensor<float>
+{
+    typedef float2 V;
+    typedef uint4 Frag;   // TF32 (hi b0, hi b1, lo b0, lo b1)
+    static __device__ __forceinline__ int swz(int j) { return swz8(j); }
+    static __device__ __forceinline__ void cp_async(V *smem, const V *gmem)
+    {
+        const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+    }
+    static __device__ __forceinline__ void tf32mma(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                                   uint32_t b0, uint32_t b1)
+    {
+        asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    }
+    // D += A B with A and B split into TF32 high and low parts (layout as
+    // for FP64); the small terms go first
+    static __device__ __forceinline__ void mma(float (&d)[4], float a0, float a1, float a2, float a3, const Frag &b)
+    {
+        const uint32_t h0 = to_tf32(a0), h1 = to_tf32(a1), h2 = to_tf32(a2), h3 = to_tf32(a3);
+        const uint32_t l0 = to_tf32(a0 - __uint_as_float(h0)), l1 = to_tf32(a1 - __uint_as_float(h1));
+        const uint32_t l2 = to_tf32(a2 - __uint_as_float(h2)), l3 = to_tf32(a3 - __uint_as_float(h3));
+        tf32mma(d, l0, l1, l2, l3, b.x, b.y);
+        tf32mma(d, h0, h1, h2, h3, b.z, b.w);
+        tf32mma(d, h0, h1, h2, h3, b.x, b.y);
+    }
+};
+
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <typename Real>
 __global__ void __launch_bounds__(kThreads, 3) tensor_pass_kernel(const __grid_constant__ TPassParams p)
 {
+    typedef Tensor<Real> TT;
+    typedef typename TT::V V;
+    typedef typename TT::Frag Frag;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2 *smem = reinterpret_cast<double2 *>(smem_raw);
-    double2 *const state = static_cast<double2 *>(p.state);
+    V *smem = reinterpret_cast<V *>(smem_raw);
+    V *const state = static_cast<V *>(p.state);
+    const Frag *const mats = reinterpret_cast<const Frag *>(p.mats);
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
@@ -98,38 +169,66 @@ __global__ void __launch_bounds__(kThreads, 3) tensor_pass_kernel(const __grid_c
                 off |= hb[b];
         return off;
     };
-    auto issue_load = [&](uint64_t c, double2 *dst) {
-        const uint64_t cb = chunk_base(c);
+    auto issue_load = [&](uint64_t cb, V *dst) {
         if (p.from_zero)
         {
 #pragma unroll
             for (int m = 0; m < kSlots; ++m)
             {
                 const bool one = cb == 0 && m == 0 && tid == 0;
-                dst[swz2(tid + m * kThreads)] = make_double2(one ? 1.0 : 0.0, 0.0);
+                dst[TT::swz(tid + m * kThreads)] = V{one ? Real(1) : Real(0), Real(0)};
             }
         }
         else
         {
 #pragma unroll
             for (int m = 0; m < kSlots; ++m)
-                cp_async16(dst + swz2(tid + m * kThreads), state + (cb | elem_offset(m)));
+                TT::cp_async(dst + TT::swz(tid + m * kThreads), state + (cb | elem_offset(m)));
         }
         cp_commit();
+    };
+
+    // B fragments of one stage matrix: (Mr, Mi, Mr + Mi) x k-step j x
+    // n-tile i. The warp loads the next stage's fragments (or the next
+    // chunk's first stage's) before the barrier that ends a stage, so that
+    // their latency overlaps the wait.
+    Frag bf[kTensorFragments];
+    int bf_st = -1;
+    uint32_t bf_v = 0;
+    auto matrix_of = [&](int st, uint64_t cb, int mt) -> uint32_t {
+        const TStage &S = p.stages[st];
+        uint32_t vc = 0;
+        for (int i = 0; i < S.ngc; ++i)
+            vc |= static_cast<uint32_t>((cb >> S.gq[i]) & 1) << i;
+        const uint32_t tile = static_cast<uint32_t>(mt | (warp << 1));
+        return (tile & ((1u << S.nlc) - 1u)) | (vc << S.nlc);
+    };
+    auto fetch = [&](int st, uint32_t v) {
+        const Frag *w = mats + (static_cast<size_t>(p.stages[st].woff + v) * kTensorFragments) * 32 + lane;
+#pragma unroll
+        for (int f = 0; f < kTensorFragments; ++f)
+            bf[f] = __ldg(w + f * 32);
+        bf_st = st;
+        bf_v = v;
     };
 
     uint64_t c = blockIdx.x;
     if (c >= p.chunks)
         return;
-    issue_load(c, smem);
+    uint64_t cbase_next = chunk_base(c);
+    issue_load(cbase_next, smem);
+    if (p.nstages > 0)
+        fetch(0, matrix_of(0, cbase_next, 0));
     int cur = 0;
     for (; c < p.chunks; c += gridDim.x)
     {
-        double2 *sb = smem + cur * kChunk;
+        V *sb = smem + cur * kChunk;
+        const uint64_t cbase = cbase_next;
         const uint64_t next = c + gridDim.x;
         if (next < p.chunks)
         {
-            issue_load(next, smem + (cur ^ 1) * kChunk);
+            cbase_next = chunk_base(next);
+            issue_load(cbase_next, smem + (cur ^ 1) * kChunk);
             cp_wait<1>();
         }
         else
@@ -137,98 +236,83 @@ __global__ void __launch_bounds__(kThreads, 3) tensor_pass_kernel(const __grid_c
             cp_wait<0>();
         }
         __syncthreads();
-        const uint64_t cbase = chunk_base(c);
 
         for (int st = 0; st < p.nstages; ++st)
         {
-            const TStage &S = p.stages[st];
             // swizzled offsets of the group and slot bits (the swizzle is
             // linear over GF(2): positions combine by XOR)
+            const uint16_t *sw = p.swz[st];
             uint32_t gbit[7], sbit[kStageBits];
 #pragma unroll
             for (int i = 0; i < 7; ++i)
-                gbit[i] = static_cast<uint32_t>(swz2(1 << S.gpos[i]));
+                gbit[i] = sw[i];
 #pragma unroll
             for (int b = 0; b < kStageBits; ++b)
-                sbit[b] = static_cast<uint32_t>(swz2(1 << S.sbits[b]));
-            uint32_t vc = 0;
-            for (int i = 0; i < S.ngc; ++i)
-                vc |= static_cast<uint32_t>((cbase >> S.gq[i]) & 1) << i;
-            uint32_t lane_pos = ((g & 1) ? gbit[0] : 0u) ^ ((g & 2) ? gbit[1] : 0u) ^ ((g & 4) ? gbit[2] : 0u) ^
-                                ((t & 1) ? sbit[0] : 0u) ^ ((t & 2) ? sbit[1] : 0u);
+                sbit[b] = sw[7 + b];
+            const uint32_t lane_pos = ((g & 1) ? gbit[0] : 0u) ^ ((g & 2) ? gbit[1] : 0u) ^
+                                      ((g & 4) ? gbit[2] : 0u) ^ ((t & 1) ? sbit[0] : 0u) ^ ((t & 2) ? sbit[1] : 0u);
             const uint32_t hpos = gbit[3];
-            uint32_t last_v = 0xffffffffu;
-            double2 bf[kTensorFragments];
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt)
             {
                 const uint32_t tile = static_cast<uint32_t>(mt | (warp << 1));
-                const uint32_t v = (tile & ((1u << S.nlc) - 1u)) | (vc << S.nlc);
-                if (v != last_v)
-                {
-                    const double2 *w = p.mats + (static_cast<size_t>(S.woff + v) * kTensorFragments) * 32 + lane;
-#pragma unroll
-                    for (int f = 0; f < kTensorFragments; ++f)
-                        bf[f] = __ldg(w + f * 32);
-                    last_v = v;
-                }
+                const uint32_t v = matrix_of(st, cbase, mt);
+                if (bf_st != st || bf_v != v)
+                    fetch(st, v);
                 const uint32_t base = lane_pos ^ ((tile & 1) ? gbit[4] : 0u) ^ ((tile & 2) ? gbit[5] : 0u) ^
                                       ((tile & 4) ? gbit[6] : 0u);
                 auto pos = [&](int h, int m) {
                     return base ^ (h ? hpos : 0u) ^ ((m & 1) ? sbit[2] : 0u) ^ ((m & 2) ? sbit[3] : 0u);
                 };
-                double2 x[2][4];
+                // x[h][m]: row g + 8h, input slot t + 4m
+                V x[2][4];
+                Real xs[2][4];
 #pragma unroll
                 for (int h = 0; h < 2; ++h)
 #pragma unroll
                     for (int m = 0; m < 4; ++m)
+                    {
                         x[h][m] = sb[pos(h, m)];
+                        xs[h][m] = x[h][m].x + x[h][m].y;
+                    }
 #pragma unroll
-                for (int ih = 0; ih < 2; ++ih)
+                for (int i = 0; i < 2; ++i)
                 {
-                    double racc[2][4], sacc[2][4];
+                    Real t1[4] = {0, 0, 0, 0}, t2[4] = {0, 0, 0, 0}, t3[4] = {0, 0, 0, 0};
 #pragma unroll
-                    for (int ii = 0; ii < 2; ++ii)
-#pragma unroll
-                        for (int e = 0; e < 4; ++e)
-                            racc[ii][e] = sacc[ii][e] = 0.0;
-#pragma unroll
-                    for (int ii = 0; ii < 2; ++ii)
+                    for (int j = 0; j < 2; ++j)
                     {
-                        const int i = 2 * ih + ii;
-#pragma unroll
-                        for (int j = 0; j < 2; ++j)
-                        {
-                            const double2 b = bf[j * 4 + i];
-                            dmma(racc[ii], x[0][2 * j].x, x[1][2 * j].x, x[0][2 * j + 1].x, x[1][2 * j + 1].x, b.x, b.y);
-                            dmma(sacc[ii], x[0][2 * j].y, x[1][2 * j].y, x[0][2 * j + 1].y, x[1][2 * j + 1].y, b.x, b.y);
-                        }
+                        TT::mma(t1, x[0][2 * j].x, x[1][2 * j].x, x[0][2 * j + 1].x, x[1][2 * j + 1].x,
+                                bf[0 * 4 + j * 2 + i]);
+                        TT::mma(t2, x[0][2 * j].y, x[1][2 * j].y, x[0][2 * j + 1].y, x[1][2 * j + 1].y,
+                                bf[1 * 4 + j * 2 + i]);
+                        TT::mma(t3, xs[0][2 * j], xs[1][2 * j], xs[0][2 * j + 1], xs[1][2 * j + 1],
+                                bf[2 * 4 + j * 2 + i]);
                     }
+                    // e = 0: row g, slot t + 8i; 1: row g, slot t + 8i + 4; 2, 3: row g + 8
 #pragma unroll
-                    for (int ii = 0; ii < 2; ++ii)
-                    {
-                        const int i = 2 * ih + ii;
-                        sb[pos(0, i)] = make_double2(racc[ii][0] - sacc[ii][1], racc[ii][1] + sacc[ii][0]);
-                        sb[pos(1, i)] = make_double2(racc[ii][2] - sacc[ii][3], racc[ii][3] + sacc[ii][2]);
-                    }
+                    for (int e = 0; e < 4; ++e)
+                        sb[pos(e >> 1, 2 * i + (e & 1))] = V{t1[e] - t2[e], t3[e] - (t1[e] + t2[e])};
                 }
             }
+            if (st + 1 < p.nstages)
+                fetch(st + 1, matrix_of(st + 1, cbase, 0));
+            else if (next < p.chunks)
+                fetch(0, matrix_of(0, cbase_next, 0));
             __syncthreads();
         }
 
 #pragma unroll
         for (int m = 0; m < kSlots; ++m)
-            __stcs(state + (cbase | elem_offset(m)), sb[swz2(tid + m * kThreads)]);
+            __stcs(state + (cbase | elem_offset(m)), sb[TT::swz(tid + m * kThreads)]);
         __syncthreads();
         cur ^= 1;
     }
 }
 
-int residue(int pos) { return pos % 3; }
-
 } // namespace
 
-bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, TPassParams &tp,
+bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, int amp_bytes, TPassParams &tp,
                         TBuildParams &tb)
 {
     if (prm.k != kTensorLocal || static_cast<int>(conds.size()) != prm.nstages || prm.nstages <= 0)
@@ -241,6 +325,14 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
     std::memcpy(tp.qmasks, prm.qmasks, sizeof(tp.qmasks));
     std::memcpy(tp.qbit, prm.qbit, sizeof(tp.qbit));
     tp.nstages = prm.nstages;
+    // A quarter warp's (16-byte amplitudes) or half warp's (8-byte) loads go
+    // to distinct bank groups when the lane bits of a stage (slot bits 0 and
+    // 1, group bit 0, and for 8-byte amplitudes group bit 1) sit on local
+    // positions of distinct residues mod 3 (mod 4): the swizzle sends
+    // position l to bank-group bit l mod 3 (mod 4).
+    const bool c64 = amp_bytes == 8;
+    const int mod = c64 ? 4 : 3;
+    const int row_bank_bits = c64 ? 2 : 1;
     uint32_t woff = 0;
     for (int s = 0; s < prm.nstages; ++s)
     {
@@ -254,15 +346,12 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
         if (woff + nm > static_cast<uint32_t>(kTensorMaxMats))
             return false;
         TStage &S = tp.stages[s];
-        // slot bits 0 and 1 (the lanes of a quarter warp) and group bit 0 on
-        // positions of three different residues mod 3: the swizzle then
-        // sends the quarter warp's eight 16-byte accesses to eight bank
-        // groups
+        // slot bits 0 and 1: two stage bits of distinct residues where there are
         int pr[kStageBits] = {0, 1, 2, 3};
         bool found = false;
         for (int a = 0; a < kStageBits && !found; ++a)
             for (int b = a + 1; b < kStageBits && !found; ++b)
-                if (residue(FS.sbits[a]) != residue(FS.sbits[b]))
+                if (FS.sbits[a] % mod != FS.sbits[b] % mod)
                 {
                     int rest = 0;
                     pr[0] = a;
@@ -280,22 +369,28 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
         }
         S.perm = perm;
         // group bits: the local condition bits first among the tile bits
-        // (4..6), the other positions outside the stage after them; group
-        // bit 0 on the residue that slot bits 0 and 1 leave free
+        // (4..6), the other positions outside the stage after them; the first
+        // row bits on the residues the slot bits leave free
         uint32_t stage_mask = 0;
         for (int b = 0; b < kStageBits; ++b)
             stage_mask |= 1u << FS.sbits[b];
-        std::vector<int> tile, rows;
+        std::vector<int> tile, rows, other;
         for (int l = 0; l < kTensorLocal; ++l)
             if ((cond.lmask >> l) & 1)
                 tile.push_back(l);
-        std::vector<int> other;
         for (int l = 0; l < kTensorLocal; ++l)
             if (!((stage_mask >> l) & 1) && !((cond.lmask >> l) & 1))
                 other.push_back(l);
-        const int want = 3 - residue(S.sbits[0]) - residue(S.sbits[1]);
-        std::stable_partition(other.begin(), other.end(), [&](int l) { return residue(l) == want; });
-        // rows take the first four (the free residue first), tiles the rest
+        uint32_t used = (1u << (S.sbits[0] % mod)) | (1u << (S.sbits[1] % mod));
+        for (int r = 0; r < row_bank_bits; ++r)
+            for (size_t i = 0; i < other.size(); ++i)
+                if (!((used >> (other[i] % mod)) & 1))
+                {
+                    used |= 1u << (other[i] % mod);
+                    rows.push_back(other[i]);
+                    other.erase(other.begin() + static_cast<long>(i));
+                    break;
+                }
         for (int l : other)
             (rows.size() < 4 ? rows : tile).push_back(l);
         if (rows.size() != 4 || tile.size() != 3)
@@ -313,15 +408,24 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
         S.woff = woff;
         woff += nm;
         tb.stages[s] = S;
+        for (int gb = 0; gb < 7; ++gb)
+            tp.swz[s][gb] = static_cast<uint16_t>(c64 ? swz8(1 << S.gpos[gb]) : swz16(1 << S.gpos[gb]));
+        for (int b = 0; b < kStageBits; ++b)
+            tp.swz[s][7 + b] = static_cast<uint16_t>(c64 ? swz8(1 << S.sbits[b]) : swz16(1 << S.sbits[b]));
     }
     tb.nstages = prm.nstages;
     tb.nmats = woff;
+    tb.tf32 = c64 ? 1 : 0;
     return true;
 }
 
-double register_pass_cost(const FPassParams &prm)
+// Pass costs in one unit (multiply-adds per amplitude at the register path's
+// FP64 rate), calibrated on B200 with the 30-qubit layered and matching
+// circuits: register passes keep the FP64 pipe about 45% busy; complex64
+// register passes take about 0.75 of the complex128 time; a complex128
+// tensor stage measured like 82 units, a complex64 one like 30.
+double register_pass_cost(const FPassParams &prm, int amp_bytes)
 {
-    // multiply-adds per amplitude of each op on the register path
     double fma = 0.0;
     for (int o = 0; o < prm.nops; ++o)
     {
@@ -340,35 +444,37 @@ double register_pass_cost(const FPassParams &prm)
         default: fma += 0.5; break;   // exchanges, sign flips, terms
         }
     }
-    // the register path keeps the FP64 pipe about 45% busy (measured)
-    return fma / 0.45;
+    return fma / 0.45 * (amp_bytes == 8 ? 0.75 : 1.0);
 }
 
-double tensor_pass_cost(const TPassParams &tp)
+double tensor_pass_cost(const TPassParams &tp, int amp_bytes)
 {
-    return 64.0 * tp.nstages / 0.85;
+    return (amp_bytes == 8 ? 30.0 : 82.0) * tp.nstages;
 }
 
-template <>
-int launch_tensor_pass<double>(const TPassParams &tp, cudaStream_t stream)
+template <typename R>
+int launch_tensor_pass(const TPassParams &tp, cudaStream_t stream)
 {
-    const size_t smem = 2 * sizeof(double2) * kChunk;
+    typedef typename Tensor<R>::V V;
+    const size_t smem = 2 * sizeof(V) * kChunk;
     static bool configured[64] = {};
     int dev = 0, sms = 0, per_sm = 0;
     QCSB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64 || !configured[dev])
     {
-        QCSB_CUDA(cudaFuncSetAttribute(tensor_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        QCSB_CUDA(cudaFuncSetAttribute(tensor_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem)));
         if (dev >= 0 && dev < 64)
             configured[dev] = true;
     }
     QCSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tensor_pass_kernel, kThreads, smem));
+    QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tensor_pass_kernel<R>, kThreads, smem));
     const uint64_t grid = std::min<uint64_t>(tp.chunks, static_cast<uint64_t>(sms) * std::max(per_sm, 1));
-    tensor_pass_kernel<<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(tp);
+    tensor_pass_kernel<R><<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(tp);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }
+template int launch_tensor_pass<double>(const TPassParams &, cudaStream_t);
+template int launch_tensor_pass<float>(const TPassParams &, cudaStream_t);
 
 } // namespace qcsb

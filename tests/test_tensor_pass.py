@@ -124,3 +124,43 @@ def test_tensor_mode_argument_checks(gpu_lib):
     with qcs_b200.Simulator(gpu_lib, 12) as sim:
         with pytest.raises(qcs_b200.QCSError, match="tensor pass mode"):
             sim.set_tensor_passes(3)
+
+
+def _run64(lib, n, circ, tensor, seed=1):
+    with qcs_b200.Simulator(lib, n, n, seed=seed, fusion=FUSION_GREEDY, precision=64) as sim:
+        sim.set_tensor_passes(tensor)
+        sim.run(circ)
+        state = sim.statevector()
+        return state, sim.clbits_string(), sim.stats()
+
+
+@pytest.mark.parametrize("n", [12, 16, 20])
+def test_complex64_tensor_passes(gpu_lib, oracle_lib, n):
+    """complex64 tensor passes (TF32 with a three-term split, FP32
+    accumulation): fidelity >= 1 - 1e-6 against the complex128 oracle, as
+    for the complex64 register path, and amplitudes within 1e-5."""
+    for circ in (C.layered_u3_cz_cx_toffoli(n, 8, seed=n), C.u3_random_matching(n, 8, seed=n + 1),
+                 C.random_circuit(n, 200, seed=900 + n, max_controls=2, gates=TWO_TARGET)):
+        ref, _, _ = _run(oracle_lib, n, circ)
+        got, _, stats = _run64(gpu_lib, n, circ, TENSOR_ALWAYS)
+        assert stats["tensor_passes"] > 0
+        assert qcs_b200.fidelity(got, ref) >= 1 - 1e-6
+        assert np.max(np.abs(got - ref)) <= 1e-5
+        reg, _, stats0 = _run64(gpu_lib, n, circ, TENSOR_NEVER)
+        assert stats0["tensor_passes"] == 0
+        assert qcs_b200.fidelity(got, reg) >= 1 - 1e-6
+
+
+def test_complex64_measurements(gpu_lib, oracle_lib):
+    n = 14
+    circ = [("h", (), (q,), (), ()) for q in range(n)]
+    circ += C.layered_u3_cz(n, 4, seed=5)
+    circ += [("measure", (q,), (q,), (), ()) for q in range(0, n, 3)]
+    circ += C.layered_u3_cz_cx_toffoli(n, 3, seed=6)
+    ref, rbits, _ = _run(oracle_lib, n, circ, seed=3)
+    got, gbits, stats = _run64(gpu_lib, n, circ, TENSOR_ALWAYS, seed=3)
+    assert stats["tensor_passes"] > 0
+    # outcomes follow the same draws unless a probability sits within the
+    # complex64 error of a draw (none does for this seed)
+    assert gbits == rbits
+    assert qcs_b200.fidelity(got, ref) >= 1 - 1e-6
