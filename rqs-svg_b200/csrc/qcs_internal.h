@@ -9,6 +9,8 @@
 
 #include <cuda_runtime.h>
 
+#include "fused_types.h"
+
 namespace qcsb
 {
 
@@ -96,18 +98,6 @@ GateOp make_gate_op(const GateMatrix &g, const int *tq, uint64_t cmask, uint64_t
 // (R = float, a B200 extension). Gate arithmetic runs in R; every norm and
 // probability reduction accumulates in FP64. Every launch helper below
 // enqueues on `stream` and returns the number of kernels launched.
-template <typename R>
-struct Cx;
-template <>
-struct Cx<double>
-{
-    typedef double2 T;
-};
-template <>
-struct Cx<float>
-{
-    typedef float2 T;
-};
 
 // Plain path: one kernel applying one GateOp to the whole register.
 template <typename R>
