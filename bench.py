@@ -114,14 +114,15 @@ def parse_args():
                     help="learned (default): the cost model is trained on pass timings recorded on smaller "
                          "registers, its plan and the greedy plan are both timed during warm-up and the faster "
                          "one runs; greedy: fused passes cut greedily; plain: one kernel per gate")
-    ap.add_argument("--tensor", choices=["never", "auto", "always"], default="auto",
-                    help="tensor passes (complex128 stages as 16x16 matrices on the FP64 tensor cores): "
-                         "auto (default) where the estimated FP64 work is lower")
+    ap.add_argument("--tensor", choices=["never", "auto", "always", "8x8"], default="auto",
+                    help="tensor passes (stages as dense matrices on the tensor cores): auto (default) where the "
+                         "cost estimate favours them, 16x16 or 8x8 stages; always: 16x16 stages wherever allowed; "
+                         "8x8: 8x8 stages wherever allowed")
     ap.add_argument("--precision", type=int, choices=[128, 64], default=None,
                     help="amplitude bits (default 128; 64 for hea_batch)")
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--depth", type=int, default=None, help="layers (default 40 layered, 60 matching)")
-    ap.add_argument("--train-qubits", default="18,20,22,24",
+    ap.add_argument("--train-qubits", default="20,22,24,26",
                     help="register sizes (comma-separated) the cost model's timings come from")
     ap.add_argument("--train-samples", type=int, default=20000, help="pass timings recorded to train the cost model")
     ap.add_argument("--batch-circuits", type=int, default=BATCH_CIRCUITS, help="circuits of the hea_batch workload")
@@ -378,7 +379,7 @@ def main():
               "learned": qcs_b200.FUSION_LEARNED}[args.fusion]
     sim = qcs_b200.Simulator(lib, n, seed=1234 + RANK, fusion=fusion, precision=args.precision)
     sim.set_tensor_passes({"never": qcs_b200.TENSOR_NEVER, "auto": qcs_b200.TENSOR_AUTO,
-                           "always": qcs_b200.TENSOR_ALWAYS}[args.tensor])
+                           "always": qcs_b200.TENSOR_ALWAYS, "8x8": qcs_b200.TENSOR_ALWAYS_8X8}[args.tensor])
     model, training, judge = None, None, None
     if fusion == qcs_b200.FUSION_LEARNED:
         model, training = train_planner(lib, args)

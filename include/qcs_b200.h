@@ -164,33 +164,44 @@ int qcs_simulator_get_kernel_times(qcs_simulator *sim, qcs_b200_kernel_times *ti
 int qcs_simulator_set_planner_options(qcs_simulator *sim, int max_gates_per_pass, int local_qubits);
 
 /*
- * Tensor passes (complex128 registers): a fused pass whose stages depend on
- * few bits outside themselves can run every stage as dense 16 x 16 matrices
- * on the FP64 tensor cores instead of gate by gate. mode 0: never; 1 (the
- * default): when the estimated FP64 work is lower; 2: whenever the pass
- * allows it. Results agree with the other paths to the rounding of the
- * matrix products (they replace the reference's per-pair 2x2 products,
- * src/qcs.cu:1139-1174, by products of whole stages).
+ * Tensor passes: a fused pass whose stages depend on few bits outside
+ * themselves can run every stage as a dense complex matrix on the tensor
+ * cores instead of gate by gate: 16 x 16 matrices (four qubits per stage) or
+ * 8 x 8 matrices (three qubits per stage, half the tensor work per stage),
+ * FP64 (DMMA) for complex128 registers, TF32 with a three-term split for
+ * complex64. mode 0: never; 1 (the default): whichever of the register path
+ * and the two matrix sizes the cost estimate favours; 2: 16 x 16 stages
+ * wherever a pass allows them; 3: 8 x 8 stages wherever a pass allows them.
+ * Results agree with the other paths to the rounding of the matrix products
+ * (they replace the reference's per-pair 2x2 products, src/qcs.cu:1139-1174,
+ * by products of whole stages).
  */
 #define QCS_TENSOR_NEVER 0
 #define QCS_TENSOR_AUTO 1
 #define QCS_TENSOR_ALWAYS 2
+#define QCS_TENSOR_ALWAYS_8X8 3
 int qcs_simulator_set_tensor_passes(qcs_simulator *sim, int mode);
 int qcs_simulator_get_tensor_passes(const qcs_simulator *sim, int *mode);
 
 /*
  * Pass timings recorded while kernel timing is enabled: for each fused pass
- * its features (4 floats: local qubits k; arithmetic ops, which run complex
- * multiply-adds on every amplitude; light ops, diagonal phases and
- * permutations such as X, CX, SWAP; log2 of the number of chunks, n - k,
- * capped at 16) and its device time in milliseconds. Reading synchronizes,
- * returns up to capacity records in *count and clears them.
+ * its QCS_PASS_FEATURES features and its device time in milliseconds. The
+ * features: block width (1 when the pass applies its gates one by one on
+ * the register path, 3 or 4 when it runs its stages as dense 8 x 8 or
+ * 16 x 16 matrices on the tensor cores); blocks (the pass's stages);
+ * arithmetic gates (complex multiply-adds on every amplitude); light ops
+ * (diagonal phases and permutations such as X, CX, SWAP); the target-qubit
+ * stride, log2 of the largest stride among the pass's local qubits (its
+ * highest local qubit); log2 of the number of chunks, n - k, capped at 16.
+ * Reading synchronizes, returns up to capacity records in *count and
+ * clears them.
  */
+#define QCS_PASS_FEATURES 6
 int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *milliseconds, uint32_t capacity,
                                    uint32_t *count);
 
 /*
- * Learned cost model of fused passes: an MLP 4 -> 64 -> 64 -> 1 (FP32, ReLU)
+ * Learned cost model of fused passes: an MLP 6 -> 64 -> 64 -> 1 (FP32, ReLU)
  * whose training and inference run as this library's own CUDA kernels.
  * Inputs are the pass features above; the target is log(device time per
  * amplitude in nanoseconds) = log(ms * 1e6 / 2^n). A model is trained on
@@ -200,8 +211,8 @@ int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *m
  * one.
  */
 typedef struct qcs_b200_cost_model qcs_b200_cost_model;
-#define QCS_COST_MODEL_PARAMS 4545
-#define QCS_COST_MODEL_SCALING 10
+#define QCS_COST_MODEL_PARAMS 4673
+#define QCS_COST_MODEL_SCALING 14
 
 int qcs_b200_cost_model_create(qcs_b200_cost_model **model, uint32_t seed);
 int qcs_b200_cost_model_destroy(qcs_b200_cost_model *model);
@@ -210,13 +221,13 @@ int qcs_b200_cost_model_destroy(qcs_b200_cost_model *model);
 int qcs_b200_cost_model_train(qcs_b200_cost_model *model, const float *features, const float *targets,
                               uint32_t count, uint32_t epochs, uint32_t batch, float learning_rate, float *final_loss);
 int qcs_b200_cost_model_predict(qcs_b200_cost_model *model, const float *features, uint32_t count, float *predictions);
-/* Gradient of the mean squared error w.r.t. the parameters (layout W1[64x4],
+/* Gradient of the mean squared error w.r.t. the parameters (layout W1[64x6],
    b1[64], W2[64x64], b2[64], W3[64], b3) for inputs and targets that are
    already standardised; loss (may be NULL) gets the loss. */
 int qcs_b200_cost_model_gradients(qcs_b200_cost_model *model, const float *inputs, const float *targets,
                                   uint32_t count, float *gradients, float *loss);
-/* params: QCS_COST_MODEL_PARAMS floats; scaling: input means[4], input
-   deviations[4], target mean, target deviation. */
+/* params: QCS_COST_MODEL_PARAMS floats; scaling: input means[6], input
+   deviations[6], target mean, target deviation. */
 int qcs_b200_cost_model_get_params(qcs_b200_cost_model *model, float *params, float *scaling);
 int qcs_b200_cost_model_set_params(qcs_b200_cost_model *model, const float *params, const float *scaling);
 /* The simulator keeps a pointer (the caller keeps the model alive). */
@@ -311,9 +322,9 @@ typedef struct qcs_b200_plan_summary
     uint32_t kinds[QCS_B200_PLAN_KINDS];
     uint64_t table_entries;     /* complex entries of the phase-run factor tables */
     uint32_t tensor_passes;     /* passes a complex128 register runs as tensor passes (automatic choice) */
-    uint32_t tensor_eligible;   /* passes whose stages allow a tensor pass */
+    uint32_t tensor_eligible;   /* passes whose stages allow a tensor pass of 16 x 16 stages */
     uint32_t tensor_matrices;   /* stage matrices over the tensor passes */
-    uint32_t reserved;
+    uint32_t tensor8_passes;    /* tensor passes of 8 x 8 stages (a subset of tensor_passes) */
 } qcs_b200_plan_summary;
 int qcs_b200_plan_summary_get(int num_qubits, const qcs_b200_gate *gates, uint64_t num_gates,
                               qcs_b200_plan_summary *summary);

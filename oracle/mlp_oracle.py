@@ -2,9 +2,9 @@
 
 The tests load this module to check the CUDA training kernels
 (rqs-svg_b200/csrc/cost_model.cu): it restates, in float64 numpy, the same
-MLP 4 -> 64 -> 64 -> 1 with ReLU activations, the mean squared error and its
+MLP 6 -> 64 -> 64 -> 1 with ReLU activations, the mean squared error and its
 gradient with respect to every parameter, in the parameter layout the
-library uses: W1[64x4], b1[64], W2[64x64], b2[64], W3[64], b3[1].
+library uses: W1[64x6], b1[64], W2[64x64], b2[64], W3[64], b3[1].
 
 The model has no counterpart in the reference simulator (its fusion planner
 is an addition of the B200 build); parity here is against this restatement.
@@ -12,7 +12,7 @@ is an addition of the B200 build); parity here is against this restatement.
 
 import numpy as np
 
-IN, HID = 4, 64
+IN, HID = 6, 64
 SIZES = [("W1", (HID, IN)), ("b1", (HID,)), ("W2", (HID, HID)), ("b2", (HID,)), ("W3", (1, HID)), ("b3", (1,))]
 NPARAMS = sum(int(np.prod(s)) for _, s in SIZES)
 

@@ -613,8 +613,8 @@ extern "C" int qcs_simulator_get_pass_records(qcs_simulator *sim, float *feature
         const uint32_t n = static_cast<uint32_t>(std::min<size_t>(capacity, f.size()));
         for (uint32_t i = 0; i < n; ++i)
         {
-            for (int j = 0; j < 4; ++j)
-                features[4 * i + j] = f[i].f[j];
+            for (int j = 0; j < QCS_PASS_FEATURES; ++j)
+                features[QCS_PASS_FEATURES * i + j] = f[i].f[j];
             milliseconds[i] = ms[i];
         }
         *count = n;

@@ -1,13 +1,16 @@
-// Learned cost model of fused passes: a 4 -> 64 -> 64 -> 1 FP32 MLP with
+// Learned cost model of fused passes: a 6 -> 64 -> 64 -> 1 FP32 MLP with
 // ReLU activations, trained on the GPU by the kernels below (forward,
 // backward, Adam) on pass timings the simulator records itself.
 //
-// Inputs (per pass): block width (local qubits k), arithmetic ops, light ops
-// (diagonal phases and permutations), log2 of the chunk count (capped).
-// Target: log(device time per amplitude in ns). Inputs and target are
-// standardised with the training set's mean and deviation.
+// Inputs (per pass, PassFeatures): block width (1: gates one by one on the
+// register path; 3, 4: 8 x 8 or 16 x 16 tensor stages), blocks (stages),
+// arithmetic gates, light ops (diagonal phases and permutations), the
+// target-qubit stride (log2 of the largest local qubit's stride) and log2 of
+// the chunk count (capped). Target: log(device time per amplitude in ns).
+// Inputs and target are standardised with the training set's mean and
+// deviation.
 //
-// Parameter layout (one float buffer): W1[64x4], b1[64], W2[64x64], b2[64],
+// Parameter layout (one float buffer): W1[64x6], b1[64], W2[64x64], b2[64],
 // W3[64], b3[1].
 //
 // One training step (gather a mini-batch, three layers forward, loss

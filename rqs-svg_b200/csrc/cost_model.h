@@ -11,7 +11,7 @@ namespace qcsb
 class CostModel
 {
   public:
-    static constexpr int kInputs = 4;
+    static constexpr int kInputs = 6;
     static constexpr int kHidden = 64;
     static constexpr int kParams = kHidden * kInputs + kHidden + kHidden * kHidden + kHidden + kHidden + 1;
     static constexpr int kScaling = 2 * kInputs + 2;

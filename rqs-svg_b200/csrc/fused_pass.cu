@@ -62,9 +62,10 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
 {
     typedef typename Cx<Real>::T V;
     __shared__ V scratch[64][R];
+    const int width = tb.width;   // 4: 16 x 16 matrices, 3: 8 x 8 (one thread per column)
     const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t mat = gid >> kStageBits;
-    const int col = static_cast<int>(gid & (R - 1));
+    const uint32_t mat = gid >> width;
+    const int col = static_cast<int>(gid & ((1u << width) - 1u));
     if (mat >= tb.nmats)
         return;
     int st = 0;
@@ -99,12 +100,15 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
             tidx |= 1u << pos;
         ++pos;
     }
-    // slot u of the tensor layout is slot reg(u) of the register layout
+    // slot u of the tensor layout is slot reg(u) of the register layout; for
+    // 8 x 8 stages the fourth register bit takes the value this matrix's
+    // condition bits give it (it is a group bit of the tensor layout)
+    const int pad = width == 3 && ((j0 >> S.sbits[3]) & 1) ? 1 << ((S.perm >> 6) & 3) : 0;
     auto reg = [&](int u) {
-        int r = 0;
+        int r = pad;
 #pragma unroll
         for (int b = 0; b < kStageBits; ++b)
-            if ((u >> b) & 1)
+            if (b < width && ((u >> b) & 1))
                 r |= 1 << ((S.perm >> (2 * b)) & 3);
         return r;
     };
@@ -148,6 +152,42 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
         if ((cbase & op.gcmask) != op.gcval)
             continue;
         apply_op<V>(a, op, PoolEntries<V>{p, op.moff}, j0, cbase, ss);
+    }
+    if (width == 3)
+    {
+        // B[u][nu] = M[s(nu)][u], output slot s(nu) = (nu >> 1) + 4 (nu & 1);
+        // lane 4 nu + t of fragment part holds (B[t][nu], B[t + 4][nu])
+        const int b = col >> 2, t = col & 3;
+#pragma unroll
+        for (int nu = 0; nu < 8; ++nu)
+        {
+            const V y = a[reg((nu >> 1) + 4 * (nu & 1))];
+            const double parts[3] = {y.x, y.y, y.x + y.y};
+            const int lane = nu * 4 + t;
+#pragma unroll
+            for (int part = 0; part < 3; ++part)
+            {
+                if (tb.tf32)
+                {
+                    uint32_t hi, lo;
+                    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(static_cast<float>(parts[part])));
+                    asm("cvt.rna.tf32.f32 %0, %1;"
+                        : "=r"(lo)
+                        : "f"(static_cast<float>(parts[part] - __uint_as_float(hi))));
+                    uint32_t *f = reinterpret_cast<uint32_t *>(tb.out) +
+                                  ((static_cast<size_t>(mat) * kTensor3Fragments + part) * 32 + lane) * 4;
+                    f[b] = hi;
+                    f[2 + b] = lo;
+                }
+                else
+                {
+                    Real *f = reinterpret_cast<Real *>(tb.out) +
+                              ((static_cast<size_t>(mat) * kTensor3Fragments + part) * 32 + lane) * 2;
+                    f[b] = parts[part];
+                }
+            }
+        }
+        return;
     }
     const int j = col >> 3, b = (col >> 2) & 1, t = col & 3;
     if (tb.tf32)
@@ -198,7 +238,7 @@ template <typename R>
 int launch_stage_matrices(const FPassParams &prm, const TBuildParams &tb, cudaStream_t stream)
 {
     const unsigned threads = 64;
-    const unsigned blocks = static_cast<unsigned>((static_cast<uint64_t>(tb.nmats) * (1u << kStageBits) + threads - 1) / threads);
+    const unsigned blocks = static_cast<unsigned>((static_cast<uint64_t>(tb.nmats) * (1u << tb.width) + threads - 1) / threads);
     stage_matrix_kernel<R><<<blocks, threads, 0, stream>>>(prm, tb);
     QCSB_CUDA(cudaGetLastError());
     return 1;
@@ -474,7 +514,7 @@ void schedule_stages(const std::vector<GateOp> &q, const PlannedPass &pp, const 
                 if (!ready)
                     continue;
                 const uint32_t nb = bits | need[i];
-                if (__builtin_popcount(nb) > kStageBits)
+                if (__builtin_popcount(nb) > pp.stage_width)
                     continue;
                 bits = nb;
                 ops.push_back((int)i);
@@ -734,7 +774,26 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
     for (size_t si = 0; si < stage_ops.size(); ++si)
     {
         // stage bits: the needed ones, padded with the lowest other local bits
+        // (three-bit stages: with bits no op of the stage involves first, so
+        // that the fourth bit is no condition of an 8 x 8 tensor stage)
         uint32_t bits = stage_bits[si];
+        if (pp.stage_width < kStageBits)
+        {
+            uint32_t touched = 0;
+            for (int oi : stage_ops[si])
+            {
+                const GateOp &op = q[pp.ops[oi]];
+                uint64_t pattern = op.cmask;
+                for (int i = 0; i < op.nt; ++i)
+                    pattern |= 1ull << op.tq[i];
+                for (int b = 0; b < n; ++b)
+                    if (((pattern >> b) & 1) && loc_of[b] >= 0)
+                        touched |= 1u << loc_of[b];
+            }
+            for (int l = 0; l < k && __builtin_popcount(bits) < kStageBits; ++l)
+                if (!((touched >> l) & 1))
+                    bits |= 1u << l;
+        }
         for (int l = 0; l < k && __builtin_popcount(bits) < kStageBits; ++l)
             bits |= 1u << l;
         uint8_t sbits[kStageBits];
@@ -748,6 +807,7 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
             }
         // the bits outside the stage that its ops depend on
         StageCond cond;
+        cond.dense = stage_bits[si];
         for (int oi : stage_ops[si])
         {
             const GateOp &op = q[pp.ops[oi]];
@@ -763,6 +823,8 @@ bool build_params_body(const std::vector<GateOp> &q, const PlannedPass &pp, int 
                     cond.gmask |= 1ull << b;
                 else if (!((bits >> l) & 1))
                     cond.lmask |= 1u << l;
+                else
+                    cond.touch |= 1u << l;
             }
         }
         // the scheduled stage becomes one register stage, opened at its first op
@@ -1402,6 +1464,81 @@ bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, st
            build_pieces(q, b, n, params, srcs, pieces, tables, conds);
 }
 
+// How a planned pass runs: its pieces (built by build_pieces and already
+// appended to params / pieces / conds from index `before` on) on the
+// register path or as 16 x 16 tensor stages, per piece whichever the cost
+// estimate favours (tensor mode 1) or 16 x 16 wherever allowed (2); or the
+// same gates replanned with three dense bits per stage as 8 x 8 tensor
+// stages, which then replace those pieces: when the estimate favours them
+// (1) or wherever every piece allows them (3).
+void choose_execution(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int amp_bytes, int tensor_mode,
+                      std::vector<FPassParams> &params, std::vector<PlannedPass> &pieces,
+                      std::vector<std::vector<StageCond>> &conds, std::vector<double2> *tables, PassChoice &out,
+                      size_t before)
+{
+    out = PassChoice();
+    double cost4 = 0.0;
+    for (size_t i = before; i < params.size(); ++i)
+    {
+        out.tensor.push_back(-1);
+        const double creg = register_pass_cost(params[i], amp_bytes);
+        double cost = creg;
+        if (tensor_mode == 1 || tensor_mode == 2)
+        {
+            TPassParams tp;
+            TBuildParams tb;
+            const bool ok = make_tensor_params(params[i], conds[i], amp_bytes, tp, tb);
+            const double ct = ok ? tensor_pass_cost(tp, amp_bytes) : 0.0;
+            if (ok && (tensor_mode == 2 || ct < creg))
+            {
+                out.tparams.push_back(tp);
+                out.tbuild.push_back(tb);
+                out.tensor.back() = static_cast<int>(out.tparams.size()) - 1;
+                cost = ct;
+            }
+        }
+        cost4 += cost;
+    }
+    out.cost = cost4;
+    if ((tensor_mode != 1 && tensor_mode != 3) || pp.k != kTensorLocal)
+        return;
+    PlannedPass p3 = pp;
+    p3.stage_width = 3;
+    std::vector<FPassParams> params3;
+    std::vector<PlannedPass> pieces3;
+    std::vector<std::vector<StageCond>> conds3;
+    const size_t tables_before = tables ? tables->size() : 0;
+    bool ok = build_pieces(q, p3, n, params3, nullptr, &pieces3, tables, &conds3);
+    std::vector<TPassParams> tp3(ok ? params3.size() : 0);
+    std::vector<TBuildParams> tb3(tp3.size());
+    double cost3 = 0.0;
+    for (size_t j = 0; ok && j < params3.size(); ++j)
+    {
+        ok = make_tensor_params(params3[j], conds3[j], amp_bytes, tp3[j], tb3[j], 3);
+        cost3 += ok ? tensor_pass_cost(tp3[j], amp_bytes) : 0.0;
+    }
+    if (!ok || (tensor_mode == 1 && cost3 >= cost4))
+    {
+        if (tables)
+            tables->resize(tables_before);
+        return;
+    }
+    params.resize(before);
+    pieces.resize(before);
+    conds.resize(before);
+    out = PassChoice();
+    out.cost = cost3;
+    for (size_t j = 0; j < params3.size(); ++j)
+    {
+        params.push_back(params3[j]);
+        pieces.push_back(pieces3[j]);
+        conds.push_back(std::move(conds3[j]));
+        out.tparams.push_back(tp3[j]);
+        out.tbuild.push_back(tb3[j]);
+        out.tensor.push_back(static_cast<int>(j));
+    }
+}
+
 namespace
 {
 
@@ -1483,31 +1620,31 @@ int choose_local_bits(int n, int option)
 // few instructions per amplitude; every other op runs complex multiply-adds.
 bool light_op(const GateOp &op) { return op.diag || is_x(op) || is_swap(op); }
 
-// Cost-model inputs of a pass: local qubits k, arithmetic (non-light) ops,
-// light ops, and log2 of the number of chunks (n - k) capped at
+// Cost-model inputs of a pass as it runs (PassFeatures): block width (1 on
+// the register path, 3 or 4 for 8 x 8 or 16 x 16 tensor stages), blocks
+// (stages), arithmetic (non-light) gates, light ops, the target-qubit stride
+// (log2 of the largest stride among the local qubits: the highest local
+// qubit) and log2 of the number of chunks (n - k) capped at
 // kChunkFeatureCap. The chunk count decides how well a pass fills the GPU
 // (waves of CTAs, L2 residency of small registers); past 2^16 chunks a pass
 // streams and its time per amplitude no longer depends on it, which lets
-// timings from 24-qubit registers stand for 33-qubit ones. A model is
-// trained on registers of one amplitude type.
+// timings from 24-27-qubit registers stand for 30-33-qubit ones. A model is
+// trained on registers of one amplitude type (the dtype).
 constexpr float kChunkFeatureCap = 16.0f;
 
-PassFeatures pass_features(int k, int heavy, int light, int n)
-{
-    PassFeatures f;
-    f.f[0] = static_cast<float>(k);
-    f.f[1] = static_cast<float>(heavy);
-    f.f[2] = static_cast<float>(light);
-    f.f[3] = std::min(static_cast<float>(n - k), kChunkFeatureCap);
-    return f;
-}
-
-PassFeatures pass_features(const std::vector<GateOp> &q, const PlannedPass &pp, int n)
+PassFeatures pass_features(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int width, int stages)
 {
     int light = 0;
     for (int oi : pp.ops)
         light += light_op(q[oi]) ? 1 : 0;
-    return pass_features(pp.k, (int)pp.ops.size() - light, light, n);
+    PassFeatures f;
+    f.f[0] = static_cast<float>(width);
+    f.f[1] = static_cast<float>(stages);
+    f.f[2] = static_cast<float>((int)pp.ops.size() - light);
+    f.f[3] = static_cast<float>(light);
+    f.f[4] = pp.local ? static_cast<float>(63 - __builtin_clzll(pp.local)) : 0.0f;
+    f.f[5] = std::min(static_cast<float>(n - pp.k), kChunkFeatureCap);
+    return f;
 }
 
 uint64_t fill_local(uint64_t local, int n, int k)
@@ -1519,20 +1656,24 @@ uint64_t fill_local(uint64_t local, int n, int k)
 
 // Dynamic-programming re-cut of the greedy schedule under the cost model.
 // The greedy passes, concatenated in execution order, form a valid gate
-// order; the planner chooses where to cut it into passes, and each pass's
-// number of local qubits k, to minimise the sum of predicted pass times.
-// A candidate pass [i, j) with local qubits k is feasible when the low
-// qubits plus its dense targets fit in k and it holds at most max_ops gates.
+// order; the planner chooses where to cut it into passes (each cut within
+// kLearnedShift gates of a greedy cut) and, per pass, the block width its
+// stages run with: gate by gate on the register path, or 8 x 8 or 16 x 16
+// tensor stages (the pass is scheduled with three or four dense qubits per
+// stage). Every candidate pass is built as the executor would build it, its
+// features under each width it allows go through the model in one batch,
+// and the cover of the gate order with the least predicted time wins. The
+// arithmetic of every gate is the same under any cut; only the grouping
+// changes. Passes keep the greedy plan's number of local qubits.
+constexpr int kLearnedShift = 3;
+
 std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vector<Segment> &greedy, int n,
-                                  int amp_bytes, int max_ops, CostModel &model, double *predicted_greedy,
-                                  double *predicted_learned)
+                                  int amp_bytes, int max_ops, int tensor_mode, CostModel &model,
+                                  double *predicted_greedy, double *predicted_learned)
 {
-    const int kmin = clamp_local_bits(kStageBits + 5, n);
-    const int kmax = clamp_local_bits(kMaxLocal, n);
-    const int low = std::min(kLowBits, kmin);
-    const uint64_t low_mask = (1ull << low) - 1;
     std::vector<Segment> out;
     *predicted_greedy = *predicted_learned = 0.0;
+    const double amps_ns = std::ldexp(1.0, n);
     size_t gi = 0;
     while (gi < greedy.size())
     {
@@ -1541,18 +1682,19 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
             out.push_back(greedy[gi++]);
             continue;
         }
-        std::vector<int> seq;
-        std::vector<PassFeatures> greedy_feats;
-        while (gi < greedy.size() && greedy[gi].fused)
+        const int K = greedy[gi].pass.k;
+        const int low = std::min(kLowBits, K);
+        const uint64_t low_mask = (1ull << low) - 1;
+        std::vector<int> seq, bounds{0};
+        size_t gend = gi;
+        while (gend < greedy.size() && greedy[gend].fused && greedy[gend].pass.k == K)
         {
-            seq.insert(seq.end(), greedy[gi].pass.ops.begin(), greedy[gi].pass.ops.end());
-            greedy_feats.push_back(pass_features(q, greedy[gi].pass, n));
-            ++gi;
+            seq.insert(seq.end(), greedy[gend].pass.ops.begin(), greedy[gend].pass.ops.end());
+            bounds.push_back(static_cast<int>(seq.size()));
+            ++gend;
         }
-        const int L = (int)seq.size();
+        const int L = static_cast<int>(seq.size());
         std::vector<uint64_t> dense(L);
-        std::vector<int> light_before(L + 1, 0);   // prefix counts of light ops
-        std::vector<int> entries_before(L + 1, 0); // and of gate entries
         for (int t = 0; t < L; ++t)
         {
             const GateOp &op = q[seq[t]];
@@ -1561,71 +1703,157 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
                 for (int i = 0; i < op.nt; ++i)
                     d |= 1ull << op.tq[i];
             dense[t] = d;
-            light_before[t + 1] = light_before[t] + (light_op(op) ? 1 : 0);
-            entries_before[t + 1] = entries_before[t] + op_entry_count(op);
         }
-        struct Cand
+        std::vector<int> cuts;
+        for (int b : bounds)
+            for (int d = -kLearnedShift; d <= kLearnedShift; ++d)
+                if (b + d >= 0 && b + d <= L)
+                    cuts.push_back(b + d);
+        std::sort(cuts.begin(), cuts.end());
+        cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+        const int C = static_cast<int>(cuts.size());
+
+        // candidates (ci, cj): ops [cuts[ci], cuts[cj]) in one pass, priced
+        // under each block width they allow (feature rows [row0, row1) are
+        // the pieces of one option)
+        struct Option
         {
-            int i, j, k;
-            uint64_t local;
+            int ci, cj, width, row0, row1;
         };
-        std::vector<Cand> cands;
+        std::vector<Option> opts;
         std::vector<float> feats;
-        for (int j = 1; j <= L; ++j)
+        std::vector<double2> scratch_tables;
+        auto add_rows = [&](const std::vector<PlannedPass> &pieces, const std::vector<int> &widths,
+                            const std::vector<int> &stages, int ci, int cj, int width) {
+            Option o{ci, cj, width, static_cast<int>(feats.size() / CostModel::kInputs), 0};
+            for (size_t i = 0; i < pieces.size(); ++i)
+            {
+                const PassFeatures f = pass_features(q, pieces[i], n, widths[i], stages[i]);
+                feats.insert(feats.end(), f.f, f.f + CostModel::kInputs);
+            }
+            o.row1 = static_cast<int>(feats.size() / CostModel::kInputs);
+            opts.push_back(o);
+        };
+        for (int ci = 0; ci < C; ++ci)
         {
             uint64_t d = low_mask;
-            for (int i = j - 1; i >= 0 && j - i <= max_ops; --i)
+            for (int cj = ci + 1; cj < C; ++cj)
             {
-                d |= dense[i];
-                const int need = __builtin_popcountll(d);
-                if (need > kmax || entries_before[j] - entries_before[i] > kFusedMaxEntries)
+                const int i = cuts[ci], j = cuts[cj];
+                if (j - i > max_ops)
                     break;
-                for (int k = std::max(need, kmin); k <= kmax; ++k)
+                for (int t = cuts[cj - 1]; t < j; ++t)
+                    if (t >= i)
+                        d |= dense[t];
+                if (__builtin_popcountll(d) > K)
+                    break;
+                PlannedPass cp;
+                cp.k = K;
+                cp.local = fill_local(d, n, K);
+                cp.ops.assign(seq.begin() + i, seq.begin() + j);
+                std::vector<FPassParams> params;
+                std::vector<PlannedPass> pieces;
+                std::vector<std::vector<StageCond>> conds;
+                scratch_tables.clear();
+                if (!build_pieces(q, cp, n, params, nullptr, &pieces, &scratch_tables, &conds))
+                    continue;
+                std::vector<int> widths(params.size(), 1), stages(params.size());
+                for (size_t pi = 0; pi < params.size(); ++pi)
+                    stages[pi] = params[pi].nstages;
+                add_rows(pieces, widths, stages, ci, cj, 1);
+                if (tensor_mode != 0)
                 {
-                    const int light = light_before[j] - light_before[i];
-                    const PassFeatures f = pass_features(k, j - i - light, light, n);
-                    cands.push_back({i, j, k, fill_local(d, n, k)});
-                    feats.insert(feats.end(), f.f, f.f + 4);
+                    bool ok = true;
+                    for (size_t pi = 0; pi < params.size() && ok; ++pi)
+                    {
+                        TPassParams tp;
+                        TBuildParams tb;
+                        ok = make_tensor_params(params[pi], conds[pi], amp_bytes, tp, tb);
+                    }
+                    if (ok)
+                        add_rows(pieces, std::vector<int>(params.size(), 4), stages, ci, cj, 4);
+                    PlannedPass p3 = cp;
+                    p3.stage_width = 3;
+                    std::vector<FPassParams> params3;
+                    std::vector<PlannedPass> pieces3;
+                    std::vector<std::vector<StageCond>> conds3;
+                    ok = build_pieces(q, p3, n, params3, nullptr, &pieces3, &scratch_tables, &conds3);
+                    std::vector<int> stages3(params3.size());
+                    for (size_t pi = 0; pi < params3.size() && ok; ++pi)
+                    {
+                        TPassParams tp;
+                        TBuildParams tb;
+                        ok = make_tensor_params(params3[pi], conds3[pi], amp_bytes, tp, tb, 3);
+                        stages3[pi] = params3[pi].nstages;
+                    }
+                    if (ok)
+                        add_rows(pieces3, std::vector<int>(params3.size(), 3), stages3, ci, cj, 3);
                 }
             }
         }
-        std::vector<float> pred(cands.size());
-        model.predict(feats.data(), (int)cands.size(), pred.data());
-        std::vector<float> gpred(greedy_feats.size());
-        model.predict(&greedy_feats[0].f[0], (int)greedy_feats.size(), gpred.data());
-        const double amps_ns = std::ldexp(1.0, n);
-        for (float v : gpred)
-            *predicted_greedy += std::exp(double(v)) * amps_ns;
+        const int rows = static_cast<int>(feats.size() / CostModel::kInputs);
+        std::vector<float> pred(rows);
+        if (rows > 0)
+            model.predict(feats.data(), rows, pred.data());
+        // cheapest option per candidate, then the cheapest cover
         const double inf = 1e300;
-        std::vector<double> best(L + 1, inf);
-        std::vector<int> from(L + 1, -1);
+        std::vector<double> best(C, inf);
+        std::vector<int> from(C, -1);
         best[0] = 0.0;
-        // candidates are grouped by j ascending, so best[i] is final when read
-        for (size_t c = 0; c < cands.size(); ++c)
+        std::vector<double> cost(opts.size(), 0.0);
+        for (size_t o = 0; o < opts.size(); ++o)
+            for (int r = opts[o].row0; r < opts[o].row1; ++r)
+                cost[o] += std::exp(double(pred[r])) * amps_ns;
+        // options are grouped by ci ascending, so best[ci] is final when read
+        for (size_t o = 0; o < opts.size(); ++o)
         {
-            const Cand &cd = cands[c];
-            const double cost = best[cd.i] + std::exp(double(pred[c])) * amps_ns;
-            if (cost < best[cd.j])
+            const Option &op = opts[o];
+            if (best[op.ci] >= inf)
+                continue;
+            const double c = best[op.ci] + cost[o];
+            if (c < best[op.cj])
             {
-                best[cd.j] = cost;
-                from[cd.j] = (int)c;
+                best[op.cj] = c;
+                from[op.cj] = static_cast<int>(o);
             }
         }
-        *predicted_learned += best[L];
-        std::vector<Segment> run;
-        for (int j = L; j > 0;)
+        // the greedy cut's predicted time (each pass at its cheapest width)
+        for (size_t p = 0; p + 1 < bounds.size(); ++p)
         {
-            const Cand &cd = cands[from[j]];
+            double g = inf;
+            for (size_t o = 0; o < opts.size(); ++o)
+                if (cuts[opts[o].ci] == bounds[p] && cuts[opts[o].cj] == bounds[p + 1])
+                    g = std::min(g, cost[o]);
+            *predicted_greedy += g < inf ? g : 0.0;
+        }
+        if (from[C - 1] < 0)
+        {
+            // no cover (a candidate failed to build): keep the greedy passes
+            for (size_t p = gi; p < gend; ++p)
+                out.push_back(greedy[p]);
+            gi = gend;
+            continue;
+        }
+        *predicted_learned += best[C - 1];
+        std::vector<Segment> run;
+        for (int c = C - 1; c > 0;)
+        {
+            const Option &op = opts[from[c]];
             Segment sg;
             sg.fused = true;
             sg.plain_op = -1;
-            sg.pass.k = cd.k;
-            sg.pass.local = cd.local;
-            sg.pass.ops.assign(seq.begin() + cd.i, seq.begin() + cd.j);
+            sg.width = op.width;
+            sg.pass.k = K;
+            uint64_t d = low_mask;
+            for (int t = cuts[op.ci]; t < cuts[op.cj]; ++t)
+                d |= dense[t];
+            sg.pass.local = fill_local(d, n, K);
+            sg.pass.ops.assign(seq.begin() + cuts[op.ci], seq.begin() + cuts[op.cj]);
             run.push_back(std::move(sg));
-            j = cd.i;
+            c = op.ci;
         }
         out.insert(out.end(), run.rbegin(), run.rend());
+        gi = gend;
     }
     return out;
 }
@@ -1787,8 +2015,24 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         last_plan_learned = use_learned ? 1 : 0;
         if (use_learned)
         {
-            double pg = 0.0, pl = 0.0;
-            segs = plan_learned(ops, segs, n, amp_bytes, max_ops, *model_, &pg, &pl);
+            // the learned plan of a queue is computed once (building and
+            // pricing every candidate pass takes host time) and reused
+            const uint64_t key = sig ^ (static_cast<uint64_t>(n) << 56) ^ (static_cast<uint64_t>(amp_bytes) << 48) ^
+                                 (static_cast<uint64_t>(tensor_mode_) << 44) ^ static_cast<uint64_t>(max_ops);
+            const std::vector<Segment> *cached = nullptr;
+            for (const auto &e : learned_plans_)
+                if (e.first == key)
+                    cached = &e.second;
+            if (cached != nullptr)
+            {
+                segs = *cached;
+            }
+            else
+            {
+                double pg = 0.0, pl = 0.0;
+                segs = plan_learned(ops, segs, n, amp_bytes, max_ops, tensor_mode_, *model_, &pg, &pl);
+                learned_plans_.push_back({key, segs});
+            }
         }
         if (entry->learned_ms < 0.0 || entry->greedy_ms < 0.0)
         {
@@ -1833,7 +2077,8 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         prm.tables = tables_dev;
         if (timer.enabled)
         {
-            const PassFeatures f = pass_features(ops, pieces[st], n);
+            const int width = tensor_of[st] >= 0 ? tparams[tensor_of[st]].width : 1;
+            const PassFeatures f = pass_features(ops, pieces[st], n, width, prm.nstages);
             timer.begin(stream_, KernelTimer::kFused, 2.0 * amp_bytes * std::ldexp(1.0, n), &f);
         }
         if (tensor_of[st] >= 0)
@@ -1891,31 +2136,37 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
                 add_step(-1 - (long)oi);
             continue;
         }
-        deferring = deferring || !tables_.empty();
+        // a width the learned planner chose fixes the path (where the pass
+        // allows it; else the register path)
+        int mode = tensor_mode_;
+        if (s.width == 1)
+            mode = 0;
+        else if (s.width == 4 && tensor_mode_ != 0)
+            mode = 2;
+        else if (s.width == 3 && tensor_mode_ != 0)
+            mode = 3;
+        PassChoice choice;
+        choose_execution(ops, s.pass, n, amp_bytes, mode, params, pieces, conds, &tables_, choice, before);
         for (size_t i = before; i < params.size(); ++i)
         {
-            tensor_of.push_back(-1);
-            if (tensor_mode_ != 0)
+            const int t = choice.tensor[i - before];
+            if (t >= 0)
             {
-                tparams.emplace_back();
-                tbuild.emplace_back();
-                if (make_tensor_params(params[i], conds[i], amp_bytes, tparams.back(), tbuild.back()) &&
-                    (tensor_mode_ == 2 ||
-                     tensor_pass_cost(tparams.back(), amp_bytes) < register_pass_cost(params[i], amp_bytes)))
-                {
-                    tensor_of.back() = static_cast<int>(tparams.size()) - 1;
-                }
-                else
-                {
-                    tparams.pop_back();
-                    tbuild.pop_back();
-                }
+                tparams.push_back(choice.tparams[t]);
+                tbuild.push_back(choice.tbuild[t]);
+                tensor_of.push_back(static_cast<int>(tparams.size()) - 1);
             }
-            // complex64 register passes read their entries as float2; tensor
-            // passes build their matrices from the double2 entries
-            if (c64 && tensor_of.back() < 0)
-                entries_to_float(params[i].entries, params[i].nentries);
+            else
+            {
+                tensor_of.push_back(-1);
+            }
         }
+        deferring = deferring || !tables_.empty();
+        // complex64 register passes read their entries as float2; tensor
+        // passes build their matrices from the double2 entries
+        for (size_t i = before; i < params.size(); ++i)
+            if (c64 && tensor_of[i] < 0)
+                entries_to_float(params[i].entries, params[i].nentries);
         for (size_t i = before; i < params.size(); ++i)
             add_step((long)i);
     }

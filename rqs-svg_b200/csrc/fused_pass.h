@@ -21,6 +21,8 @@ struct StageCond
 {
     uint32_t lmask = 0;   // local positions (bit l: local qubit l of the pass)
     uint64_t gmask = 0;   // physical qubits that are not local
+    uint32_t dense = 0;   // local positions of the stage bits that dense ops target
+    uint32_t touch = 0;   // local positions of the stage bits that some op's pattern involves
 };
 
 // ---------------------------------------------------------------- tensor passes
@@ -39,16 +41,22 @@ constexpr int kTensorMaxMats = 4096;   // matrices of one pass
 // 16 bytes: (b0, b1) in FP64 for complex128, (b0, b1) TF32 high parts and
 // (b0, b1) TF32 low parts for complex64; 6 KiB either way.
 constexpr int kTensorFragments = 12;
+// 8 x 8 stages (three slot bits): one k-step and one n-tile, 3 fragments
+// (1.5 KiB) per matrix; 256 rows per chunk in 16 tiles, four per warp, so up
+// to four local condition bits pick a tile's matrix.
+constexpr int kTensor3Fragments = 3;
+constexpr int kTensor3TileBits = 4;
 
 struct TStage
 {
-    uint8_t sbits[kStageBits];   // local positions of slot bits 0..3
-    uint8_t gpos[7];             // local positions of group bits 0..6 (bits 4..6 pick the tile)
+    uint8_t sbits[kStageBits];   // local positions of slot bits 0..3 (8 x 8 stages: slot bits 0..2, then the
+                                 // stage's fourth register bit)
+    uint8_t gpos[8];             // local positions of group bits (16 x 16: 0..6, 8 x 8: 0..7); bits 4.. pick the tile
     uint8_t nlc;                 // local condition bits: gpos[4 .. 4 + nlc)
     uint8_t ngc;                 // chunk condition bits: physical qubits gq[0 .. ngc)
     uint8_t gq[kTensorMaxCond];
-    uint8_t perm;                // slot bit b of the tensor layout is bit (perm >> 2b) & 3 of the register layout
-    uint8_t pad[2];
+    uint8_t perm;                // sbits[b] is bit (perm >> 2b) & 3 of the register stage's slot index
+    uint8_t pad;
     uint32_t woff;               // first matrix of the stage
 };
 static_assert(sizeof(TStage) == 28, "TStage layout");
@@ -61,6 +69,7 @@ struct TBuildParams
     int nstages;
     uint32_t nmats;
     int tf32;                    // fragments as TF32 high/low parts (complex64 passes)
+    int width;                   // slot bits of the stages: 4 (16 x 16) or 3 (8 x 8)
     double2 *out;                // nmats x kTensorFragments x 32 lanes x 16 bytes
     TStage stages[kFusedMaxStages];
 };
@@ -71,22 +80,25 @@ struct TPassParams
     const double2 *mats;
     int n;
     int from_zero;
+    int width;                   // 4: 16 x 16 stages, 3: 8 x 8 stages
     uint64_t chunks;
     uint64_t qmasks[kMaxLocal];
     uint64_t qbit[kMaxLocal];
     int nstages;
     TStage stages[kFusedMaxStages];
-    // per stage: shared-memory offsets (swizzled) of group bits 0..6 and
-    // slot bits 0..3
+    // per stage: shared-memory offsets (swizzled) of the group bits, then of
+    // the slot bits (16 x 16: 7 + 4, 8 x 8: 8 + 3)
     uint16_t swz[kFusedMaxStages][12];
 };
 
 // Tensor-pass layout of a built pass (amp_bytes 16: complex128, 8:
-// complex64): false when a stage depends on more condition bits than a
-// tensor pass handles (or k is not kTensorLocal). The matrices are built
-// from prm's entries in FP64 (complex64 passes keep them as double2).
+// complex64) with stages of `width` slot bits (4: 16 x 16, 3: 8 x 8; a
+// width-3 layout needs a pass planned with stage_width 3): false when a
+// stage depends on more condition bits than a tensor pass handles (or k is
+// not kTensorLocal). The matrices are built from prm's entries in FP64
+// (complex64 passes keep them as double2).
 bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, int amp_bytes, TPassParams &tp,
-                        TBuildParams &tb);
+                        TBuildParams &tb, int width = kStageBits);
 // Estimated time of a pass on the register path and on the tensor path, in
 // one unit (multiply-adds per amplitude at the register path's FP64 rate).
 double register_pass_cost(const FPassParams &prm, int amp_bytes);
@@ -110,6 +122,10 @@ struct PlannedPass
     std::vector<int> ops;   // indices into the queue, in execution order
     uint64_t local = 0;     // physical qubits of Q
     int k = 0;              // |Q|
+    // stage bits that dense ops may occupy: kStageBits (register stages and
+    // 16 x 16 tensor stages) or 3 (8 x 8 tensor stages; the fourth bit of
+    // each register-format stage then carries no dense op)
+    int stage_width = kStageBits;
 };
 
 struct Segment
@@ -117,6 +133,10 @@ struct Segment
     bool fused;
     int plain_op;           // when !fused
     PlannedPass pass;
+    // block width the learned planner chose for the pass: 1 the register
+    // path, 3 or 4 tensor stages of 8 x 8 or 16 x 16; -1 lets the executor's
+    // cost estimate choose
+    int width = -1;
 };
 
 // Which queued op an FOp came from, and whether its two targets were
@@ -162,6 +182,20 @@ int op_entry_count(const GateOp &op);
 bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, std::vector<FPassParams> &params,
                   std::vector<std::vector<FOpSource>> *srcs = nullptr, std::vector<PlannedPass> *pieces = nullptr,
                   std::vector<double2> *tables = nullptr, std::vector<std::vector<StageCond>> *conds = nullptr);
+// How one planned pass runs (choose_execution, fused_pass.cu): per piece an
+// index into tparams / tbuild (a tensor pass) or -1 (the register path), and
+// the estimated cost of the whole.
+struct PassChoice
+{
+    std::vector<int> tensor;
+    std::vector<TPassParams> tparams;
+    std::vector<TBuildParams> tbuild;
+    double cost = 0.0;
+};
+void choose_execution(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int amp_bytes, int tensor_mode,
+                      std::vector<FPassParams> &params, std::vector<PlannedPass> &pieces,
+                      std::vector<std::vector<StageCond>> &conds, std::vector<double2> *tables, PassChoice &out,
+                      size_t before);
 int clamp_local_bits(int k, int n);
 // Complex64 passes read their entries as float2: round count double2 entries
 // in place into the first half of the same memory.

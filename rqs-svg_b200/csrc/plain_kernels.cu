@@ -272,6 +272,23 @@ __global__ void sequential_kernel(V *state, uint64_t count)
 template <typename V>
 __global__ void set_one_kernel(V *state, uint64_t index, V value) { state[index] = value; }
 
+// a *= sqrt(target / norm), the factor formed in FP64 from the squared norm
+// the reduction left in device memory (no host round trip); a zero norm
+// leaves the state as it is.
+template <typename V>
+__global__ void rescale_kernel(V *state, uint64_t count, double target, const double *norm)
+{
+    const double nrm = *norm;
+    if (!(nrm > 0.0))
+        return;
+    const double f = sqrt(target / nrm);
+    for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (uint64_t)gridDim.x * kThreads)
+    {
+        const V a = state[i];
+        __stcs(state + i, make_cx<V>(a.x * f, a.y * f));
+    }
+}
+
 // ------------------------------------------------------------ reductions
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -670,6 +687,16 @@ int launch_init_sequential(typename Cx<R>::T *state, int n, cudaStream_t stream)
 }
 
 template <typename R>
+int launch_rescale(typename Cx<R>::T *state, int n, double target, const double *norm_dev, cudaStream_t stream)
+{
+    typedef typename Cx<R>::T V;
+    const uint64_t count = 1ull << n;
+    rescale_kernel<V><<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, count, target, norm_dev);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+template <typename R>
 int launch_set_amplitude(typename Cx<R>::T *state, uint64_t index, double re, double im, cudaStream_t stream)
 {
     typedef typename Cx<R>::T V;
@@ -790,6 +817,7 @@ int launch_narrow(const double2 *in, uint64_t count, typename Cx<R>::T *out, cud
     template int launch_init_flat<R>(Cx<R>::T *, int, cudaStream_t);                                                \
     template int launch_init_sequential<R>(Cx<R>::T *, int, cudaStream_t);                                          \
     template int launch_set_amplitude<R>(Cx<R>::T *, uint64_t, double, double, cudaStream_t);                      \
+    template int launch_rescale<R>(Cx<R>::T *, int, double, const double *, cudaStream_t);                          \
     template int launch_measure_probs<R>(const Cx<R>::T *, int, int, uint64_t, uint64_t, double2 *, double2 *,      \
                                          unsigned *, cudaStream_t);                                                 \
     template int launch_collapse<R>(Cx<R>::T *, int, int, int, cudaStream_t);                                       \

@@ -89,25 +89,33 @@ void plan_summary(int n, const qcs_b200_gate *gates, uint64_t count, qcs_b200_pl
             continue;
         }
         std::vector<FPassParams> params;
+        std::vector<PlannedPass> pieces;
         std::vector<std::vector<StageCond>> conds;
-        if (!build_pieces(queue, s.pass, n, params, nullptr, nullptr, &tables, &conds))
+        if (!build_pieces(queue, s.pass, n, params, nullptr, &pieces, &tables, &conds))
         {
             out.plain_gates += static_cast<uint32_t>(s.pass.ops.size());
             continue;
         }
         for (size_t pi = 0; pi < params.size(); ++pi)
         {
-            const FPassParams &p = params[pi];
             TPassParams tp;
             TBuildParams tb;
-            if (make_tensor_params(p, conds[pi], 16, tp, tb))
-            {
+            if (make_tensor_params(params[pi], conds[pi], 16, tp, tb))
                 ++out.tensor_eligible;
-                if (tensor_pass_cost(tp, 16) < register_pass_cost(p, 16))
-                {
-                    ++out.tensor_passes;
-                    out.tensor_matrices += tb.nmats;
-                }
+        }
+        // the executor's choice for a complex128 register (automatic mode)
+        PassChoice choice;
+        choose_execution(queue, s.pass, n, 16, 1, params, pieces, conds, &tables, choice, 0);
+        for (size_t pi = 0; pi < params.size(); ++pi)
+        {
+            const FPassParams &p = params[pi];
+            const int t = choice.tensor[pi];
+            if (t >= 0)
+            {
+                ++out.tensor_passes;
+                out.tensor_matrices += choice.tbuild[t].nmats;
+                if (choice.tparams[t].width == 3)
+                    ++out.tensor8_passes;
             }
             ++out.passes;
             out.stages += static_cast<uint32_t>(p.nstages);

@@ -113,6 +113,10 @@ template <typename R>
 int launch_init_sequential(typename Cx<R>::T *state, int n, cudaStream_t stream);
 template <typename R>
 int launch_set_amplitude(typename Cx<R>::T *state, uint64_t index, double re, double im, cudaStream_t stream);
+// Scale every amplitude by sqrt(target / *norm_dev) (norm_dev: a squared norm
+// in device memory, written earlier on the same stream).
+template <typename R>
+int launch_rescale(typename Cx<R>::T *state, int n, double target, const double *norm_dev, cudaStream_t stream);
 
 // Squared-norm sums (P0, P1) of target qubit t over the subspace where
 // (index & cmask) == cval, in one launch. partials must hold kReduceBlocks

@@ -1,6 +1,7 @@
 // Host side of the simulator: the state behind one qcs_simulator handle.
 #pragma once
 
+#include "fused_pass.h"
 #include "qcs_internal.h"
 #include "qcs_b200.h"
 
@@ -13,12 +14,15 @@ namespace qcsb
 class FusedExecutor;
 class CostModel;
 
-// Features of one fused pass, the cost model's inputs: local qubits k,
-// arithmetic ops (complex multiply-adds per amplitude), light ops (diagonal
-// phases and permutations), log2 of the chunk count (capped at 16).
+// Features of one fused pass as it runs, the cost model's inputs: block
+// width (1: the register path, gates one by one; 3 or 4: tensor stages of
+// 8 x 8 or 16 x 16 matrices), blocks (stages), arithmetic gates (complex
+// multiply-adds on every amplitude), light ops (diagonal phases and
+// permutations), target-qubit stride (log2 of the largest stride among the
+// local qubits) and log2 of the chunk count (capped at 16).
 struct PassFeatures
 {
-    float f[4];
+    float f[6];
 };
 
 // Optional per-launch timing with CUDA events on the launching stream.
@@ -174,6 +178,13 @@ class Simulator
     double2 *staging_dev_ = nullptr;
     double2 *staging_host_ = nullptr;
     uint64_t staging_count_ = 0;
+    // Squared norm the register should have (complex64 registers; -1 when
+    // unknown): 1 after |0..0>, the kept branch's weight after a measurement
+    // (the collapse does not renormalise), unchanged by gates. A flush that
+    // ran complex64 tensor passes rescales the register back to it (see
+    // flush()).
+    double norm_target_ = -1.0;
+    void restore_norm(uint64_t tensor_passes_before);
     // sampler: marginal tree, uniforms and outcomes, kept between calls and
     // grown when a call needs more (per-call stream-ordered allocations made
     // some calls stall for tenths of a second)
@@ -197,9 +208,17 @@ class FusedExecutor
         max_ops_ = max_ops;
         local_bits_ = local_bits;
     }
-    void set_cost_model(CostModel *model) { model_ = model; }
+    // a new model plans anew: its plans and the judge's times are dropped
+    void set_cost_model(CostModel *model)
+    {
+        model_ = model;
+        learned_plans_.clear();
+        judge_.clear();
+    }
     // Tensor passes (tensor_pass.cu): 0 never, 1 where the cost estimate
-    // favours them (default), 2 wherever a pass's stages allow them.
+    // favours them (default; 16 x 16 or 8 x 8 stages, whichever it favours),
+    // 2 with 16 x 16 stages wherever a pass allows them, 3 with 8 x 8 stages
+    // wherever a pass allows them.
     void set_tensor_mode(int mode) { tensor_mode_ = mode; }
 
     // Which planner ran the last flush in learned mode (1 = learned,
@@ -236,6 +255,8 @@ class FusedExecutor
     // time of a flush under each planner; once both are known the faster one
     // is used for that queue from then on.
     std::vector<std::pair<uint64_t, JudgeEntry>> judge_;
+    // learned plans by queue signature (with size, precision and options)
+    std::vector<std::pair<uint64_t, std::vector<Segment>>> learned_plans_;
     cudaEvent_t judge_a_ = nullptr, judge_b_ = nullptr;
     uint64_t pending_sig_ = 0;
     int pending_learned_ = -1;

@@ -71,16 +71,24 @@ struct Tensor<double>
         const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
     }
-    // D += A B, m16n8k8 FP64: a0 = A[g][t], a1 = A[g + 8][t], a2 = A[g][t + 4],
-    // a3 = A[g + 8][t + 4]; b0 = B[t][g], b1 = B[t + 4][g]; d0 = D[g][2t],
+    // A fragment: a0 = A[g][t], a1 = A[g + 8][t], a2 = A[g][t + 4],
+    // a3 = A[g + 8][t + 4]
+    struct AFrag
+    {
+        double a0, a1, a2, a3;
+    };
+    static __device__ __forceinline__ AFrag afrag(double a0, double a1, double a2, double a3)
+    {
+        return AFrag{a0, a1, a2, a3};
+    }
+    // D += A B, m16n8k8 FP64: b0 = B[t][g], b1 = B[t + 4][g]; d0 = D[g][2t],
     // d1 = D[g][2t + 1], d2 = D[g + 8][2t], d3 = D[g + 8][2t + 1]
-    static __device__ __forceinline__ void mma(double (&d)[4], double a0, double a1, double a2, double a3,
-                                               const Frag &b)
+    static __device__ __forceinline__ void mma(double (&d)[4], const AFrag &a, const Frag &b)
     {
         asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
             "{%0,%1,%2,%3};\n"
             : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-            : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b.x), "d"(b.y));
+            : "d"(a.a0), "d"(a.a1), "d"(a.a2), "d"(a.a3), "d"(b.x), "d"(b.y));
     }
 };
 
@@ -110,16 +118,32 @@ struct Tensor<float>
             : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
             : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
     }
-    // D += A B with A and B split into TF32 high and low parts (layout as
-    // for FP64); the small terms go first
-    static __device__ __forceinline__ void mma(float (&d)[4], float a0, float a1, float a2, float a3, const Frag &b)
+    // A fragment (layout as for FP64) split into TF32 high and low parts,
+    // once per tile: both n-tiles use it
+    struct AFrag
     {
-        const uint32_t h0 = to_tf32(a0), h1 = to_tf32(a1), h2 = to_tf32(a2), h3 = to_tf32(a3);
-        const uint32_t l0 = to_tf32(a0 - __uint_as_float(h0)), l1 = to_tf32(a1 - __uint_as_float(h1));
-        const uint32_t l2 = to_tf32(a2 - __uint_as_float(h2)), l3 = to_tf32(a3 - __uint_as_float(h3));
-        tf32mma(d, l0, l1, l2, l3, b.x, b.y);
-        tf32mma(d, h0, h1, h2, h3, b.z, b.w);
-        tf32mma(d, h0, h1, h2, h3, b.x, b.y);
+        uint32_t h0, h1, h2, h3, l0, l1, l2, l3;
+    };
+    static __device__ __forceinline__ AFrag afrag(float a0, float a1, float a2, float a3)
+    {
+        AFrag f;
+        f.h0 = to_tf32(a0);
+        f.h1 = to_tf32(a1);
+        f.h2 = to_tf32(a2);
+        f.h3 = to_tf32(a3);
+        f.l0 = to_tf32(a0 - __uint_as_float(f.h0));
+        f.l1 = to_tf32(a1 - __uint_as_float(f.h1));
+        f.l2 = to_tf32(a2 - __uint_as_float(f.h2));
+        f.l3 = to_tf32(a3 - __uint_as_float(f.h3));
+        return f;
+    }
+    // D += A B with A and B split into TF32 high and low parts; the small
+    // terms go first
+    static __device__ __forceinline__ void mma(float (&d)[4], const AFrag &a, const Frag &b)
+    {
+        tf32mma(d, a.l0, a.l1, a.l2, a.l3, b.x, b.y);
+        tf32mma(d, a.h0, a.h1, a.h2, a.h3, b.z, b.w);
+        tf32mma(d, a.h0, a.h1, a.h2, a.h3, b.x, b.y);
     }
 };
 
@@ -264,17 +288,18 @@ __global__ void __launch_bounds__(kThreads, 3) tensor_pass_kernel(const __grid_c
                 auto pos = [&](int h, int m) {
                     return base ^ (h ? hpos : 0u) ^ ((m & 1) ? sbit[2] : 0u) ^ ((m & 2) ? sbit[3] : 0u);
                 };
-                // x[h][m]: row g + 8h, input slot t + 4m
-                V x[2][4];
-                Real xs[2][4];
+                // x[h][m]: row g + 8h, input slot t + 4m; A fragments of the
+                // real parts, the imaginary parts and their sums per k-step j
+                typename TT::AFrag ar[2], ai[2], as[2];
 #pragma unroll
-                for (int h = 0; h < 2; ++h)
-#pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                    {
-                        x[h][m] = sb[pos(h, m)];
-                        xs[h][m] = x[h][m].x + x[h][m].y;
-                    }
+                for (int j = 0; j < 2; ++j)
+                {
+                    const V x00 = sb[pos(0, 2 * j)], x10 = sb[pos(1, 2 * j)];
+                    const V x01 = sb[pos(0, 2 * j + 1)], x11 = sb[pos(1, 2 * j + 1)];
+                    ar[j] = TT::afrag(x00.x, x10.x, x01.x, x11.x);
+                    ai[j] = TT::afrag(x00.y, x10.y, x01.y, x11.y);
+                    as[j] = TT::afrag(x00.x + x00.y, x10.x + x10.y, x01.x + x01.y, x11.x + x11.y);
+                }
 #pragma unroll
                 for (int i = 0; i < 2; ++i)
                 {
@@ -282,12 +307,9 @@ __global__ void __launch_bounds__(kThreads, 3) tensor_pass_kernel(const __grid_c
 #pragma unroll
                     for (int j = 0; j < 2; ++j)
                     {
-                        TT::mma(t1, x[0][2 * j].x, x[1][2 * j].x, x[0][2 * j + 1].x, x[1][2 * j + 1].x,
-                                bf[0 * 4 + j * 2 + i]);
-                        TT::mma(t2, x[0][2 * j].y, x[1][2 * j].y, x[0][2 * j + 1].y, x[1][2 * j + 1].y,
-                                bf[1 * 4 + j * 2 + i]);
-                        TT::mma(t3, xs[0][2 * j], xs[1][2 * j], xs[0][2 * j + 1], xs[1][2 * j + 1],
-                                bf[2 * 4 + j * 2 + i]);
+                        TT::mma(t1, ar[j], bf[0 * 4 + j * 2 + i]);
+                        TT::mma(t2, ai[j], bf[1 * 4 + j * 2 + i]);
+                        TT::mma(t3, as[j], bf[2 * 4 + j * 2 + i]);
                     }
                     // e = 0: row g, slot t + 8i; 1: row g, slot t + 8i + 4; 2, 3: row g + 8
 #pragma unroll
@@ -310,18 +332,184 @@ __global__ void __launch_bounds__(kThreads, 3) tensor_pass_kernel(const __grid_c
     }
 }
 
+// 8 x 8 stages (three slot bits; TPassParams::width 3). A warp takes 16
+// rows (8-amplitude groups) at a time: lane (g, t) holds rows g and g + 8 at
+// input slots t and t + 4 (one k-step), and output column nu = 2t + e of the
+// single n-tile stands for output slot t + 4e, so the lane stores to the
+// positions it loaded. Three m16n8k8 products per 16 rows (Gauss, as above):
+// 24 multiply-adds per amplitude and stage, half those of a 16 x 16 stage
+// for three quarters of its qubits. 256 rows per chunk: 16 tiles, four per
+// warp; group bits 4..7 pick the tile.
+template <typename Real>
+__global__ void __launch_bounds__(kThreads, 3) tensor3_pass_kernel(const __grid_constant__ TPassParams p)
+{
+    typedef Tensor<Real> TT;
+    typedef typename TT::V V;
+    typedef typename TT::Frag Frag;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *smem = reinterpret_cast<V *>(smem_raw);
+    V *const state = static_cast<V *>(p.state);
+    const Frag *const mats = reinterpret_cast<const Frag *>(p.mats);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+
+    uint64_t dep_tid = 0;
+    for (int i = 0; i < kTensorLocal - kStageBits; ++i)
+        if ((tid >> i) & 1)
+            dep_tid |= p.qbit[i];
+    uint64_t hb[kStageBits];
+#pragma unroll
+    for (int b = 0; b < kStageBits; ++b)
+        hb[b] = p.qbit[kTensorLocal - kStageBits + b];
+    auto chunk_base = [&](uint64_t c) -> uint64_t {
+        uint64_t x = c;
+        for (int i = 0; i < kTensorLocal; ++i)
+        {
+            const uint64_t lo = x & p.qmasks[i];
+            x = lo | ((x ^ lo) << 1);
+        }
+        return x;
+    };
+    auto elem_offset = [&](int m) -> uint64_t {
+        uint64_t off = dep_tid;
+#pragma unroll
+        for (int b = 0; b < kStageBits; ++b)
+            if ((m >> b) & 1)
+                off |= hb[b];
+        return off;
+    };
+    auto issue_load = [&](uint64_t cb, V *dst) {
+        if (p.from_zero)
+        {
+#pragma unroll
+            for (int m = 0; m < kSlots; ++m)
+            {
+                const bool one = cb == 0 && m == 0 && tid == 0;
+                dst[TT::swz(tid + m * kThreads)] = V{one ? Real(1) : Real(0), Real(0)};
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int m = 0; m < kSlots; ++m)
+                TT::cp_async(dst + TT::swz(tid + m * kThreads), state + (cb | elem_offset(m)));
+        }
+        cp_commit();
+    };
+
+    Frag bf[kTensor3Fragments];
+    int bf_st = -1;
+    uint32_t bf_v = 0;
+    auto matrix_of = [&](int st, uint64_t cb, int mt) -> uint32_t {
+        const TStage &S = p.stages[st];
+        uint32_t vc = 0;
+        for (int i = 0; i < S.ngc; ++i)
+            vc |= static_cast<uint32_t>((cb >> S.gq[i]) & 1) << i;
+        const uint32_t tile = static_cast<uint32_t>(mt | (warp << 2));
+        return (tile & ((1u << S.nlc) - 1u)) | (vc << S.nlc);
+    };
+    auto fetch = [&](int st, uint32_t v) {
+        const Frag *w = mats + (static_cast<size_t>(p.stages[st].woff + v) * kTensor3Fragments) * 32 + lane;
+#pragma unroll
+        for (int f = 0; f < kTensor3Fragments; ++f)
+            bf[f] = __ldg(w + f * 32);
+        bf_st = st;
+        bf_v = v;
+    };
+
+    uint64_t c = blockIdx.x;
+    if (c >= p.chunks)
+        return;
+    uint64_t cbase_next = chunk_base(c);
+    issue_load(cbase_next, smem);
+    if (p.nstages > 0)
+        fetch(0, matrix_of(0, cbase_next, 0));
+    int cur = 0;
+    for (; c < p.chunks; c += gridDim.x)
+    {
+        V *sb = smem + cur * kChunk;
+        const uint64_t cbase = cbase_next;
+        const uint64_t next = c + gridDim.x;
+        if (next < p.chunks)
+        {
+            cbase_next = chunk_base(next);
+            issue_load(cbase_next, smem + (cur ^ 1) * kChunk);
+            cp_wait<1>();
+        }
+        else
+        {
+            cp_wait<0>();
+        }
+        __syncthreads();
+
+        for (int st = 0; st < p.nstages; ++st)
+        {
+            const uint16_t *sw = p.swz[st];
+            uint32_t gbit[8], sbit[3];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                gbit[i] = sw[i];
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+                sbit[b] = sw[8 + b];
+            const uint32_t lane_pos = ((g & 1) ? gbit[0] : 0u) ^ ((g & 2) ? gbit[1] : 0u) ^
+                                      ((g & 4) ? gbit[2] : 0u) ^ ((t & 1) ? sbit[0] : 0u) ^ ((t & 2) ? sbit[1] : 0u);
+            const uint32_t hpos = gbit[3];
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt)
+            {
+                const uint32_t tile = static_cast<uint32_t>(mt | (warp << 2));
+                const uint32_t v = matrix_of(st, cbase, mt);
+                if (bf_st != st || bf_v != v)
+                    fetch(st, v);
+                const uint32_t base = lane_pos ^ ((tile & 1) ? gbit[4] : 0u) ^ ((tile & 2) ? gbit[5] : 0u) ^
+                                      ((tile & 4) ? gbit[6] : 0u) ^ ((tile & 8) ? gbit[7] : 0u);
+                auto pos = [&](int h, int m) { return base ^ (h ? hpos : 0u) ^ (m ? sbit[2] : 0u); };
+                const V x00 = sb[pos(0, 0)], x10 = sb[pos(1, 0)], x01 = sb[pos(0, 1)], x11 = sb[pos(1, 1)];
+                const typename TT::AFrag ar = TT::afrag(x00.x, x10.x, x01.x, x11.x);
+                const typename TT::AFrag ai = TT::afrag(x00.y, x10.y, x01.y, x11.y);
+                const typename TT::AFrag as =
+                    TT::afrag(x00.x + x00.y, x10.x + x10.y, x01.x + x01.y, x11.x + x11.y);
+                Real t1[4] = {0, 0, 0, 0}, t2[4] = {0, 0, 0, 0}, t3[4] = {0, 0, 0, 0};
+                TT::mma(t1, ar, bf[0]);
+                TT::mma(t2, ai, bf[1]);
+                TT::mma(t3, as, bf[2]);
+                // e = 0: row g, slot t; 1: row g, slot t + 4; 2, 3: row g + 8
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    sb[pos(e >> 1, e & 1)] = V{t1[e] - t2[e], t3[e] - (t1[e] + t2[e])};
+            }
+            if (st + 1 < p.nstages)
+                fetch(st + 1, matrix_of(st + 1, cbase, 0));
+            else if (next < p.chunks)
+                fetch(0, matrix_of(0, cbase_next, 0));
+            __syncthreads();
+        }
+
+#pragma unroll
+        for (int m = 0; m < kSlots; ++m)
+            __stcs(state + (cbase | elem_offset(m)), sb[TT::swz(tid + m * kThreads)]);
+        __syncthreads();
+        cur ^= 1;
+    }
+}
+
 } // namespace
 
 bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, int amp_bytes, TPassParams &tp,
-                        TBuildParams &tb)
+                        TBuildParams &tb, int width)
 {
     if (prm.k != kTensorLocal || static_cast<int>(conds.size()) != prm.nstages || prm.nstages <= 0)
+        return false;
+    if (width != 3 && width != kStageBits)
         return false;
     std::memset(&tp, 0, sizeof(tp));
     std::memset(&tb, 0, sizeof(tb));
     tp.n = prm.n;
     tp.from_zero = prm.from_zero;
     tp.chunks = prm.chunks;
+    tp.width = width;
     std::memcpy(tp.qmasks, prm.qmasks, sizeof(tp.qmasks));
     std::memcpy(tp.qbit, prm.qbit, sizeof(tp.qbit));
     tp.nstages = prm.nstages;
@@ -333,53 +521,95 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
     const bool c64 = amp_bytes == 8;
     const int mod = c64 ? 4 : 3;
     const int row_bank_bits = c64 ? 2 : 1;
+    const int tile_bits = width == 3 ? kTensor3TileBits : kTensorTileBits;
+    const int ngroup = kTensorLocal - width;   // 7 (4 rows + 3 tile bits) or 8 (4 + 4)
     uint32_t woff = 0;
     for (int s = 0; s < prm.nstages; ++s)
     {
         const FStage &FS = prm.stages[s];
         const StageCond &cond = conds[s];
-        const int nlc = __builtin_popcount(cond.lmask);
+        // register slots (0..3) that become tensor slots: all four, or for
+        // 8 x 8 stages the ones dense ops target, then untouched ones; the
+        // remaining register bit (pad) is a group bit of the tensor layout,
+        // and a condition bit when an op's pattern involves it
+        int slots[kStageBits], nslots = 0, padslot = -1;
+        auto taken = [&](int b) {
+            for (int i = 0; i < nslots; ++i)
+                if (slots[i] == b)
+                    return true;
+            return false;
+        };
+        if (width == kStageBits)
+        {
+            for (int b = 0; b < kStageBits; ++b)
+                slots[nslots++] = b;
+        }
+        else
+        {
+            if (__builtin_popcount(cond.dense) > width)
+                return false;
+            for (int b = 0; b < kStageBits; ++b)
+                if ((cond.dense >> FS.sbits[b]) & 1)
+                    slots[nslots++] = b;
+            for (int b = 0; b < kStageBits && nslots < width; ++b)
+                if (!taken(b) && !((cond.touch >> FS.sbits[b]) & 1))
+                    slots[nslots++] = b;
+            for (int b = 0; b < kStageBits && nslots < width; ++b)
+                if (!taken(b))
+                    slots[nslots++] = b;
+            for (int b = 0; b < kStageBits; ++b)
+                if (!taken(b))
+                    padslot = b;
+        }
+        const bool pad_cond = padslot >= 0 && ((cond.touch >> FS.sbits[padslot]) & 1);
+        const int nlc = __builtin_popcount(cond.lmask) + (pad_cond ? 1 : 0);
         const int ngc = __builtin_popcountll(cond.gmask);
-        if (nlc > kTensorTileBits || nlc + ngc > kTensorMaxCond)
+        if (nlc > tile_bits || nlc + ngc > kTensorMaxCond)
             return false;
         const uint32_t nm = 1u << (nlc + ngc);
         if (woff + nm > static_cast<uint32_t>(kTensorMaxMats))
             return false;
         TStage &S = tp.stages[s];
-        // slot bits 0 and 1: two stage bits of distinct residues where there are
-        int pr[kStageBits] = {0, 1, 2, 3};
+        // slot bits 0 and 1: two of distinct residues where there are
+        int order[kStageBits] = {slots[0], slots[1], slots[2], slots[3 % nslots]};
         bool found = false;
-        for (int a = 0; a < kStageBits && !found; ++a)
-            for (int b = a + 1; b < kStageBits && !found; ++b)
-                if (FS.sbits[a] % mod != FS.sbits[b] % mod)
+        for (int a = 0; a < nslots && !found; ++a)
+            for (int b = a + 1; b < nslots && !found; ++b)
+                if (FS.sbits[slots[a]] % mod != FS.sbits[slots[b]] % mod)
                 {
                     int rest = 0;
-                    pr[0] = a;
-                    pr[1] = b;
-                    for (int c2 = 0; c2 < kStageBits; ++c2)
+                    order[0] = slots[a];
+                    order[1] = slots[b];
+                    for (int c2 = 0; c2 < nslots; ++c2)
                         if (c2 != a && c2 != b)
-                            pr[2 + rest++] = c2;
+                            order[2 + rest++] = slots[c2];
                     found = true;
                 }
         uint8_t perm = 0;
-        for (int b = 0; b < kStageBits; ++b)
+        uint32_t tensor_mask = 0;
+        for (int b = 0; b < width; ++b)
         {
-            S.sbits[b] = FS.sbits[pr[b]];
-            perm |= static_cast<uint8_t>(pr[b] << (2 * b));
+            S.sbits[b] = FS.sbits[order[b]];
+            perm |= static_cast<uint8_t>(order[b] << (2 * b));
+            tensor_mask |= 1u << S.sbits[b];
+        }
+        if (padslot >= 0)
+        {
+            S.sbits[3] = FS.sbits[padslot];
+            perm |= static_cast<uint8_t>(padslot << 6);
         }
         S.perm = perm;
-        // group bits: the local condition bits first among the tile bits
-        // (4..6), the other positions outside the stage after them; the first
+        // group bits: the local condition bits first among the tile bits,
+        // the other positions outside the tensor slots after them; the first
         // row bits on the residues the slot bits leave free
-        uint32_t stage_mask = 0;
-        for (int b = 0; b < kStageBits; ++b)
-            stage_mask |= 1u << FS.sbits[b];
         std::vector<int> tile, rows, other;
         for (int l = 0; l < kTensorLocal; ++l)
             if ((cond.lmask >> l) & 1)
                 tile.push_back(l);
+        if (pad_cond)
+            tile.push_back(FS.sbits[padslot]);
         for (int l = 0; l < kTensorLocal; ++l)
-            if (!((stage_mask >> l) & 1) && !((cond.lmask >> l) & 1))
+            if (!((tensor_mask >> l) & 1) && !((cond.lmask >> l) & 1) && !(pad_cond && l == FS.sbits[padslot]))
                 other.push_back(l);
         uint32_t used = (1u << (S.sbits[0] % mod)) | (1u << (S.sbits[1] % mod));
         for (int r = 0; r < row_bank_bits; ++r)
@@ -393,11 +623,11 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
                 }
         for (int l : other)
             (rows.size() < 4 ? rows : tile).push_back(l);
-        if (rows.size() != 4 || tile.size() != 3)
+        if (rows.size() != 4 || static_cast<int>(tile.size()) != ngroup - 4)
             return false;
         for (int i = 0; i < 4; ++i)
             S.gpos[i] = static_cast<uint8_t>(rows[i]);
-        for (int i = 0; i < 3; ++i)
+        for (int i = 0; i < ngroup - 4; ++i)
             S.gpos[4 + i] = static_cast<uint8_t>(tile[i]);
         S.nlc = static_cast<uint8_t>(nlc);
         S.ngc = static_cast<uint8_t>(ngc);
@@ -408,14 +638,15 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
         S.woff = woff;
         woff += nm;
         tb.stages[s] = S;
-        for (int gb = 0; gb < 7; ++gb)
+        for (int gb = 0; gb < ngroup; ++gb)
             tp.swz[s][gb] = static_cast<uint16_t>(c64 ? swz8(1 << S.gpos[gb]) : swz16(1 << S.gpos[gb]));
-        for (int b = 0; b < kStageBits; ++b)
-            tp.swz[s][7 + b] = static_cast<uint16_t>(c64 ? swz8(1 << S.sbits[b]) : swz16(1 << S.sbits[b]));
+        for (int b = 0; b < width; ++b)
+            tp.swz[s][ngroup + b] = static_cast<uint16_t>(c64 ? swz8(1 << S.sbits[b]) : swz16(1 << S.sbits[b]));
     }
     tb.nstages = prm.nstages;
     tb.nmats = woff;
     tb.tf32 = c64 ? 1 : 0;
+    tb.width = width;
     return true;
 }
 
@@ -423,7 +654,7 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
 // FP64 rate), calibrated on B200 with the 30-qubit layered and matching
 // circuits: register passes keep the FP64 pipe about 45% busy; complex64
 // register passes take about 0.75 of the complex128 time; a complex128
-// tensor stage measured like 82 units, a complex64 one like 30.
+// 16 x 16 tensor stage measured like 82 units, a complex64 one like 30.
 double register_pass_cost(const FPassParams &prm, int amp_bytes)
 {
     double fma = 0.0;
@@ -449,6 +680,12 @@ double register_pass_cost(const FPassParams &prm, int amp_bytes)
 
 double tensor_pass_cost(const TPassParams &tp, int amp_bytes)
 {
+    // an 8 x 8 stage: half the tensor-core work of a 16 x 16 one and the
+    // same shared-memory round trip; measured on the 30-qubit layered and
+    // matching circuits: 0.63 of a 16 x 16 stage for complex128, 0.93 for
+    // complex64 (whose stages are not bound by the tensor pipe)
+    if (tp.width == 3)
+        return (amp_bytes == 8 ? 28.0 : 52.0) * tp.nstages;
     return (amp_bytes == 8 ? 30.0 : 82.0) * tp.nstages;
 }
 
@@ -464,13 +701,21 @@ int launch_tensor_pass(const TPassParams &tp, cudaStream_t stream)
     {
         QCSB_CUDA(cudaFuncSetAttribute(tensor_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem)));
+        QCSB_CUDA(cudaFuncSetAttribute(tensor3_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
         if (dev >= 0 && dev < 64)
             configured[dev] = true;
     }
     QCSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tensor_pass_kernel<R>, kThreads, smem));
+    if (tp.width == 3)
+        QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tensor3_pass_kernel<R>, kThreads, smem));
+    else
+        QCSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tensor_pass_kernel<R>, kThreads, smem));
     const uint64_t grid = std::min<uint64_t>(tp.chunks, static_cast<uint64_t>(sms) * std::max(per_sm, 1));
-    tensor_pass_kernel<R><<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(tp);
+    if (tp.width == 3)
+        tensor3_pass_kernel<R><<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(tp);
+    else
+        tensor_pass_kernel<R><<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(tp);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }

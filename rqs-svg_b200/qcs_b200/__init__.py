@@ -28,8 +28,8 @@ _P = ctypes.c_void_p
 _BN = ctypes.POINTER(bit_num_t)
 _FP = ctypes.POINTER(ctypes.c_float)
 
-COST_MODEL_PARAMS = 4545
-COST_MODEL_SCALING = 10
+COST_MODEL_PARAMS = 4673
+COST_MODEL_SCALING = 14
 
 # name -> (number of double parameters, number of targets)
 GATES = {
@@ -45,7 +45,10 @@ GATES = {
 }
 
 FUSION_PLAIN, FUSION_GREEDY, FUSION_LEARNED = 0, 1, 2
-TENSOR_NEVER, TENSOR_AUTO, TENSOR_ALWAYS = 0, 1, 2
+TENSOR_NEVER, TENSOR_AUTO, TENSOR_ALWAYS, TENSOR_ALWAYS_8X8 = 0, 1, 2, 3
+# cost-model inputs per pass (QCS_PASS_FEATURES): block width, blocks, gates,
+# light ops, target-qubit stride, log2 chunks
+PASS_FEATURES = 6
 
 
 class QCSError(RuntimeError):
@@ -104,7 +107,7 @@ class PlanSummary(ctypes.Structure):
         ("tensor_passes", ctypes.c_uint32),
         ("tensor_eligible", ctypes.c_uint32),
         ("tensor_matrices", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("tensor8_passes", ctypes.c_uint32),
     ]
 
 
@@ -445,11 +448,12 @@ class Simulator:
         self.lib.call("qcs_simulator_set_planner_options", self.h, max_gates_per_pass, local_qubits)
 
     def set_tensor_passes(self, mode: int):
-        """0: never, 1: where cheaper (default), 2: wherever a pass allows."""
+        """0: never, 1: where cheaper (default), 2: 16 x 16 stages wherever a
+        pass allows, 3: 8 x 8 stages wherever a pass allows."""
         self.lib.call("qcs_simulator_set_tensor_passes", self.h, mode)
 
     def pass_records(self, capacity: int = 1 << 20):
-        feats = np.zeros((capacity, 4), dtype=np.float32)
+        feats = np.zeros((capacity, PASS_FEATURES), dtype=np.float32)
         ms = np.zeros(capacity, dtype=np.float32)
         count = ctypes.c_uint32()
         self.lib.call("qcs_simulator_get_pass_records", self.h, _fptr(feats), _fptr(ms), capacity, ctypes.byref(count))
@@ -527,7 +531,8 @@ def plan_summary(lib: "Library", num_qubits: int, circuit) -> dict:
     kinds = {name: int(out.kinds[i]) for i, name in PLAN_KIND_NAMES.items()}
     return {"passes": out.passes, "plain_gates": out.plain_gates, "stages": out.stages, "ops": out.ops,
             "kinds": kinds, "table_entries": int(out.table_entries), "tensor_passes": out.tensor_passes,
-            "tensor_eligible": out.tensor_eligible, "tensor_matrices": out.tensor_matrices}
+            "tensor_eligible": out.tensor_eligible, "tensor_matrices": out.tensor_matrices,
+            "tensor8_passes": out.tensor8_passes}
 
 
 def fidelity(a: np.ndarray, b: np.ndarray) -> float:

@@ -1,20 +1,24 @@
 """Self-recorded pass timings and training of the learned cost model.
 
-The simulator times every fused pass it launches while kernel timing is on
-(features: local qubits k, arithmetic ops, light ops -- diagonal phases and
-permutations -- and log2 of the chunk count n - k, capped at 16, beyond which
-passes stream and the count no longer matters). `collect_pass_timings` runs
-seeded random circuits with varied pass sizes on registers of several sizes
-to gather many such samples; `train_cost_model` fits the MLP on log(ns per
+The simulator times every fused pass it launches while kernel timing is on,
+with the pass's features as it ran (block width: 1 on the register path, 3
+or 4 for 8 x 8 or 16 x 16 tensor stages; blocks, i.e. stages; arithmetic
+gates; light ops -- diagonal phases and permutations; target-qubit stride,
+log2 of the largest stride among the pass's local qubits; log2 of the chunk
+count n - k, capped at 16, beyond which passes stream and the count no
+longer matters). `collect_pass_timings` runs seeded random circuits with
+varied pass sizes and execution paths on registers of several sizes to
+gather many such samples; `train_cost_model` fits the MLP on log(ns per
 amplitude) with the library's own CUDA kernels. A model is trained on one
-amplitude type.
+amplitude type (its dtype).
 """
 
 from __future__ import annotations
 
 import numpy as np
 
-from . import FUSION_GREEDY, CostModel, Library, Simulator
+from . import (FUSION_GREEDY, PASS_FEATURES, TENSOR_ALWAYS, TENSOR_ALWAYS_8X8, TENSOR_AUTO, TENSOR_NEVER, CostModel,
+               Library, Simulator)
 from . import circuits as C
 
 _MIX = ["u3", "x", "h", "rz", "p", "ry", "swap", "rzz", "rxx", "sx"]
@@ -22,7 +26,7 @@ _MIX = ["u3", "x", "h", "rz", "p", "ry", "swap", "rzz", "rxx", "sx"]
 
 def collect_pass_timings(lib: Library, n, min_samples: int, seed: int = 1, max_rounds: int = 100000,
                          precision: int = 128):
-    """Return (features [N x 4] float32, target [N] float32 = log(ns/amp)),
+    """Return (features [N x PASS_FEATURES] float32, target [N] float32 = log(ns/amp)),
     recorded on registers of n qubits (an int or a list of sizes, which share
     the samples equally)."""
     sizes = [n] if isinstance(n, int) else list(n)
@@ -41,8 +45,10 @@ def _collect(lib: Library, n: int, min_samples: int, seed: int, max_rounds: int,
         while total < min_samples and rounds < max_rounds:
             rounds += 1
             max_ops = int(rng.integers(1, 257))
-            local = int(rng.integers(9, 12))
-            sim.set_planner_options(max_ops, local)
+            # the planner's passes keep 11 local qubits; every execution path
+            # is recorded: register, 16 x 16 and 8 x 8 tensor stages
+            sim.set_planner_options(max_ops, 11)
+            sim.set_tensor_passes(int(rng.choice([TENSOR_NEVER, TENSOR_ALWAYS, TENSOR_ALWAYS_8X8])))
             gates = list(rng.choice(_MIX, size=int(rng.integers(2, len(_MIX) + 1)), replace=False))
             circ = C.random_circuit(n, int(rng.integers(64, 400)), seed=int(rng.integers(1 << 30)),
                                     max_controls=int(rng.integers(0, 3)), gates=gates)
@@ -55,8 +61,9 @@ def _collect(lib: Library, n: int, min_samples: int, seed: int, max_rounds: int,
                 total += len(ms)
         sim.set_kernel_timing(False)
         sim.set_planner_options(0, 0)
+        sim.set_tensor_passes(TENSOR_AUTO)
     if not feats:
-        return np.zeros((0, 4), np.float32), np.zeros(0, np.float32)
+        return np.zeros((0, PASS_FEATURES), np.float32), np.zeros(0, np.float32)
     return np.concatenate(feats), np.concatenate(targets)
 
 

@@ -147,7 +147,7 @@ def test_mlp_oracle_gradient_matches_finite_differences():
 
     rng = np.random.default_rng(0)
     params = rng.normal(scale=0.3, size=mlp_oracle.NPARAMS)
-    x = rng.normal(size=(7, 4))
+    x = rng.normal(size=(7, mlp_oracle.IN))
     t = rng.normal(size=7)
     _, g = mlp_oracle.loss_and_gradients(params, x, t)
     idx = rng.choice(mlp_oracle.NPARAMS, size=60, replace=False)

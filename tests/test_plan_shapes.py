@@ -122,6 +122,10 @@ def test_tensor_pass_choice(gpu_lib):
     s = _summary(gpu_lib, 30, C.layered_u3_cz_cx_toffoli(30, 40, seed=1))
     assert s["tensor_eligible"] == s["passes"] and s["tensor_passes"] >= s["passes"] - 2
     assert s["tensor_matrices"] <= 4096 * s["tensor_passes"]
+    # with three dense qubits per stage the estimate favours 8 x 8 stages
+    # (half the tensor work per stage, a third more stages)
+    assert s["tensor8_passes"] >= 0.9 * s["tensor_passes"]
+    assert 3.0 <= s["stages"] / s["passes"] <= 4.5
     s = _summary(gpu_lib, 30, C.u3_random_matching(30, 60, seed=1))
     assert s["tensor_passes"] >= 0.8 * s["passes"]
     s = _summary(gpu_lib, 33, C.qft(33, seed=1)[0])

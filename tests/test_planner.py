@@ -31,7 +31,7 @@ def test_cost_model_gradients_match_numpy(gpu_lib):
         params, _ = model.params()
         rng = np.random.default_rng(0)
         for B in (1, 17, 256):
-            x = rng.normal(size=(B, 4)).astype(np.float32)
+            x = rng.normal(size=(B, qcs_b200.PASS_FEATURES)).astype(np.float32)
             t = rng.normal(size=B).astype(np.float32)
             g, loss = model.gradients(x, t)
             ref_loss, ref_g = mlp_oracle.loss_and_gradients(params, x, t)
@@ -44,8 +44,8 @@ def test_cost_model_gradients_match_numpy(gpu_lib):
 
 def test_cost_model_learns_a_smooth_function(gpu_lib):
     rng = np.random.default_rng(1)
-    x = rng.uniform([9, 3, 1, 16], [11, 30, 64, 16], size=(4096, 4)).astype(np.float32)
-    t = (0.05 * x[:, 2] + 0.3 * np.sin(x[:, 1] / 5.0) - 0.1 * (x[:, 0] - 10)).astype(np.float32)
+    x = rng.uniform([1, 1, 3, 1, 10, 16], [4, 8, 30, 64, 29, 16], size=(4096, 6)).astype(np.float32)
+    t = (0.05 * x[:, 3] + 0.3 * np.sin(x[:, 2] / 5.0) - 0.1 * (x[:, 0] - 2) + 0.02 * x[:, 1]).astype(np.float32)
     model = qcs_b200.CostModel(gpu_lib, seed=2)
     try:
         loss = model.train(x, t, epochs=60, batch=128, lr=3e-3)
@@ -60,8 +60,11 @@ def test_pass_timings_and_learned_plans_keep_results_exact(gpu_lib, oracle_lib):
     n = 18
     feats, target = planner.collect_pass_timings(gpu_lib, n, min_samples=1500, seed=4)
     assert len(target) >= 1500
-    assert np.all(feats[:, 0] >= 9) and np.all(feats[:, 0] <= 11)
-    assert np.all(feats[:, 3] == n - feats[:, 0])   # log2 of the chunk count
+    # every execution path was recorded: register (1), 8 x 8 (3), 16 x 16 (4)
+    assert set(np.unique(feats[:, 0]).tolist()) == {1.0, 3.0, 4.0}
+    assert np.all(feats[:, 1] >= 1)                 # stages
+    assert np.all(feats[:, 4] <= n - 1)             # highest local qubit
+    assert np.all(feats[:, 5] == n - 11)            # log2 of the chunk count
     model, loss = planner.train_cost_model(gpu_lib, feats, target, epochs=40)
     try:
         assert loss < 1.0
