@@ -118,6 +118,9 @@ def parse_args():
                     help="tensor passes (stages as dense matrices on the tensor cores): auto (default) where the "
                          "cost estimate favours them, 16x16 or 8x8 stages; always: 16x16 stages wherever allowed; "
                          "8x8: 8x8 stages wherever allowed")
+    ap.add_argument("--engine", choices=["tcgen05", "mma.sync"], default="tcgen05",
+                    help="tensor engine of complex64 16x16 stages: tcgen05 (default, where a pass allows it) or "
+                         "warp-level mma.sync")
     ap.add_argument("--precision", type=int, choices=[128, 64], default=None,
                     help="amplitude bits (default 128; 64 for hea_batch)")
     ap.add_argument("--qubits", type=int, default=30)
@@ -380,6 +383,7 @@ def main():
     sim = qcs_b200.Simulator(lib, n, seed=1234 + RANK, fusion=fusion, precision=args.precision)
     sim.set_tensor_passes({"never": qcs_b200.TENSOR_NEVER, "auto": qcs_b200.TENSOR_AUTO,
                            "always": qcs_b200.TENSOR_ALWAYS, "8x8": qcs_b200.TENSOR_ALWAYS_8X8}[args.tensor])
+    sim.set_tensor_engine(qcs_b200.ENGINE_TCGEN05 if args.engine == "tcgen05" else qcs_b200.ENGINE_MMA_SYNC)
     model, training, judge = None, None, None
     if fusion == qcs_b200.FUSION_LEARNED:
         model, training = train_planner(lib, args)
@@ -416,9 +420,12 @@ def main():
     passes = None
     if len(pass_ms):
         passes = {"per_step": len(pass_ms) / args.steps, "tensor_per_step": stats["tensor_passes"] / args.steps,
+                  "tensor8_per_step": stats["tensor8_passes"] / args.steps,
+                  "tcgen05_per_step": stats["tcgen05_passes"] / args.steps,
                   "median_ms": float(np.median(pass_ms)),
-                  "max_ms": float(np.max(pass_ms)), "arith_ops_per_pass": float(np.mean(pass_feats[:, 1])),
-                  "light_ops_per_pass": float(np.mean(pass_feats[:, 2])),
+                  "max_ms": float(np.max(pass_ms)), "stages_per_pass": float(np.mean(pass_feats[:, 1])),
+                  "gates_per_pass": float(np.mean(pass_feats[:, 2])),
+                  "light_ops_per_pass": float(np.mean(pass_feats[:, 3])),
                   "hbm_floor_ms": 2 * bpa * (1 << n) / (hbm_peak()[0] * 1e9) * 1e3}
 
     # end to end through the C ABI: host wall clock, host inputs (gate
@@ -517,6 +524,7 @@ def main():
         "data": "synthetic (seeded circuit)",
         "config": {"workload": workload, "qubits": n, "depth": depth, "gates": len(circuit),
                    "shots": SHOTS if draws_shots else 0, "fusion": args.fusion, "tensor_passes": args.tensor,
+                   "tensor_engine": args.engine,
                    "precision": args.precision,
                    "parallelism": f"replicas x{WORLD}",
                    "l2": f"state ({bpa << n >> 20} MiB) larger than L2; no flush" if (bpa << n) > (126 << 20)

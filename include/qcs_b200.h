@@ -130,6 +130,8 @@ typedef struct qcs_b200_stats
     uint64_t plain_gate_kernels;
     double algorithmic_bytes;
     uint64_t tensor_passes;       /* fused passes run as tensor passes (a subset of fused_passes) */
+    uint64_t tensor8_passes;      /* tensor passes of 8 x 8 stages (a subset of tensor_passes) */
+    uint64_t tcgen05_passes;      /* tensor passes issued as tcgen05.mma (a subset of tensor_passes) */
 } qcs_b200_stats;
 
 int qcs_simulator_get_stats(const qcs_simulator *sim, qcs_b200_stats *stats);
@@ -182,6 +184,21 @@ int qcs_simulator_set_planner_options(qcs_simulator *sim, int max_gates_per_pass
 #define QCS_TENSOR_ALWAYS_8X8 3
 int qcs_simulator_set_tensor_passes(qcs_simulator *sim, int mode);
 int qcs_simulator_get_tensor_passes(const qcs_simulator *sim, int *mode);
+
+/*
+ * Tensor engine of complex64 16 x 16 stages: 1 (the default) issues them as
+ * tcgen05.mma with TF32 operands and FP32 accumulators in tensor memory
+ * where a pass allows it (at most one local condition bit per stage); 0
+ * keeps every tensor pass on warp-level mma.sync. complex128 stages always
+ * run on the FP64 tensor cores through mma.sync (tcgen05 has no FP64 kind).
+ * A tcgen05 pass waits on its tensor cores with a time limit; past it the
+ * next call that reads results fails with a message (the register is then
+ * invalid).
+ */
+#define QCS_TENSOR_ENGINE_MMA_SYNC 0
+#define QCS_TENSOR_ENGINE_TCGEN05 1
+int qcs_simulator_set_tensor_engine(qcs_simulator *sim, int engine);
+int qcs_simulator_get_tensor_engine(const qcs_simulator *sim, int *engine);
 
 /*
  * Pass timings recorded while kernel timing is enabled: for each fused pass

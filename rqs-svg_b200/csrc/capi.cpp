@@ -598,6 +598,14 @@ extern "C" int qcs_simulator_get_tensor_passes(const qcs_simulator *sim, int *mo
 {
     return guarded([&] { write_result(mode, core(sim).tensor_mode()); });
 }
+extern "C" int qcs_simulator_set_tensor_engine(qcs_simulator *sim, int engine)
+{
+    return guarded([&] { core(sim).set_tensor_engine(engine); });
+}
+extern "C" int qcs_simulator_get_tensor_engine(const qcs_simulator *sim, int *engine)
+{
+    return guarded([&] { write_result(engine, core(sim).tensor_engine()); });
+}
 
 extern "C" int qcs_simulator_get_pass_records(qcs_simulator *sim, float *features, float *milliseconds,
                                               uint32_t capacity, uint32_t *count)

@@ -153,6 +153,35 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
             continue;
         apply_op<V>(a, op, PoolEntries<V>{p, op.moff}, j0, cbase, ss);
     }
+    if (tb.umma)
+    {
+        // the 32 x 32 real operand W of a tcgen05 pass (outputs n: Re 0-15,
+        // Im 16-31; inputs k likewise): column u of M gives
+        // W[u][o] = Mr[o][u], W[u][16 + o] = Mi[o][u],
+        // W[16 + u][o] = -Mi[o][u], W[16 + u][16 + o] = Mr[o][u]; each as a
+        // TF32 high part and the TF32 rounding of the remainder
+        unsigned char *hi_base = reinterpret_cast<unsigned char *>(tb.out) + static_cast<size_t>(mat) * kUmmaSlab;
+        unsigned char *lo_base = hi_base + static_cast<size_t>(tb.nmats) * kUmmaSlab;
+        auto put = [&](int nn, int kk, double w) {
+            const size_t off = static_cast<size_t>((nn >> 3) * 1024 + (kk >> 3) * 256 + ((kk >> 2) & 1) * 128 +
+                                                   (nn & 7) * 16 + (kk & 3) * 4);
+            uint32_t h, l;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(static_cast<float>(w)));
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(static_cast<float>(w - __uint_as_float(h))));
+            *reinterpret_cast<uint32_t *>(hi_base + off) = h;
+            *reinterpret_cast<uint32_t *>(lo_base + off) = l;
+        };
+#pragma unroll
+        for (int o = 0; o < R; ++o)
+        {
+            const V y = a[reg(o)];
+            put(o, col, y.x);
+            put(16 + o, col, y.y);
+            put(o, 16 + col, -y.y);
+            put(16 + o, 16 + col, y.x);
+        }
+        return;
+    }
     if (width == 3)
     {
         // B[u][nu] = M[s(nu)][u], output slot s(nu) = (nu >> 1) + 4 (nu & 1);
@@ -1474,7 +1503,7 @@ bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, st
 void choose_execution(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int amp_bytes, int tensor_mode,
                       std::vector<FPassParams> &params, std::vector<PlannedPass> &pieces,
                       std::vector<std::vector<StageCond>> &conds, std::vector<double2> *tables, PassChoice &out,
-                      size_t before)
+                      size_t before, int engine)
 {
     out = PassChoice();
     double cost4 = 0.0;
@@ -1487,7 +1516,11 @@ void choose_execution(const std::vector<GateOp> &q, const PlannedPass &pp, int n
         {
             TPassParams tp;
             TBuildParams tb;
-            const bool ok = make_tensor_params(params[i], conds[i], amp_bytes, tp, tb);
+            // complex64 16 x 16 stages on tcgen05 where the pass allows it
+            bool ok = engine == 1 && amp_bytes == 8 &&
+                      make_tensor_params(params[i], conds[i], amp_bytes, tp, tb, kStageBits, true);
+            if (!ok)
+                ok = make_tensor_params(params[i], conds[i], amp_bytes, tp, tb);
             const double ct = ok ? tensor_pass_cost(tp, amp_bytes) : 0.0;
             if (ok && (tensor_mode == 2 || ct < creg))
             {
@@ -1890,10 +1923,26 @@ void entries_to_float(double2 *entries, size_t count)
     }
 }
 
-FusedExecutor::FusedExecutor(cudaStream_t stream) : stream_(stream) {}
+FusedExecutor::FusedExecutor(cudaStream_t stream) : stream_(stream)
+{
+    QCSB_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&err_host_), sizeof(int), cudaHostAllocMapped));
+    *err_host_ = 0;
+    QCSB_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&err_dev_), err_host_, 0));
+}
+
+void FusedExecutor::check_device_error()
+{
+    if (err_host_ != nullptr && *const_cast<volatile int *>(err_host_) != 0)
+    {
+        *err_host_ = 0;
+        throw std::runtime_error("a tensor-memory pass gave up waiting for its tensor cores; the register is invalid");
+    }
+}
 
 FusedExecutor::~FusedExecutor()
 {
+    if (err_host_)
+        cudaFreeHost(err_host_);
     if (judge_a_)
         cudaEventDestroy(judge_a_);
     if (judge_b_)
@@ -2093,16 +2142,22 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
                 mats_dev_ = nullptr;
                 mats_cap_ = 0;
                 const size_t cap = std::max<size_t>(tb.nmats, 256);
-                QCSB_CUDA(cudaMalloc(&mats_dev_, cap * kTensorFragments * 32 * sizeof(double2)));
+                QCSB_CUDA(cudaMalloc(&mats_dev_, cap * kTensorMatrixBytes));
                 mats_cap_ = cap;
             }
             prm.state = state;
             tb.out = mats_dev_;
             tp.mats = mats_dev_;
             tp.state = state;
+            tp.err = err_dev_;
             launches += launch_stage_matrices<double>(prm, tb, stream_);
-            launches += c64 ? launch_tensor_pass<float>(tp, stream_) : launch_tensor_pass<double>(tp, stream_);
+            if (tp.umma)
+                launches += launch_tc_pass(tp, stream_);
+            else
+                launches += c64 ? launch_tensor_pass<float>(tp, stream_) : launch_tensor_pass<double>(tp, stream_);
             ++stats.tensor_passes;
+            stats.tensor8_passes += tp.width == 3 ? 1 : 0;
+            stats.tcgen05_passes += tp.umma ? 1 : 0;
         }
         else
         {
@@ -2146,7 +2201,8 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         else if (s.width == 3 && tensor_mode_ != 0)
             mode = 3;
         PassChoice choice;
-        choose_execution(ops, s.pass, n, amp_bytes, mode, params, pieces, conds, &tables_, choice, before);
+        choose_execution(ops, s.pass, n, amp_bytes, mode, params, pieces, conds, &tables_, choice, before,
+                         tensor_engine_);
         for (size_t i = before; i < params.size(); ++i)
         {
             const int t = choice.tensor[i - before];

@@ -64,15 +64,28 @@ static_assert(sizeof(TStage) == 28, "TStage layout");
 // The matrices of a pass: one per (stage, assignment of its condition bits);
 // matrix woff + v of a stage has local condition bit i equal to bit i of v
 // and chunk condition bit i equal to bit nlc + i of v.
+// complex64 16 x 16 stages on tcgen05 (tensor_pass_tc.cu): per matrix a
+// 32 x 32 real B operand [[Mr^T, Mi^T], [-Mi^T, Mr^T]] of TF32 values, in
+// the tensor cores' shared-memory layout (K-major, no swizzle: output n,
+// input k at byte (n / 8) * 1024 + (k / 8) * 256 + ((k % 8) / 4) * 128 +
+// (n % 8) * 16 + (k % 4) * 4), one 4 KiB slab per matrix for the high parts
+// and one for the low parts (all high slabs first).
+constexpr int kUmmaSlab = 4096;
+constexpr int kUmmaMaxLocalCond = 1;   // matrices of a stage side by side in N (two at most)
+
 struct TBuildParams
 {
     int nstages;
     uint32_t nmats;
     int tf32;                    // fragments as TF32 high/low parts (complex64 passes)
     int width;                   // slot bits of the stages: 4 (16 x 16) or 3 (8 x 8)
-    double2 *out;                // nmats x kTensorFragments x 32 lanes x 16 bytes
+    int umma;                    // B operands of tcgen05 passes instead of mma.sync fragments
+    double2 *out;                // nmats x kTensorFragments x 32 lanes x 16 bytes (umma: 2 x nmats slabs)
     TStage stages[kFusedMaxStages];
 };
+// bytes of the matrix buffer per matrix, either format
+constexpr size_t kTensorMatrixBytes =
+    kTensorFragments * 32 * 16 > 2 * kUmmaSlab ? kTensorFragments * 32 * 16 : 2 * kUmmaSlab;
 
 struct TPassParams
 {
@@ -81,6 +94,9 @@ struct TPassParams
     int n;
     int from_zero;
     int width;                   // 4: 16 x 16 stages, 3: 8 x 8 stages
+    int umma;                    // complex64 16 x 16 stages on tcgen05 (tensor_pass_tc.cu)
+    uint32_t nmats;              // matrices in mats (umma: the low-part slabs follow the high ones)
+    int *err;                    // set to 1 when a tcgen05 pass gives up waiting (host-mapped), or null
     uint64_t chunks;
     uint64_t qmasks[kMaxLocal];
     uint64_t qbit[kMaxLocal];
@@ -95,10 +111,15 @@ struct TPassParams
 // complex64) with stages of `width` slot bits (4: 16 x 16, 3: 8 x 8; a
 // width-3 layout needs a pass planned with stage_width 3): false when a
 // stage depends on more condition bits than a tensor pass handles (or k is
-// not kTensorLocal). The matrices are built from prm's entries in FP64
-// (complex64 passes keep them as double2).
+// not kTensorLocal). umma: the layout of a tcgen05 pass (complex64, width 4;
+// its rows are threads, so the group bits are ordered for its bank pattern
+// and a local condition bit lands on warp bit 0). The matrices are built
+// from prm's entries in FP64 (complex64 passes keep them as double2).
 bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, int amp_bytes, TPassParams &tp,
-                        TBuildParams &tb, int width = kStageBits);
+                        TBuildParams &tb, int width = kStageBits, bool umma = false);
+// A tcgen05 pass (complex64, 16 x 16 stages, at most kUmmaMaxLocalCond local
+// condition bits per stage); returns the number of kernels launched.
+int launch_tc_pass(const TPassParams &tp, cudaStream_t stream);
 // Estimated time of a pass on the register path and on the tensor path, in
 // one unit (multiply-adds per amplitude at the register path's FP64 rate).
 double register_pass_cost(const FPassParams &prm, int amp_bytes);
@@ -184,7 +205,8 @@ bool build_pieces(const std::vector<GateOp> &q, const PlannedPass &pp, int n, st
                   std::vector<double2> *tables = nullptr, std::vector<std::vector<StageCond>> *conds = nullptr);
 // How one planned pass runs (choose_execution, fused_pass.cu): per piece an
 // index into tparams / tbuild (a tensor pass) or -1 (the register path), and
-// the estimated cost of the whole.
+// the estimated cost of the whole. engine 1 runs complex64 16 x 16 stages
+// on tcgen05 where a pass allows it, 0 keeps every tensor pass on mma.sync.
 struct PassChoice
 {
     std::vector<int> tensor;
@@ -195,7 +217,7 @@ struct PassChoice
 void choose_execution(const std::vector<GateOp> &q, const PlannedPass &pp, int n, int amp_bytes, int tensor_mode,
                       std::vector<FPassParams> &params, std::vector<PlannedPass> &pieces,
                       std::vector<std::vector<StageCond>> &conds, std::vector<double2> *tables, PassChoice &out,
-                      size_t before);
+                      size_t before, int engine = 1);
 int clamp_local_bits(int k, int n);
 // Complex64 passes read their entries as float2: round count double2 entries
 // in place into the first half of the same memory.

@@ -152,6 +152,7 @@ void Simulator::allocate_memory()
     fused_ = new FusedExecutor(stream_);
     fused_->set_options(opt_max_ops_, opt_local_bits_);
     fused_->set_tensor_mode(opt_tensor_);
+    fused_->set_tensor_engine(opt_engine_);
     fused_->set_cost_model(model_);
     set_zero_state();
 }
@@ -178,6 +179,17 @@ void Simulator::set_tensor_mode(int mode)
     opt_tensor_ = mode;
     if (fused_)
         fused_->set_tensor_mode(mode);
+}
+
+void Simulator::set_tensor_engine(int engine)
+{
+    if (engine < 0 || engine > 1)
+        throw std::runtime_error(strformat("tensor engine %d is not 0 (mma.sync) or 1 (tcgen05 where possible)", engine));
+    if (allocated())
+        flush();
+    opt_engine_ = engine;
+    if (fused_)
+        fused_->set_tensor_engine(engine);
 }
 
 void Simulator::set_cost_model(CostModel *model)
@@ -435,6 +447,7 @@ void Simulator::synchronize()
     require_allocated("synchronize");
     flush();
     QCSB_CUDA(cudaStreamSynchronize(stream_));
+    fused_->check_device_error();
 }
 
 int Simulator::measure(int q)
@@ -463,6 +476,7 @@ int Simulator::measure(int q)
     double2 *h = static_cast<double2 *>(host_pinned_);
     stats.kernel_launches += QCSB_ON_STATE(launch_measure_probs, n_, t, cmask, cval, red_partials_, h, red_ticket_, stream_);
     QCSB_CUDA(cudaStreamSynchronize(stream_));
+    fused_->check_device_error();
     const double p0 = h->x, p1 = h->y;
     const double sum = p0 + p1;
     std::uniform_real_distribution<double> dist(0, sum);
@@ -601,6 +615,7 @@ void Simulator::logical_transfer(double *host, uint64_t count, bool to_host)
             const double2 *src = stage_chunk_out(begin, cnt);
             QCSB_CUDA(cudaMemcpyAsync(staging_host_, src, bytes, cudaMemcpyDeviceToHost, stream_));
             QCSB_CUDA(cudaStreamSynchronize(stream_));
+            fused_->check_device_error();
             std::memcpy(host + 2 * begin, staging_host_, bytes);
         }
         else
@@ -702,6 +717,7 @@ void Simulator::expectation_z(double *out, double *norm)
     double *h = static_cast<double *>(host_pinned_);
     QCSB_CUDA(cudaMemcpyAsync(h, zsum_result_, sizeof(double) * (n_ + 1), cudaMemcpyDeviceToHost, stream_));
     QCSB_CUDA(cudaStreamSynchronize(stream_));
+    fused_->check_device_error();
     const double total = h[0];
     for (int q = 0; q < n_; ++q)
     {
@@ -760,6 +776,7 @@ void Simulator::sample(uint32_t num_shots, uint64_t *out)
     QCSB_CUDA(cudaStreamSynchronize(stream_));   // the pinned buffer is reused below
     QCSB_CUDA(cudaMemcpyAsync(host_pinned_, bits_dev, sizeof(uint64_t) * num_shots, cudaMemcpyDeviceToHost, stream_));
     QCSB_CUDA(cudaStreamSynchronize(stream_));
+    fused_->check_device_error();
     std::memcpy(out, host_pinned_, sizeof(uint64_t) * num_shots);
 }
 

@@ -123,6 +123,8 @@ class Simulator
     void set_planner_options(int max_ops, int local_bits);
     void set_tensor_mode(int mode);
     int tensor_mode() const { return opt_tensor_; }
+    void set_tensor_engine(int engine);
+    int tensor_engine() const { return opt_engine_; }
     void set_cost_model(CostModel *model);
     FusedExecutor *fused_executor() { return fused_; }
 
@@ -165,7 +167,7 @@ class Simulator
     size_t pending_gates_ = 0;   // queued ops other than deferred collapses
     FusedExecutor *fused_ = nullptr;
     CostModel *model_ = nullptr;
-    int opt_max_ops_ = 0, opt_local_bits_ = 0, opt_tensor_ = 1;
+    int opt_max_ops_ = 0, opt_local_bits_ = 0, opt_tensor_ = 1, opt_engine_ = 1;
 
     // scratch: reduction partials and results, pinned host mirror,
     // chunk staging for logical-order transfers, sampler tree
@@ -220,6 +222,12 @@ class FusedExecutor
     // 2 with 16 x 16 stages wherever a pass allows them, 3 with 8 x 8 stages
     // wherever a pass allows them.
     void set_tensor_mode(int mode) { tensor_mode_ = mode; }
+    // 1 (default): complex64 16 x 16 stages on tcgen05 where a pass allows
+    // it; 0: every tensor pass on warp-level mma.sync
+    void set_tensor_engine(int engine) { tensor_engine_ = engine; }
+    // Throws when a tcgen05 pass gave up waiting on its tensor cores since
+    // the last check (the flag is host-mapped: no copy, read after a sync).
+    void check_device_error();
 
     // Which planner ran the last flush in learned mode (1 = learned,
     // 0 = greedy) and the device times the judge holds for that queue.
@@ -246,6 +254,9 @@ class FusedExecutor
     int max_ops_ = 0;
     int local_bits_ = 0;
     int tensor_mode_ = 1;
+    int tensor_engine_ = 1;
+    int *err_host_ = nullptr;   // host-mapped error flag of tcgen05 passes
+    int *err_dev_ = nullptr;
     // matrices of the tensor pass being run: every pass's builder writes
     // them right before the pass reads them, in stream order
     double2 *mats_dev_ = nullptr;

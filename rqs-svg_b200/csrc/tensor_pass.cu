@@ -31,11 +31,11 @@
 // gate), at the FP64 tensor rate, which on B200 equals the FMA rate, but
 // with one instruction per 1024 multiply-adds instead of 32.
 //
-// complex64: every operand is split into a TF32 high part and the TF32
-// rounding of the remainder; each product is a_lo b_hi + a_hi b_lo +
-// a_hi b_hi (the lo x lo term, 2^-22 relative, is dropped) accumulated in
-// FP32, about FP32's own accuracy, at the TF32 tensor rate (7.5x the FP64
-// rate on B200).
+// complex64: every operand is split into a TF32 high part and a TF32 low
+// part (the matrices rounded to nearest when they are built, the data by
+// masking: within 2^-21 relative); each product is a_lo b_hi + a_hi b_lo +
+// a_hi b_hi (the lo x lo term, ~2^-21 relative, is dropped) accumulated in
+// FP32, at the TF32 tensor rate (7.3x the FP64 rate on B200).
 
 #include "fused_pass.h"
 
@@ -92,13 +92,6 @@ struct Tensor<double>
     }
 };
 
-__device__ __forceinline__ uint32_t to_tf32(float x)
-{
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
-
 template <>
 struct Tensor<float>
 {
@@ -124,17 +117,21 @@ struct Tensor<float>
     {
         uint32_t h0, h1, h2, h3, l0, l1, l2, l3;
     };
+    // high part: x's top 10 mantissa bits (masked); low part: the next 11
+    // significant bits of the exact remainder (|x - hi - lo| <= 2^-21 |x|);
+    // two integer ops and one subtraction per value
+    static __device__ __forceinline__ void split(float x, uint32_t &h, uint32_t &l)
+    {
+        h = __float_as_uint(x) & 0xFFFFE000u;
+        l = __float_as_uint(x - __uint_as_float(h)) & 0xFFFFE000u;
+    }
     static __device__ __forceinline__ AFrag afrag(float a0, float a1, float a2, float a3)
     {
         AFrag f;
-        f.h0 = to_tf32(a0);
-        f.h1 = to_tf32(a1);
-        f.h2 = to_tf32(a2);
-        f.h3 = to_tf32(a3);
-        f.l0 = to_tf32(a0 - __uint_as_float(f.h0));
-        f.l1 = to_tf32(a1 - __uint_as_float(f.h1));
-        f.l2 = to_tf32(a2 - __uint_as_float(f.h2));
-        f.l3 = to_tf32(a3 - __uint_as_float(f.h3));
+        split(a0, f.h0, f.l0);
+        split(a1, f.h1, f.l1);
+        split(a2, f.h2, f.l2);
+        split(a3, f.h3, f.l3);
         return f;
     }
     // D += A B with A and B split into TF32 high and low parts; the small
@@ -498,11 +495,13 @@ __global__ void __launch_bounds__(kThreads, 3) tensor3_pass_kernel(const __grid_
 } // namespace
 
 bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &conds, int amp_bytes, TPassParams &tp,
-                        TBuildParams &tb, int width)
+                        TBuildParams &tb, int width, bool umma)
 {
     if (prm.k != kTensorLocal || static_cast<int>(conds.size()) != prm.nstages || prm.nstages <= 0)
         return false;
     if (width != 3 && width != kStageBits)
+        return false;
+    if (umma && (amp_bytes != 8 || width != kStageBits))
         return false;
     std::memset(&tp, 0, sizeof(tp));
     std::memset(&tb, 0, sizeof(tb));
@@ -518,10 +517,14 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
     // 1, group bit 0, and for 8-byte amplitudes group bit 1) sit on local
     // positions of distinct residues mod 3 (mod 4): the swizzle sends
     // position l to bank-group bit l mod 3 (mod 4).
+    // A tcgen05 pass's rows are threads: a half warp (16 rows, one slot each
+    // per load) meets distinct bank pairs when group bits 0-3 (thread bits
+    // 0-3) sit on positions of distinct residues mod 4; the slot bits are
+    // free.
     const bool c64 = amp_bytes == 8;
     const int mod = c64 ? 4 : 3;
-    const int row_bank_bits = c64 ? 2 : 1;
-    const int tile_bits = width == 3 ? kTensor3TileBits : kTensorTileBits;
+    const int row_bank_bits = umma ? 4 : c64 ? 2 : 1;
+    const int tile_bits = umma ? kUmmaMaxLocalCond : width == 3 ? kTensor3TileBits : kTensorTileBits;
     const int ngroup = kTensorLocal - width;   // 7 (4 rows + 3 tile bits) or 8 (4 + 4)
     uint32_t woff = 0;
     for (int s = 0; s < prm.nstages; ++s)
@@ -611,7 +614,7 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
         for (int l = 0; l < kTensorLocal; ++l)
             if (!((tensor_mask >> l) & 1) && !((cond.lmask >> l) & 1) && !(pad_cond && l == FS.sbits[padslot]))
                 other.push_back(l);
-        uint32_t used = (1u << (S.sbits[0] % mod)) | (1u << (S.sbits[1] % mod));
+        uint32_t used = umma ? 0u : (1u << (S.sbits[0] % mod)) | (1u << (S.sbits[1] % mod));
         for (int r = 0; r < row_bank_bits; ++r)
             for (size_t i = 0; i < other.size(); ++i)
                 if (!((used >> (other[i] % mod)) & 1))
@@ -647,6 +650,9 @@ bool make_tensor_params(const FPassParams &prm, const std::vector<StageCond> &co
     tb.nmats = woff;
     tb.tf32 = c64 ? 1 : 0;
     tb.width = width;
+    tb.umma = umma ? 1 : 0;
+    tp.umma = umma ? 1 : 0;
+    tp.nmats = woff;
     return true;
 }
 
@@ -686,6 +692,8 @@ double tensor_pass_cost(const TPassParams &tp, int amp_bytes)
     // complex64 (whose stages are not bound by the tensor pipe)
     if (tp.width == 3)
         return (amp_bytes == 8 ? 28.0 : 52.0) * tp.nstages;
+    if (tp.umma)
+        return 14.0 * tp.nstages;
     return (amp_bytes == 8 ? 30.0 : 82.0) * tp.nstages;
 }
 

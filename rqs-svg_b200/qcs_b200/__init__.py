@@ -46,6 +46,7 @@ GATES = {
 
 FUSION_PLAIN, FUSION_GREEDY, FUSION_LEARNED = 0, 1, 2
 TENSOR_NEVER, TENSOR_AUTO, TENSOR_ALWAYS, TENSOR_ALWAYS_8X8 = 0, 1, 2, 3
+ENGINE_MMA_SYNC, ENGINE_TCGEN05 = 0, 1
 # cost-model inputs per pass (QCS_PASS_FEATURES): block width, blocks, gates,
 # light ops, target-qubit stride, log2 chunks
 PASS_FEATURES = 6
@@ -64,6 +65,8 @@ class Stats(ctypes.Structure):
         ("plain_gate_kernels", ctypes.c_uint64),
         ("algorithmic_bytes", ctypes.c_double),
         ("tensor_passes", ctypes.c_uint64),
+        ("tensor8_passes", ctypes.c_uint64),
+        ("tcgen05_passes", ctypes.c_uint64),
     ]
 
 
@@ -198,6 +201,8 @@ class Library:
             "qcs_simulator_set_planner_options": [_P, ctypes.c_int, ctypes.c_int],
             "qcs_simulator_set_tensor_passes": [_P, ctypes.c_int],
             "qcs_simulator_get_tensor_passes": [_P, ctypes.POINTER(ctypes.c_int)],
+            "qcs_simulator_set_tensor_engine": [_P, ctypes.c_int],
+            "qcs_simulator_get_tensor_engine": [_P, ctypes.POINTER(ctypes.c_int)],
             "qcs_simulator_set_precision": [_P, ctypes.c_int],
             "qcs_simulator_get_precision": [_P, ctypes.POINTER(ctypes.c_int)],
             "qcs_simulator_get_pass_records": [_P, _FP, _FP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)],
@@ -446,6 +451,11 @@ class Simulator:
 
     def set_planner_options(self, max_gates_per_pass: int = 0, local_qubits: int = 0):
         self.lib.call("qcs_simulator_set_planner_options", self.h, max_gates_per_pass, local_qubits)
+
+    def set_tensor_engine(self, engine: int):
+        """1: complex64 16 x 16 stages on tcgen05 where allowed (default);
+        0: every tensor pass on warp-level mma.sync."""
+        self.lib.call("qcs_simulator_set_tensor_engine", self.h, engine)
 
     def set_tensor_passes(self, mode: int):
         """0: never, 1: where cheaper (default), 2: 16 x 16 stages wherever a

@@ -134,9 +134,10 @@ def test_tensor_mode_argument_checks(gpu_lib):
             sim.set_tensor_passes(4)
 
 
-def _run64(lib, n, circ, tensor, seed=1):
+def _run64(lib, n, circ, tensor, seed=1, engine=qcs_b200.ENGINE_TCGEN05):
     with qcs_b200.Simulator(lib, n, n, seed=seed, fusion=FUSION_GREEDY, precision=64) as sim:
         sim.set_tensor_passes(tensor)
+        sim.set_tensor_engine(engine)
         sim.run(circ)
         state = sim.statevector()
         return state, sim.clbits_string(), sim.stats()
@@ -197,3 +198,48 @@ def test_complex64_tensor_passes_keep_the_norm(gpu_lib, oracle_lib, measure, mod
     assert abs(ngot - nref) <= 1e-6 * nref, (ngot, nref)
     raw = abs(np.vdot(ref, got)) ** 2 / nref ** 2
     assert raw >= 1 - 1e-6, raw
+
+
+@pytest.mark.parametrize("n", [16, 20])
+def test_complex64_tcgen05_passes(gpu_lib, oracle_lib, n):
+    """complex64 16 x 16 stages issued as tcgen05.mma (rows in tensor memory,
+    TF32 high/low parts, FP32 accumulators in tensor memory) against the
+    complex128 oracle, and against the same passes on warp-level mma.sync:
+    fidelity >= 1 - 1e-6, amplitudes within 1e-5, as for every complex64
+    path. A pass goes to tcgen05 when each of its stages depends on at most
+    one local bit outside the stage; the other passes of a circuit stay on
+    mma.sync, so the circuits together must have run some on tcgen05."""
+    ran = 0
+    for circ in (C.layered_u3_cz_cx_toffoli(n, 8, seed=n), C.u3_random_matching(n, 8, seed=n + 1),
+                 C.random_circuit(n, 200, seed=900 + n, max_controls=2, gates=TWO_TARGET),
+                 C.qft(n, seed=3)[0]):
+        ref, _, _ = _run(oracle_lib, n, circ)
+        got, _, stats = _run64(gpu_lib, n, circ, TENSOR_ALWAYS)
+        ran += stats["tcgen05_passes"]
+        assert qcs_b200.fidelity(got, ref) >= 1 - 1e-6
+        assert np.max(np.abs(got - ref)) <= 1e-5
+        warp, _, stats0 = _run64(gpu_lib, n, circ, TENSOR_ALWAYS, engine=qcs_b200.ENGINE_MMA_SYNC)
+        assert stats0["tcgen05_passes"] == 0
+        assert qcs_b200.fidelity(got, warp) >= 1 - 1e-6
+    assert ran > 0
+
+
+def test_complex64_tcgen05_measurements_and_norm(gpu_lib, oracle_lib):
+    n = 20
+    circ = [("h", (), (q,), (), ()) for q in range(n)]
+    circ += C.u3_random_matching(n, 10, seed=4)
+    circ += [("measure", (q,), (q,), (), ()) for q in range(0, n, 4)]
+    circ += C.layered_u3_cz_cx_toffoli(n, 4, seed=8)
+    ref, rbits, _ = _run(oracle_lib, n, circ, seed=9)
+    got, gbits, stats = _run64(gpu_lib, n, circ, TENSOR_ALWAYS, seed=9)
+    assert stats["tensor_passes"] > 0
+    assert gbits == rbits
+    nref = np.vdot(ref, ref).real
+    assert abs(np.vdot(got, got).real - nref) <= 1e-6 * nref
+    assert abs(np.vdot(ref, got)) ** 2 / nref ** 2 >= 1 - 1e-6
+
+
+def test_tensor_engine_argument_checks(gpu_lib):
+    with qcs_b200.Simulator(gpu_lib, 12) as sim:
+        with pytest.raises(qcs_b200.QCSError, match="tensor engine"):
+            sim.set_tensor_engine(2)
