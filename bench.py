@@ -65,7 +65,6 @@ import qcs_b200  # noqa: E402
 from qcs_b200 import circuits as C  # noqa: E402
 
 PEAKS = REPO / "MEASURED_PEAKS.json"
-TRAFFIC_FILE = REPO / "profiles" / "fused_pass_traffic.txt"
 FALLBACK_HBM = 6650.0
 SHOTS = 4096
 
@@ -143,16 +142,29 @@ def hbm_peak():
         return FALLBACK_HBM, "fallback"
 
 
-def traffic_per_launch(n):
-    """dram read+write bytes of one fused pass from the committed ncu summary
-    (scaled by 2^n from the captured size)."""
+def traffic_per_launch(n, kernel="fused_pass_kernel"):
+    """dram read+write bytes of one pass of this kernel from the committed ncu
+    summary profiles/<kernel>_traffic.txt (complex128 bytes per amplitude,
+    scaled by 2^n from the captured size), or None."""
+    path = REPO / "profiles" / f"{kernel}_traffic.txt"
     try:
-        for line in TRAFFIC_FILE.read_text().splitlines():
+        for line in path.read_text().splitlines():
             if line.startswith("traffic_bytes_per_amplitude:"):
                 return float(line.split(":")[1]) * (1 << n)
     except Exception:
         pass
     return None
+
+
+def dominant_pass_kernel(stats):
+    """The kernel that runs most fused passes: the register pass, or the
+    tensor pass of 8x8 stages, of 16x16 stages on mma.sync, or on tcgen05."""
+    fused, tensor = stats["fused_passes"], stats["tensor_passes"]
+    if tensor * 2 < fused:
+        return "fused_pass_kernel"
+    t8, tc = stats["tensor8_passes"], stats["tcgen05_passes"]
+    t16 = tensor - t8 - tc
+    return max([(t8, "tensor3_pass_kernel"), (tc, "tc_pass_kernel"), (t16, "tensor_pass_kernel")])[1]
 
 
 class Clocks:
@@ -486,13 +498,17 @@ def main():
 
     peak, peak_kind = hbm_peak()
     if fusion != qcs_b200.FUSION_PLAIN and ktimes["fused_launches"]:
+        # every fused pass (register or tensor) reads and writes the register
+        # once; the timings cover all of them, the name says which kernel runs
+        # most of them
         launches, ms, by = ktimes["fused_launches"], ktimes["fused_ms"], ktimes["fused_bytes"]
-        kernel = "fused_pass_kernel"
+        kernel = dominant_pass_kernel(stats)
     else:
         launches, ms, by = ktimes["plain_launches"], ktimes["plain_ms"], ktimes["plain_bytes"]
         kernel = "gate_plain_kernel"
     achieved = (by / launches) / (ms / launches * 1e-3) / 1e9 if launches else 0.0
-    traffic = traffic_per_launch(n) * bpa / 16 if kernel == "fused_pass_kernel" and traffic_per_launch(n) else None
+    tpl = traffic_per_launch(n, kernel) if kernel != "gate_plain_kernel" else None
+    traffic = tpl * bpa / 16 if tpl else None
     roofline = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": f"{peak_kind} (copy, MEASURED_PEAKS hbm_gbs)" if peak_kind == "measured" else "fallback",
                 "frac_of_8tbs": achieved / 8000.0, "traffic": traffic,
