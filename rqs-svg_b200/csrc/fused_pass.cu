@@ -1506,6 +1506,11 @@ void choose_execution(const std::vector<GateOp> &q, const PlannedPass &pp, int n
                       size_t before, int engine)
 {
     out = PassChoice();
+    // automatic mode: registers below kTensorMinQubits fit in L2 and their
+    // passes are bound by launch latency, where a tensor pass's extra launch
+    // (the matrix build) and second planning cost more than they save
+    if (tensor_mode == 1 && n < kTensorMinQubits)
+        tensor_mode = 0;
     double cost4 = 0.0;
     for (size_t i = before; i < params.size(); ++i)
     {
@@ -1699,6 +1704,10 @@ uint64_t fill_local(uint64_t local, int n, int k)
 // arithmetic of every gate is the same under any cut; only the grouping
 // changes. Passes keep the greedy plan's number of local qubits.
 constexpr int kLearnedShift = 3;
+// relative margin by which the model must predict a block width other than
+// the executor's own choice to be faster before the planner takes it (the
+// model's median error on its training timings is about 6%)
+constexpr double kLearnedMargin = 0.10;
 
 std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vector<Segment> &greedy, int n,
                                   int amp_bytes, int max_ops, int tensor_mode, CostModel &model,
@@ -1707,6 +1716,7 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
     std::vector<Segment> out;
     *predicted_greedy = *predicted_learned = 0.0;
     const double amps_ns = std::ldexp(1.0, n);
+    const bool tensor_ok = tensor_mode != 0 && !(tensor_mode == 1 && n < kTensorMinQubits);
     size_t gi = 0;
     while (gi < greedy.size())
     {
@@ -1752,13 +1762,14 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
         struct Option
         {
             int ci, cj, width, row0, row1;
+            double factor;   // 1 for the executor's own choice, 1 + kLearnedMargin for the others
         };
         std::vector<Option> opts;
         std::vector<float> feats;
         std::vector<double2> scratch_tables;
         auto add_rows = [&](const std::vector<PlannedPass> &pieces, const std::vector<int> &widths,
-                            const std::vector<int> &stages, int ci, int cj, int width) {
-            Option o{ci, cj, width, static_cast<int>(feats.size() / CostModel::kInputs), 0};
+                            const std::vector<int> &stages, int ci, int cj, int width, double factor) {
+            Option o{ci, cj, width, static_cast<int>(feats.size() / CostModel::kInputs), 0, factor};
             for (size_t i = 0; i < pieces.size(); ++i)
             {
                 const PassFeatures f = pass_features(q, pieces[i], n, widths[i], stages[i]);
@@ -1791,37 +1802,58 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
                 if (!build_pieces(q, cp, n, params, nullptr, &pieces, &scratch_tables, &conds))
                     continue;
                 std::vector<int> widths(params.size(), 1), stages(params.size());
+                double creg = 0.0, c16 = 0.0, c8 = 0.0;
                 for (size_t pi = 0; pi < params.size(); ++pi)
-                    stages[pi] = params[pi].nstages;
-                add_rows(pieces, widths, stages, ci, cj, 1);
-                if (tensor_mode != 0)
                 {
-                    bool ok = true;
-                    for (size_t pi = 0; pi < params.size() && ok; ++pi)
+                    stages[pi] = params[pi].nstages;
+                    creg += register_pass_cost(params[pi], amp_bytes);
+                }
+                bool ok16 = false, ok8 = false;
+                std::vector<PlannedPass> pieces3;
+                std::vector<int> stages3;
+                if (tensor_ok)
+                {
+                    ok16 = true;
+                    for (size_t pi = 0; pi < params.size() && ok16; ++pi)
                     {
                         TPassParams tp;
                         TBuildParams tb;
-                        ok = make_tensor_params(params[pi], conds[pi], amp_bytes, tp, tb);
+                        ok16 = make_tensor_params(params[pi], conds[pi], amp_bytes, tp, tb);
+                        c16 += ok16 ? tensor_pass_cost(tp, amp_bytes) : 0.0;
                     }
-                    if (ok)
-                        add_rows(pieces, std::vector<int>(params.size(), 4), stages, ci, cj, 4);
                     PlannedPass p3 = cp;
                     p3.stage_width = 3;
                     std::vector<FPassParams> params3;
-                    std::vector<PlannedPass> pieces3;
                     std::vector<std::vector<StageCond>> conds3;
-                    ok = build_pieces(q, p3, n, params3, nullptr, &pieces3, &scratch_tables, &conds3);
-                    std::vector<int> stages3(params3.size());
-                    for (size_t pi = 0; pi < params3.size() && ok; ++pi)
+                    ok8 = build_pieces(q, p3, n, params3, nullptr, &pieces3, &scratch_tables, &conds3);
+                    stages3.resize(params3.size());
+                    for (size_t pi = 0; pi < params3.size() && ok8; ++pi)
                     {
                         TPassParams tp;
                         TBuildParams tb;
-                        ok = make_tensor_params(params3[pi], conds3[pi], amp_bytes, tp, tb, 3);
+                        ok8 = make_tensor_params(params3[pi], conds3[pi], amp_bytes, tp, tb, 3);
                         stages3[pi] = params3[pi].nstages;
+                        c8 += ok8 ? tensor_pass_cost(tp, amp_bytes) : 0.0;
                     }
-                    if (ok)
-                        add_rows(pieces3, std::vector<int>(params3.size(), 3), stages3, ci, cj, 3);
                 }
+                // the executor's own choice for this pass (its cost estimate);
+                // the model must predict the others faster by more than its
+                // error to take them
+                int own = 1;
+                double best = creg;
+                if (ok16 && c16 < best)
+                {
+                    own = 4;
+                    best = c16;
+                }
+                if (ok8 && c8 < best)
+                    own = 3;
+                const double other = 1.0 + kLearnedMargin;
+                add_rows(pieces, widths, stages, ci, cj, 1, own == 1 ? 1.0 : other);
+                if (ok16)
+                    add_rows(pieces, std::vector<int>(params.size(), 4), stages, ci, cj, 4, own == 4 ? 1.0 : other);
+                if (ok8)
+                    add_rows(pieces3, std::vector<int>(pieces3.size(), 3), stages3, ci, cj, 3, own == 3 ? 1.0 : other);
             }
         }
         const int rows = static_cast<int>(feats.size() / CostModel::kInputs);
@@ -1835,8 +1867,11 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
         best[0] = 0.0;
         std::vector<double> cost(opts.size(), 0.0);
         for (size_t o = 0; o < opts.size(); ++o)
+        {
             for (int r = opts[o].row0; r < opts[o].row1; ++r)
                 cost[o] += std::exp(double(pred[r])) * amps_ns;
+            cost[o] *= opts[o].factor;
+        }
         // options are grouped by ci ascending, so best[ci] is final when read
         for (size_t o = 0; o < opts.size(); ++o)
         {

@@ -33,6 +33,7 @@ struct StageCond
 // the GPU from the pass's ops (stage_matrix_kernel) and applied to every
 // 16-amplitude group of the stage by warp-level MMAs.
 constexpr int kTensorLocal = 11;       // local qubits of a tensor pass (2^11-amplitude chunks)
+constexpr int kTensorMinQubits = 24;   // automatic mode: smaller registers stay on the register path
 constexpr int kTensorTileBits = 3;     // group bits that pick a warp's tiles: local condition bits go there
 constexpr int kTensorMaxCond = 8;      // condition bits of a stage: at most 2^8 matrices
 constexpr int kTensorMaxMats = 4096;   // matrices of one pass

@@ -6,9 +6,9 @@ or 4 for 8 x 8 or 16 x 16 tensor stages; blocks, i.e. stages; arithmetic
 gates; light ops -- diagonal phases and permutations; target-qubit stride,
 log2 of the largest stride among the pass's local qubits; log2 of the chunk
 count n - k, capped at 16, beyond which passes stream and the count no
-longer matters). `collect_pass_timings` runs seeded random circuits with
-varied pass sizes and execution paths on registers of several sizes to
-gather many such samples; `train_cost_model` fits the MLP on log(ns per
+longer matters). `collect_pass_timings` runs seeded circuits (layered
+families and random mixes) with varied pass sizes and execution paths on
+registers of several sizes to gather many such samples; `train_cost_model` fits the MLP on log(ns per
 amplitude) with the library's own CUDA kernels. A model is trained on one
 amplitude type (its dtype).
 """
@@ -49,9 +49,18 @@ def _collect(lib: Library, n: int, min_samples: int, seed: int, max_rounds: int,
             # is recorded: register, 16 x 16 and 8 x 8 tensor stages
             sim.set_planner_options(max_ops, 11)
             sim.set_tensor_passes(int(rng.choice([TENSOR_NEVER, TENSOR_ALWAYS, TENSOR_ALWAYS_8X8])))
-            gates = list(rng.choice(_MIX, size=int(rng.integers(2, len(_MIX) + 1)), replace=False))
-            circ = C.random_circuit(n, int(rng.integers(64, 400)), seed=int(rng.integers(1 << 30)),
-                                    max_controls=int(rng.integers(0, 3)), gates=gates)
+            # half the rounds replay layered families (one-qubit layers with
+            # CZ / CX / Toffoli or random matchings), the others random mixes
+            cseed = int(rng.integers(1 << 30))
+            family = int(rng.integers(0, 4))
+            if family == 0:
+                circ = C.layered_u3_cz_cx_toffoli(n, int(rng.integers(2, 13)), seed=cseed)
+            elif family == 1:
+                circ = C.u3_random_matching(n, int(rng.integers(2, 13)), seed=cseed)
+            else:
+                gates = list(rng.choice(_MIX, size=int(rng.integers(2, len(_MIX) + 1)), replace=False))
+                circ = C.random_circuit(n, int(rng.integers(64, 400)), seed=cseed,
+                                        max_controls=int(rng.integers(0, 3)), gates=gates)
             sim.run(circ)
             sim.synchronize()
             f, ms = sim.pass_records()
