@@ -49,9 +49,9 @@ namespace
 
 constexpr int kThreads = 1 << (kTensorLocal - kStageBits);   // 128: 4 warps, two 16-group tiles each
 // chunk buffers of a tensor pass's CTA: 2 (double-buffered: the next chunk
-// streams in during this one's stages; three CTAs per SM) or 1 (four CTAs
-// per SM at 128 registers; measured 5.5-5.8% faster on the 30-qubit
-// circuits with 8 x 8 stages)
+// streams in during this one's stages; three CTAs per SM) or 1 (more CTAs
+// per SM instead: four for 16 x 16 stages at 128 registers, measured 5.5-5.8%
+// faster on the 30-qubit circuits; six or eight for 8 x 8 stages, below)
 constexpr int kTensor3Buffers = 1;
 constexpr int kTensor4Buffers = 1;
 constexpr int kSlots = 1 << kStageBits;
@@ -347,8 +347,16 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor_pass_kerne
 // 24 multiply-adds per amplitude and stage, half those of a 16 x 16 stage
 // for three quarters of its qubits. 256 rows per chunk: 16 tiles, four per
 // warp; group bits 4..7 pick the tile.
+// CTAs per SM of the single-buffered 8 x 8 pass: six for complex128 (80
+// registers; 6 x 32 KiB of chunk), eight for complex64 (64 registers); each
+// step from four measured faster (30-qubit layered and matching complex128:
+// 0.6998 -> 0.6725 -> 0.6551 s and 1.2803 -> 1.2310 -> 1.1979 s at 4, 5, 6)
+template <typename Real>
+constexpr int tensor3_ctas_per_sm() { return sizeof(Real) == 8 ? 6 : 8; }
+
 template <typename Real, int NBUF>
-__global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor3_pass_kernel(const __grid_constant__ TPassParams p)
+__global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real>() : 3)
+    tensor3_pass_kernel(const __grid_constant__ TPassParams p)
 {
     typedef Tensor<Real> TT;
     typedef typename TT::V V;
