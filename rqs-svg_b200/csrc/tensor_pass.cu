@@ -154,8 +154,12 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// CTAs per SM of the single-buffered 16 x 16 pass
+template <typename Real>
+constexpr int tensor_ctas_per_sm() { return sizeof(Real) == 8 ? 5 : 5; }
+
 template <typename Real, int NBUF>
-__global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor_pass_kernel(const __grid_constant__ TPassParams p)
+__global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor_ctas_per_sm<Real>() : 3) tensor_pass_kernel(const __grid_constant__ TPassParams p)
 {
     typedef Tensor<Real> TT;
     typedef typename TT::V V;
@@ -216,12 +220,9 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor_pass_kerne
     };
 
     // B fragments of one stage matrix: (Mr, Mi, Mr + Mi) x k-step j x
-    // n-tile i. The warp loads the next stage's fragments (or the next
-    // chunk's first stage's) before the barrier that ends a stage, so that
-    // their latency overlaps the wait.
-    Frag bf[kTensorFragments];
-    int bf_st = -1;
-    uint32_t bf_v = 0;
+    // n-tile i, read right before each product (from L1: every tile of a
+    // stage with the same condition bits reads the same 6 KiB); holding all
+    // 12 in registers would cost 48 registers and two CTAs per SM
     auto matrix_of = [&](int st, uint64_t cb, int mt) -> uint32_t {
         const TStage &S = p.stages[st];
         uint32_t vc = 0;
@@ -230,22 +231,12 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor_pass_kerne
         const uint32_t tile = static_cast<uint32_t>(mt | (warp << 1));
         return (tile & ((1u << S.nlc) - 1u)) | (vc << S.nlc);
     };
-    auto fetch = [&](int st, uint32_t v) {
-        const Frag *w = mats + (static_cast<size_t>(p.stages[st].woff + v) * kTensorFragments) * 32 + lane;
-#pragma unroll
-        for (int f = 0; f < kTensorFragments; ++f)
-            bf[f] = __ldg(w + f * 32);
-        bf_st = st;
-        bf_v = v;
-    };
 
     uint64_t c = blockIdx.x;
     if (c >= p.chunks)
         return;
     uint64_t cbase_next = chunk_base(c);
     issue_load(cbase_next, smem);
-    if (p.nstages > 0)
-        fetch(0, matrix_of(0, cbase_next, 0));
     int cur = 0;
     for (; c < p.chunks; c += gridDim.x)
     {
@@ -268,6 +259,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor_pass_kerne
 
         for (int st = 0; st < p.nstages; ++st)
         {
+            const TStage &S = p.stages[st];
             // swizzled offsets of the group and slot bits (the swizzle is
             // linear over GF(2): positions combine by XOR)
             const uint16_t *sw = p.swz[st];
@@ -286,8 +278,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor_pass_kerne
             {
                 const uint32_t tile = static_cast<uint32_t>(mt | (warp << 1));
                 const uint32_t v = matrix_of(st, cbase, mt);
-                if (bf_st != st || bf_v != v)
-                    fetch(st, v);
+                const Frag *w = mats + (static_cast<size_t>(S.woff + v) * kTensorFragments) * 32 + lane;
                 const uint32_t base = lane_pos ^ ((tile & 1) ? gbit[4] : 0u) ^ ((tile & 2) ? gbit[5] : 0u) ^
                                       ((tile & 4) ? gbit[6] : 0u);
                 auto pos = [&](int h, int m) {
@@ -312,9 +303,9 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor_pass_kerne
 #pragma unroll
                     for (int j = 0; j < 2; ++j)
                     {
-                        TT::mma(t1, ar[j], bf[0 * 4 + j * 2 + i]);
-                        TT::mma(t2, ai[j], bf[1 * 4 + j * 2 + i]);
-                        TT::mma(t3, as[j], bf[2 * 4 + j * 2 + i]);
+                        TT::mma(t1, ar[j], __ldg(w + (0 * 4 + j * 2 + i) * 32));
+                        TT::mma(t2, ai[j], __ldg(w + (1 * 4 + j * 2 + i) * 32));
+                        TT::mma(t3, as[j], __ldg(w + (2 * 4 + j * 2 + i) * 32));
                     }
                     // e = 0: row g, slot t + 8i; 1: row g, slot t + 8i + 4; 2, 3: row g + 8
 #pragma unroll
@@ -322,10 +313,6 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? 4 : 3) tensor_pass_kerne
                         sb[pos(e >> 1, 2 * i + (e & 1))] = V{t1[e] - t2[e], t3[e] - (t1[e] + t2[e])};
                 }
             }
-            if (st + 1 < p.nstages)
-                fetch(st + 1, matrix_of(st + 1, cbase, 0));
-            else if (next < p.chunks)
-                fetch(0, matrix_of(0, cbase_next, 0));
             __syncthreads();
         }
 
