@@ -132,6 +132,8 @@ typedef struct qcs_b200_stats
     uint64_t tensor_passes;       /* fused passes run as tensor passes (a subset of fused_passes) */
     uint64_t tensor8_passes;      /* tensor passes of 8 x 8 stages (a subset of tensor_passes) */
     uint64_t tcgen05_passes;      /* tensor passes issued as tcgen05.mma (a subset of tensor_passes) */
+    uint64_t replayed_flushes;    /* flushes launched from a kept plan: a queue seen before (the same gates,
+                                     matrices bit for bit, e.g. a circuit re-run per sample), not planned again */
 } qcs_b200_stats;
 
 int qcs_simulator_get_stats(const qcs_simulator *sim, qcs_b200_stats *stats);

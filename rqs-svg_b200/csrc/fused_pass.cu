@@ -1996,11 +1996,11 @@ FusedExecutor::~FusedExecutor()
 // flush's passes on the stream (which may still read the device buffer; the
 // copy is ordered after them). The pinned staging buffer is reused once the
 // previous copy has completed. Returns null when there are no tables.
-const double2 *FusedExecutor::upload_tables()
+const double2 *FusedExecutor::upload_tables(const std::vector<double2> &tables)
 {
-    if (tables_.empty())
+    if (tables.empty())
         return nullptr;
-    const size_t count = tables_.size();
+    const size_t count = tables.size();
     if (tables_copied_)
         QCSB_CUDA(cudaEventSynchronize(tables_copied_));
     else
@@ -2019,7 +2019,7 @@ const double2 *FusedExecutor::upload_tables()
         QCSB_CUDA(cudaMallocHost(&tables_host_, cap * sizeof(double2)));
         tables_cap_ = cap;
     }
-    std::memcpy(tables_host_, tables_.data(), count * sizeof(double2));
+    std::memcpy(tables_host_, tables.data(), count * sizeof(double2));
     QCSB_CUDA(cudaMemcpyAsync(tables_dev_, tables_host_, count * sizeof(double2), cudaMemcpyHostToDevice, stream_));
     QCSB_CUDA(cudaEventRecord(tables_copied_, stream_));
     return tables_dev_;
@@ -2043,36 +2043,194 @@ void FusedExecutor::settle_judge()
     pending_learned_ = -1;
 }
 
-int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<GateOp> &queued, int mode,
-                       qcs_b200_stats &stats, KernelTimer &timer)
+// Hash of everything a queue's plan depends on: every field of every op,
+// matrix entries bit for bit.
+static uint64_t queue_content_hash(const std::vector<GateOp> &ops)
 {
-    const bool c64 = amp_bytes == (int)sizeof(float2);
-    auto plain = [&](const GateOp &op) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        h ^= v;
+        h *= 1099511628211ull;
+    };
+    for (const GateOp &op : ops)
+    {
+        mix((uint64_t)op.nt | ((uint64_t)op.na << 8) | ((uint64_t)op.diag << 16));
+        for (int i = 0; i < op.nt; ++i)
+            mix((uint64_t)op.tq[i]);
+        mix(op.cmask);
+        mix(op.cval);
+        for (int i = 0; i < op.na; ++i)
+            mix(op.act[i]);
+        const int nm = op.diag ? op.na : op.na * op.na;
+        for (int i = 0; i < nm; ++i)
+        {
+            uint64_t re, im;
+            std::memcpy(&re, &op.mat[i].re, sizeof(re));
+            std::memcpy(&im, &op.mat[i].im, sizeof(im));
+            mix(re);
+            mix(im);
+        }
+    }
+    mix(ops.size());
+    return h;
+}
+
+static bool same_op(const GateOp &a, const GateOp &b)
+{
+    if (a.nt != b.nt || a.na != b.na || a.diag != b.diag || a.cmask != b.cmask || a.cval != b.cval)
+        return false;
+    for (int i = 0; i < a.nt; ++i)
+        if (a.tq[i] != b.tq[i])
+            return false;
+    for (int i = 0; i < a.na; ++i)
+        if (a.act[i] != b.act[i])
+            return false;
+    const int nm = a.diag ? a.na : a.na * a.na;
+    return std::memcmp(a.mat, b.mat, sizeof(a.mat[0]) * nm) == 0;
+}
+
+FusedExecutor::FlushPlan *FusedExecutor::find_plan(const std::vector<GateOp> &queued, uint64_t hash, int n,
+                                                   int amp_bytes, int k, int max_ops, int tag)
+{
+    for (auto &p : plans_)
+    {
+        if (p->hash != hash || p->n != n || p->amp_bytes != amp_bytes || p->k != k || p->max_ops != max_ops ||
+            p->tensor_mode != tensor_mode_ || p->tensor_engine != tensor_engine_ || p->tag != tag ||
+            p->queued.size() != queued.size())
+            continue;
+        bool same = true;
+        for (size_t i = 0; i < queued.size() && same; ++i)
+            same = same_op(p->queued[i], queued[i]);
+        if (same)
+            return p.get();
+    }
+    return nullptr;
+}
+
+// One launch of a plan: a plain gate kernel, a register pass, or a tensor
+// pass (its stage-matrix builder, then the pass).
+int FusedExecutor::launch_plan_step(FlushPlan &plan, long st, void *state, const double2 *tables_dev,
+                                    qcs_b200_stats &stats, KernelTimer &timer, const PassFeatures *features)
+{
+    const bool c64 = plan.amp_bytes == (int)sizeof(float2);
+    const int n = plan.n;
+    int launches = 0;
+    if (st < 0)
+    {
+        const GateOp &op = plan.ops[-1 - st];
         if (timer.enabled)
-            timer.begin(stream_, KernelTimer::kPlain, 2.0 * amp_bytes * op.changed_amps(n));
+            timer.begin(stream_, KernelTimer::kPlain, 2.0 * plan.amp_bytes * op.changed_amps(n));
         const int k = c64 ? launch_gate_plain<float>(static_cast<float2 *>(state), n, op, stream_)
                           : launch_gate_plain<double>(static_cast<double2 *>(state), n, op, stream_);
         if (timer.enabled)
             timer.end(stream_);
         stats.plain_gate_kernels += k;
         return k;
-    };
+    }
+    FPassParams &prm = plan.params[st];
+    prm.tables = tables_dev;
+    if (timer.enabled)
+        timer.begin(stream_, KernelTimer::kFused, 2.0 * plan.amp_bytes * std::ldexp(1.0, n), features);
+    const int t = plan.tensor_of[st];
+    if (t >= 0)
+    {
+        TPassParams &tp = plan.tparams[t];
+        TBuildParams &tb = plan.tbuild[t];
+        if (tb.nmats > mats_cap_)
+        {
+            // the old buffer may still be read by queued passes
+            QCSB_CUDA(cudaStreamSynchronize(stream_));
+            cudaFree(mats_dev_);
+            mats_dev_ = nullptr;
+            mats_cap_ = 0;
+            const size_t cap = std::max<size_t>(tb.nmats, 256);
+            QCSB_CUDA(cudaMalloc(&mats_dev_, cap * kTensorMatrixBytes));
+            mats_cap_ = cap;
+        }
+        prm.state = state;
+        tb.out = mats_dev_;
+        tp.mats = mats_dev_;
+        tp.state = state;
+        tp.err = err_dev_;
+        launches += launch_stage_matrices<double>(prm, tb, stream_);
+        if (tp.umma)
+            launches += launch_tc_pass(tp, stream_);
+        else
+            launches += c64 ? launch_tensor_pass<float>(tp, stream_) : launch_tensor_pass<double>(tp, stream_);
+        ++stats.tensor_passes;
+        stats.tensor8_passes += tp.width == 3 ? 1 : 0;
+        stats.tcgen05_passes += tp.umma ? 1 : 0;
+    }
+    else
+    {
+        launches += c64 ? launch_fused_pass<float>(state, plan.ks[st], prm, stream_)
+                        : launch_fused_pass<double>(state, plan.ks[st], prm, stream_);
+    }
+    if (timer.enabled)
+        timer.end(stream_);
+    ++stats.fused_passes;
+    return launches;
+}
+
+int FusedExecutor::replay(FlushPlan &plan, void *state, qcs_b200_stats &stats, KernelTimer &timer)
+{
+    const double2 *tables_dev = upload_tables(plan.tables);
     int launches = 0;
+    for (long st : plan.steps)
+        launches += launch_plan_step(plan, st, state, tables_dev, stats, timer, nullptr);
+    ++stats.replayed_flushes;
+    return launches;
+}
+
+int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<GateOp> &queued, int mode,
+                       qcs_b200_stats &stats, KernelTimer &timer)
+{
+    const bool c64 = amp_bytes == (int)sizeof(float2);
     // Small registers: a pass would not fill a warp; run gate by gate.
     if (n < fused_min_qubits())
     {
+        int launches = 0;
         for (const GateOp &op : queued)
-            launches += plain(op);
+        {
+            if (timer.enabled)
+                timer.begin(stream_, KernelTimer::kPlain, 2.0 * amp_bytes * op.changed_amps(n));
+            const int k = c64 ? launch_gate_plain<float>(static_cast<float2 *>(state), n, op, stream_)
+                              : launch_gate_plain<double>(static_cast<double2 *>(state), n, op, stream_);
+            if (timer.enabled)
+                timer.end(stream_);
+            stats.plain_gate_kernels += k;
+            launches += k;
+        }
         return launches;
     }
-    const std::vector<GateOp> ops = defer_x(queued);
     const int k = choose_local_bits(n, local_bits_);
     const int low = std::min(kLowBits, k);
     const int max_ops = (max_ops_ > 0 && max_ops_ < kFusedMaxOps) ? max_ops_ : kFusedMaxOps;
-    std::vector<Segment> segs = plan_greedy(ops, n, k, low, max_ops);
+    // Kept plans are used and made only when no pass timing is recorded (the
+    // timings carry features of the planning) and the judge is not timing
+    // this flush.
+    const uint64_t hash = timer.enabled ? 0 : queue_content_hash(queued);
+    const bool learned = mode == QCS_FUSION_LEARNED && model_ != nullptr && model_->trained();
+    int tag = 0;
+    if (!learned && !timer.enabled)
+        if (FlushPlan *kept = find_plan(queued, hash, n, amp_bytes, k, max_ops, 0))
+        {
+            last_plan_learned = 0;
+            return replay(*kept, state, stats, timer);
+        }
 
+    auto plan = std::make_unique<FlushPlan>();
+    plan->n = n;
+    plan->amp_bytes = amp_bytes;
+    plan->k = k;
+    plan->max_ops = max_ops;
+    plan->tensor_mode = tensor_mode_;
+    plan->tensor_engine = tensor_engine_;
+    plan->ops = defer_x(queued);
+    const std::vector<GateOp> &ops = plan->ops;
+    std::vector<Segment> segs;
     bool timed_flush = false;
-    if (mode == QCS_FUSION_LEARNED && model_ != nullptr && model_->trained())
+    if (learned)
     {
         settle_judge();
         const uint64_t sig = queue_signature(ops);
@@ -2097,6 +2255,12 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         last_greedy_ms = entry->greedy_ms;
         last_learned_ms = entry->learned_ms;
         last_plan_learned = use_learned ? 1 : 0;
+        tag = use_learned ? 1 : 2;
+        timed_flush = entry->learned_ms < 0.0 || entry->greedy_ms < 0.0;
+        if (!timed_flush && !timer.enabled)
+            if (FlushPlan *kept = find_plan(queued, hash, n, amp_bytes, k, max_ops, tag))
+                return replay(*kept, state, stats, timer);
+        segs = plan_greedy(ops, n, k, low, max_ops);
         if (use_learned)
         {
             // the learned plan of a queue is computed once (building and
@@ -2118,7 +2282,7 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
                 learned_plans_.push_back({key, segs});
             }
         }
-        if (entry->learned_ms < 0.0 || entry->greedy_ms < 0.0)
+        if (timed_flush)
         {
             if (!judge_a_)
             {
@@ -2128,86 +2292,38 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
             QCSB_CUDA(cudaEventRecord(judge_a_, stream_));
             pending_sig_ = sig;
             pending_learned_ = use_learned ? 1 : 0;
-            timed_flush = true;
         }
     }
     else
     {
         last_plan_learned = 0;
+        segs = plan_greedy(ops, n, k, low, max_ops);
     }
 
     // Passes launch as soon as they are built, so that the GPU runs while the
     // host plans the rest, until the first pass that needs phase-run tables:
     // from there on, passes are built first and launched after the tables of
     // all of them have gone to the device in one copy (order is kept).
-    // step >= 0: a pass (index into params), step < 0: plain op -1 - step.
-    std::vector<FPassParams> params;
     std::vector<PlannedPass> pieces;
     std::vector<std::vector<StageCond>> conds;
-    // per pass: index into tparams/tbuild when it runs as a tensor pass, else -1
-    std::vector<int> tensor_of;
-    std::vector<TPassParams> tparams;
-    std::vector<TBuildParams> tbuild;
-    std::vector<long> steps;
-    tables_.clear();
-    bool deferring = false;
-    auto launch_step = [&](long st, const double2 *tables_dev) {
-        if (st < 0)
-        {
-            launches += plain(ops[-1 - st]);
-            return;
-        }
-        FPassParams &prm = params[st];
-        prm.tables = tables_dev;
-        if (timer.enabled)
-        {
-            const int width = tensor_of[st] >= 0 ? tparams[tensor_of[st]].width : 1;
-            const PassFeatures f = pass_features(ops, pieces[st], n, width, prm.nstages);
-            timer.begin(stream_, KernelTimer::kFused, 2.0 * amp_bytes * std::ldexp(1.0, n), &f);
-        }
-        if (tensor_of[st] >= 0)
-        {
-            TPassParams &tp = tparams[tensor_of[st]];
-            TBuildParams &tb = tbuild[tensor_of[st]];
-            if (tb.nmats > mats_cap_)
-            {
-                // the old buffer may still be read by queued passes
-                QCSB_CUDA(cudaStreamSynchronize(stream_));
-                cudaFree(mats_dev_);
-                mats_dev_ = nullptr;
-                mats_cap_ = 0;
-                const size_t cap = std::max<size_t>(tb.nmats, 256);
-                QCSB_CUDA(cudaMalloc(&mats_dev_, cap * kTensorMatrixBytes));
-                mats_cap_ = cap;
-            }
-            prm.state = state;
-            tb.out = mats_dev_;
-            tp.mats = mats_dev_;
-            tp.state = state;
-            tp.err = err_dev_;
-            launches += launch_stage_matrices<double>(prm, tb, stream_);
-            if (tp.umma)
-                launches += launch_tc_pass(tp, stream_);
-            else
-                launches += c64 ? launch_tensor_pass<float>(tp, stream_) : launch_tensor_pass<double>(tp, stream_);
-            ++stats.tensor_passes;
-            stats.tensor8_passes += tp.width == 3 ? 1 : 0;
-            stats.tcgen05_passes += tp.umma ? 1 : 0;
-        }
-        else
-        {
-            launches += c64 ? launch_fused_pass<float>(state, pieces[st].k, prm, stream_)
-                             : launch_fused_pass<double>(state, pieces[st].k, prm, stream_);
-        }
-        if (timer.enabled)
-            timer.end(stream_);
-        ++stats.fused_passes;
+    size_t launched = 0;   // steps launched while planning
+    int launches = 0;
+    auto step_features = [&](long st, PassFeatures &f) -> const PassFeatures * {
+        if (!timer.enabled || st < 0)
+            return nullptr;
+        const int t = plan->tensor_of[st];
+        const int width = t >= 0 ? plan->tparams[t].width : 1;
+        f = pass_features(ops, pieces[st], n, width, plan->params[st].nstages);
+        return &f;
     };
     auto add_step = [&](long st) {
-        if (deferring)
-            steps.push_back(st);
-        else
-            launch_step(st, nullptr);
+        plan->steps.push_back(st);
+        if (plan->tables.empty())
+        {
+            PassFeatures f;
+            launches += launch_plan_step(*plan, st, state, nullptr, stats, timer, step_features(st, f));
+            launched = plan->steps.size();
+        }
     };
     for (const Segment &s : segs)
     {
@@ -2216,8 +2332,9 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
             add_step(-1 - (long)s.plain_op);
             continue;
         }
+        std::vector<FPassParams> &params = plan->params;
         const size_t before = params.size();
-        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces, &tables_, &conds))
+        if (!build_pieces(ops, s.pass, n, params, nullptr, &pieces, &plan->tables, &conds))
         {
             params.resize(before);
             pieces.resize(before);
@@ -2228,47 +2345,64 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
         }
         // a width the learned planner chose fixes the path (where the pass
         // allows it; else the register path)
-        int mode = tensor_mode_;
+        int tmode = tensor_mode_;
         if (s.width == 1)
-            mode = 0;
+            tmode = 0;
         else if (s.width == 4 && tensor_mode_ != 0)
-            mode = 2;
+            tmode = 2;
         else if (s.width == 3 && tensor_mode_ != 0)
-            mode = 3;
+            tmode = 3;
         PassChoice choice;
-        choose_execution(ops, s.pass, n, amp_bytes, mode, params, pieces, conds, &tables_, choice, before,
+        choose_execution(ops, s.pass, n, amp_bytes, tmode, params, pieces, conds, &plan->tables, choice, before,
                          tensor_engine_);
         for (size_t i = before; i < params.size(); ++i)
         {
+            plan->ks.push_back(pieces[i].k);
             const int t = choice.tensor[i - before];
             if (t >= 0)
             {
-                tparams.push_back(choice.tparams[t]);
-                tbuild.push_back(choice.tbuild[t]);
-                tensor_of.push_back(static_cast<int>(tparams.size()) - 1);
+                plan->tparams.push_back(choice.tparams[t]);
+                plan->tbuild.push_back(choice.tbuild[t]);
+                plan->tensor_of.push_back(static_cast<int>(plan->tparams.size()) - 1);
             }
             else
             {
-                tensor_of.push_back(-1);
+                plan->tensor_of.push_back(-1);
             }
         }
-        deferring = deferring || !tables_.empty();
         // complex64 register passes read their entries as float2; tensor
         // passes build their matrices from the double2 entries
         for (size_t i = before; i < params.size(); ++i)
-            if (c64 && tensor_of[i] < 0)
+            if (c64 && plan->tensor_of[i] < 0)
                 entries_to_float(params[i].entries, params[i].nentries);
         for (size_t i = before; i < params.size(); ++i)
             add_step((long)i);
     }
-    if (!steps.empty())
+    if (launched < plan->steps.size())
     {
-        const double2 *tables_dev = upload_tables();
-        for (long st : steps)
-            launch_step(st, tables_dev);
+        const double2 *tables_dev = upload_tables(plan->tables);
+        for (size_t i = launched; i < plan->steps.size(); ++i)
+        {
+            PassFeatures f;
+            const long st = plan->steps[i];
+            launches += launch_plan_step(*plan, st, state, tables_dev, stats, timer, step_features(st, f));
+        }
     }
     if (timed_flush)
         QCSB_CUDA(cudaEventRecord(judge_b_, stream_));
+    if (!timer.enabled && !timed_flush)
+    {
+        plan->queued = queued;
+        plan->hash = hash;
+        plan->tag = tag;
+        if (plans_.size() < kKeptPlans)
+            plans_.push_back(std::move(plan));
+        else
+        {
+            plans_[plans_next_] = std::move(plan);
+            plans_next_ = (plans_next_ + 1) % kKeptPlans;
+        }
+    }
     return launches;
 }
 

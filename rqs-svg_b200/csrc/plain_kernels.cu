@@ -405,6 +405,15 @@ __global__ void collapse_kernel(V *state, uint64_t ngroups, uint64_t lowmask, ui
     }
 }
 
+// Kept amplitudes are not touched (no reads at all).
+template <typename V>
+__global__ void collapse_mask_kernel(V *state, uint64_t count, uint64_t cmask, uint64_t cval)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (uint64_t)gridDim.x * kThreads)
+        if ((i & cmask) != cval)
+            __stcs(state + i, make_cx<V>(0.0, 0.0));
+}
+
 // <Z> sums. Thread k of the grid (G = gridDim * 256 = 2^gbits threads)
 // visits indices i = it * G + k. Bits of i below gbits are fixed per thread;
 // bits at or above gbits are the bits of `it`. Per block the kernel writes
@@ -741,6 +750,16 @@ int launch_collapse(typename Cx<R>::T *state, int n, int t, int keep_value, cuda
 }
 
 template <typename R>
+int launch_collapse_mask(typename Cx<R>::T *state, int n, uint64_t cmask, uint64_t cval, cudaStream_t stream)
+{
+    typedef typename Cx<R>::T V;
+    const uint64_t count = 1ull << n;
+    collapse_mask_kernel<V><<<grid_for(count, kThreads * 4), kThreads, 0, stream>>>(state, count, cmask, cval);
+    QCSB_CUDA(cudaGetLastError());
+    return 1;
+}
+
+template <typename R>
 int launch_zsums(const typename Cx<R>::T *state, int n, double *partials, double *sums, cudaStream_t stream)
 {
     typedef typename Cx<R>::T V;
@@ -821,6 +840,7 @@ int launch_narrow(const double2 *in, uint64_t count, typename Cx<R>::T *out, cud
     template int launch_measure_probs<R>(const Cx<R>::T *, int, int, uint64_t, uint64_t, double2 *, double2 *,      \
                                          unsigned *, cudaStream_t);                                                 \
     template int launch_collapse<R>(Cx<R>::T *, int, int, int, cudaStream_t);                                       \
+    template int launch_collapse_mask<R>(Cx<R>::T *, int, uint64_t, uint64_t, cudaStream_t);                        \
     template int launch_zsums<R>(const Cx<R>::T *, int, double *, double *, cudaStream_t);                          \
     template int launch_gather_logical<R>(const Cx<R>::T *, int, const int *, uint64_t, uint64_t, double2 *,        \
                                           cudaStream_t);                                                            \

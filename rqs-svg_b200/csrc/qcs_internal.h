@@ -131,6 +131,10 @@ int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t 
 // Zero every amplitude whose bit t differs from keep_value.
 template <typename R>
 int launch_collapse(typename Cx<R>::T *state, int n, int t, int keep_value, cudaStream_t stream);
+// Zero every amplitude i with (i & cmask) != cval: the collapses of several
+// measurements in one write pass.
+template <typename R>
+int launch_collapse_mask(typename Cx<R>::T *state, int n, uint64_t cmask, uint64_t cval, cudaStream_t stream);
 
 // sums[0] = sum |a|^2, sums[1 + q] = sum over amplitudes with bit q set of
 // |a|^2 (physical qubits q = 0..n-1). partials must hold

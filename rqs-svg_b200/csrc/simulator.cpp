@@ -408,6 +408,22 @@ void Simulator::flush()
 {
     if (pending_.empty() || state_ == nullptr)
         return;
+    if (pending_gates_ == 0)
+    {
+        // only collapses of measurements (each on its own qubit, since a
+        // re-measurement with no gate between is answered from the cache):
+        // one write pass zeroes every branch they exclude
+        uint64_t cmask = 0, cval = 0;
+        for (const GateOp &z : pending_)
+        {
+            cmask |= 1ull << z.tq[0];
+            if (z.act[0] == 0)
+                cval |= 1ull << z.tq[0];
+        }
+        stats.kernel_launches += QCSB_ON_STATE(launch_collapse_mask, n_, cmask, cval, stream_);
+        discard_pending();
+        return;
+    }
     if (c64() && norm_target_ < 0.0 && opt_tensor_ != 0 && fusion_mode_ != QCS_FUSION_PLAIN)
     {
         // the norm to restore after this flush is the register's norm now

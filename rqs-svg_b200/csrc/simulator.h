@@ -5,6 +5,7 @@
 #include "qcs_internal.h"
 #include "qcs_b200.h"
 
+#include <memory>
 #include <random>
 #include <vector>
 
@@ -216,6 +217,7 @@ class FusedExecutor
         model_ = model;
         learned_plans_.clear();
         judge_.clear();
+        plans_.clear();
     }
     // Tensor passes (tensor_pass.cu): 0 never, 1 where the cost estimate
     // favours them (default; 16 x 16 or 8 x 8 stages, whichever it favours),
@@ -240,13 +242,39 @@ class FusedExecutor
         double greedy_ms = -1.0;
         double learned_ms = -1.0;
     };
+    // The launches of one flush as planned. A plan is kept with the queue it
+    // was made for (every field of every op, matrices bit for bit), so that
+    // the same queue again -- a circuit re-run for every sample -- launches
+    // without planning.
+    struct FlushPlan
+    {
+        std::vector<GateOp> queued;   // the queue as given: the key
+        uint64_t hash = 0;
+        int n = 0, amp_bytes = 0, k = 0, max_ops = 0, tensor_mode = 0, tensor_engine = 0;
+        int tag = 0;                  // 0 greedy planner, 1 learned plan, 2 greedy plan chosen by the judge
+        std::vector<GateOp> ops;      // after defer_x: plain steps index into them
+        std::vector<FPassParams> params;
+        std::vector<int> ks;          // local qubits of each pass
+        std::vector<int> tensor_of;   // per pass: index into tparams / tbuild, or -1
+        std::vector<TPassParams> tparams;
+        std::vector<TBuildParams> tbuild;
+        std::vector<long> steps;      // launch order: >= 0 a pass, < 0 plain op -1 - step
+        std::vector<double2> tables;  // phase-run tables of the passes
+    };
     void settle_judge();
-    const double2 *upload_tables();
+    const double2 *upload_tables(const std::vector<double2> &tables);
+    int launch_plan_step(FlushPlan &plan, long st, void *state, const double2 *tables_dev, qcs_b200_stats &stats,
+                         KernelTimer &timer, const PassFeatures *features);
+    FlushPlan *find_plan(const std::vector<GateOp> &queued, uint64_t hash, int n, int amp_bytes, int k,
+                         int max_ops, int tag);
+    int replay(FlushPlan &plan, void *state, qcs_b200_stats &stats, KernelTimer &timer);
+    static constexpr size_t kKeptPlans = 8;
+    std::vector<std::unique_ptr<FlushPlan>> plans_;
+    size_t plans_next_ = 0;   // the slot the next kept plan replaces once all are used
 
     cudaStream_t stream_;
-    // phase-run tables of the current flush: built on the host, staged in
+    // phase-run tables: built on the host with a flush's plan, staged in
     // pinned memory, copied to the device once per flush
-    std::vector<double2> tables_;
     double2 *tables_host_ = nullptr;
     double2 *tables_dev_ = nullptr;
     size_t tables_cap_ = 0;

@@ -67,6 +67,7 @@ class Stats(ctypes.Structure):
         ("tensor_passes", ctypes.c_uint64),
         ("tensor8_passes", ctypes.c_uint64),
         ("tcgen05_passes", ctypes.c_uint64),
+        ("replayed_flushes", ctypes.c_uint64),
     ]
 
 
