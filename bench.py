@@ -117,6 +117,8 @@ def parse_args():
                     help="tensor passes (stages as dense matrices on the tensor cores): auto (default) where the "
                          "cost estimate favours them, 16x16 or 8x8 stages; always: 16x16 stages wherever allowed; "
                          "8x8: 8x8 stages wherever allowed")
+    ap.add_argument("--batch-tensor", type=int, choices=[0, 1, 2], default=1,
+                    help="hea_batch: 0 register passes only, 1 tuned per group (default), 2 tensor passes where allowed")
     ap.add_argument("--engine", choices=["tcgen05", "mma.sync"], default="tcgen05",
                     help="tensor engine of complex64 16x16 stages: tcgen05 (default, where a pass allows it) or "
                          "warp-level mma.sync")
@@ -594,6 +596,7 @@ def main_batch(args, dist):
         return run_reference_batch(args, dist, widths, circs, depth, workload)
     lib = qcs_b200.Library(qcs_b200.LIB_PATH)
     b = qcs_b200.Batch(lib, precision)
+    b.set_tensor_passes(args.batch_tensor)
     for w, c in zip(widths, circs):
         b.add_circuit(w, c)
     t0 = time.perf_counter()
@@ -647,6 +650,7 @@ def main_batch(args, dist):
         "dtype": "c128 (f64)" if precision == 128 else "c64 (f32 gates, f64 reductions)",
         "data": "synthetic (seeded circuits and parameters)",
         "config": {"workload": workload, "circuits": len(circs), "depth": depth, "precision": precision,
+                   "tensor_passes": ["never", "tuned", "always"][args.batch_tensor],
                    "amplitudes": info["amplitudes"], "parallelism": f"replicas x{WORLD}",
                    "l2": f"registers ({info['amplitudes'] * precision // 8 >> 20} MiB) larger than L2; no flush"},
         "circuits_per_s": len(circs) / sec,
@@ -661,7 +665,8 @@ def main_batch(args, dist):
                      "peak_kind": f"{peak_kind} (copy, MEASURED_PEAKS hbm_gbs)" if peak_kind == "measured" else "fallback",
                      "traffic": None, "note": "pass bytes over the whole run's device time (graph: entries in, "
                                               "passes, <Z>, results out)"},
-        "batch": {"groups": info["groups"], "passes": info["passes"], "pass_bytes": info["pass_bytes"],
+        "batch": {"groups": info["groups"], "passes": info["passes"], "tensor_passes": info["tensor_passes"],
+                  "pass_bytes": info["pass_bytes"],
                   "setup_s": setup_s, "step_s": dev},
         "cpu_baseline": cpu,
         "accuracy": accuracy,

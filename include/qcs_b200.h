@@ -295,6 +295,8 @@ typedef struct qcs_b200_batch_info
     double pass_bytes;          /* bytes the passes move per run: 2 x bytes/amplitude x 2^n per pass and register
                                    (the first pass of a register writes only) */
     double last_run_ms;         /* device time of the last run */
+    uint32_t tensor_passes;     /* passes run as 8 x 8 tensor passes (a subset of passes) */
+    uint32_t reserved;
 } qcs_b200_batch_info;
 
 /* amplitude_bits: 128 (complex128) or 64 (complex64). */
@@ -313,6 +315,14 @@ int qcs_b200_batch_expectation_z(qcs_b200_batch *batch, double *expectations, ui
 /* The register of one circuit after the last run (2 * 2^n doubles). */
 int qcs_b200_batch_get_statevector(qcs_b200_batch *batch, uint32_t index, double *amplitudes, uint64_t count);
 int qcs_b200_batch_get_info(qcs_b200_batch *batch, qcs_b200_batch_info *info);
+/* Tensor passes of a batch: every group of at least 11 qubits can run its
+   passes as 8 x 8 tensor passes, each register's stage matrices built on the
+   GPU from its own gate entries (FP64 tensor cores for complex128, split
+   TF32 for complex64). mode 0: register passes only; 1 (the default): the
+   autotuner times the tensor passes beside the register passes of each
+   group and keeps the faster; 2: tensor passes wherever a pass allows them.
+   Takes effect at the next run (which plans the batch again). */
+int qcs_b200_batch_set_tensor_passes(qcs_b200_batch *batch, int mode);
 
 /*
  * How the fused planner (greedy mode, 11 local qubits, 256 gates per pass)

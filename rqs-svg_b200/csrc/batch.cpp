@@ -111,6 +111,9 @@ void Batch::release_device()
     cudaFree(zregs_dev_);
     cudaFree(zpartials_dev_);
     cudaFree(zout_dev_);
+    cudaFree(tmats_dev_);
+    tmats_dev_ = nullptr;
+    tmats_bytes_ = 0;
     if (mats_host_)
         cudaFreeHost(mats_host_);
     if (zout_host_)
@@ -207,7 +210,7 @@ void Batch::set_parameters(const double *params, uint64_t count)
     dirty_ = built_;
 }
 
-void Batch::plan_group(Group &g, int k)
+void Batch::plan_group(Group &g, int k, bool tensor)
 {
     g.k = k;
     g.passes.clear();
@@ -217,6 +220,32 @@ void Batch::plan_group(Group &g, int k)
     {
         if (!s.fused)
             throw std::runtime_error("batch: a gate of this circuit cannot run in a fused pass");
+        if (tensor && s.pass.k == kTensorLocal)
+        {
+            // the pass replanned with 8 x 8 stages, as a tensor pass where
+            // every piece allows it
+            PlannedPass p3 = s.pass;
+            p3.stage_width = 3;
+            std::vector<FPassParams> params3;
+            std::vector<std::vector<FOpSource>> srcs3;
+            std::vector<std::vector<StageCond>> conds3;
+            bool ok = build_pieces(g.shape, p3, g.n, params3, &srcs3, nullptr, nullptr, &conds3);
+            std::vector<Pass> tpasses(ok ? params3.size() : 0);
+            for (size_t i = 0; ok && i < params3.size(); ++i)
+            {
+                Pass &p = tpasses[i];
+                p.prm = params3[i];
+                p.src = std::move(srcs3[i]);
+                p.tensor = make_tensor_params(p.prm, conds3[i], amp_bytes_, p.tp, p.tb, 3);
+                ok = p.tensor;
+            }
+            if (ok)
+            {
+                for (Pass &p : tpasses)
+                    g.passes.push_back(std::move(p));
+                continue;
+            }
+        }
         std::vector<FPassParams> params;
         std::vector<std::vector<FOpSource>> srcs;
         if (!build_pieces(g.shape, s.pass, g.n, params, &srcs))
@@ -353,6 +382,35 @@ void Batch::fill_entries(int only_group)
             std::rethrow_exception(e);
 }
 
+// The stage-matrix buffer: the largest tensor pass's matrices over all its
+// group's registers (8 x 8 stages: kTensor3Fragments x 32 lanes x 16 bytes
+// per matrix). Grown before any graph is captured.
+void Batch::ensure_tensor_mats()
+{
+    size_t need = 0;
+    for (const Group &g : groups_)
+        for (const Pass &p : g.passes)
+            if (p.tensor)
+                need = std::max(need, static_cast<size_t>(p.tb.nmats) * kTensor3Fragments * 32 * 16 * g.members.size());
+    if (need <= tmats_bytes_)
+        return;
+    if (stream_)
+        QCSB_CUDA(cudaStreamSynchronize(stream_));
+    cudaFree(tmats_dev_);
+    tmats_dev_ = nullptr;
+    tmats_bytes_ = 0;
+    QCSB_CUDA(cudaMalloc(&tmats_dev_, need));
+    tmats_bytes_ = need;
+}
+
+void Batch::set_tensor_mode(int mode)
+{
+    if (mode < 0 || mode > 2)
+        throw std::runtime_error(strformat("batch tensor mode %d is not 0 (never), 1 (tuned) or 2 (always)", mode));
+    tensor_mode_ = mode;
+    invalidate();
+}
+
 void Batch::enqueue_passes(const Group &g, cudaStream_t s, int *launches)
 {
     void *base = static_cast<char *>(arena_) + g.amp_off * amp_bytes_;
@@ -365,9 +423,28 @@ void Batch::enqueue_passes(const Group &g, cudaStream_t s, int *launches)
     }
     for (size_t pi = 0; pi < g.passes.size(); ++pi)
     {
-        FPassParams &prm = const_cast<FPassParams &>(g.passes[pi].prm);
+        Pass &pass = const_cast<Pass &>(g.passes[pi]);
+        FPassParams &prm = pass.prm;
         prm.chunks = (uint64_t)g.members.size() << (g.n - g.k);
         prm.from_zero = pi == 0 ? 1 : 0;
+        if (pass.tensor)
+        {
+            TBuildParams &tb = pass.tb;
+            TPassParams &tp = pass.tp;
+            tb.out = static_cast<double2 *>(tmats_dev_);
+            tb.regs = static_cast<uint32_t>(g.members.size());
+            tb.batch_float = amp_bytes_ == 8 ? 1 : 0;
+            *launches += launch_stage_matrices<double>(prm, tb, s);
+            tp.state = base;
+            tp.mats = static_cast<const double2 *>(tmats_dev_);
+            tp.reg_mats = tb.nmats;
+            tp.batch_cbits = g.n - g.k;
+            tp.chunks = prm.chunks;
+            tp.from_zero = prm.from_zero;
+            tp.err = nullptr;
+            *launches += amp_bytes_ == 8 ? launch_tensor_pass<float>(tp, s) : launch_tensor_pass<double>(tp, s);
+            continue;
+        }
         *launches += amp_bytes_ == 8 ? launch_fused_batch<float>(base, g.k, prm, s)
                                      : launch_fused_batch<double>(base, g.k, prm, s);
     }
@@ -398,24 +475,36 @@ void Batch::tune()
     for (int gi = 0; gi < (int)groups_.size(); ++gi)
     {
         Group &g = groups_[gi];
-        std::vector<int> cands;
+        // candidates: register passes at k = 9..11, and 8 x 8 tensor passes
+        // (k = 11) unless the mode excludes them
+        std::vector<std::pair<int, bool>> cands;
         for (int k = kStageBits + 5; k <= kDefaultLocal; ++k)
         {
             const int kk = clamp_local_bits(k, g.n);
-            if (std::find(cands.begin(), cands.end(), kk) == cands.end())
-                cands.push_back(kk);
+            if (std::find(cands.begin(), cands.end(), std::make_pair(kk, false)) == cands.end())
+                cands.push_back({kk, false});
         }
-        if (cands.size() < 2 || !tune_enabled())
+        const bool tensor_ok = g.n >= kTensorLocal && tensor_mode_ != 0;
+        if (tensor_mode_ == 2 && tensor_ok)
         {
-            plan_group(g, cands.back());
+            plan_group(g, kTensorLocal, true);
             continue;
         }
-        int best_k = cands.back();
-        float best_ms = 0.0f;
-        for (int k : cands)
+        const int default_k = clamp_local_bits(kDefaultLocal, g.n);   // the largest register-path k
+        if (tensor_ok)
+            cands.push_back({kTensorLocal, true});
+        if (cands.size() < 2 || !tune_enabled())
         {
-            plan_group(g, k);
+            plan_group(g, default_k);
+            continue;
+        }
+        std::pair<int, bool> best = cands.front();
+        float best_ms = 0.0f;
+        for (const auto &cand : cands)
+        {
+            plan_group(g, cand.first, cand.second);
             layout_entries();
+            ensure_tensor_mats();
             fill_entries(gi);
             QCSB_CUDA(cudaMemcpyAsync(mats_dev_ + g.mats_off, mats_host_ + g.mats_off,
                                       sizeof(double2) * g.stride * g.members.size(), cudaMemcpyHostToDevice, stream_));
@@ -427,14 +516,13 @@ void Batch::tune()
             QCSB_CUDA(cudaEventSynchronize(ev1_));
             float ms = 0.0f;
             QCSB_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
-            if (k == cands.front() || ms < best_ms)
+            if (cand == cands.front() || ms < best_ms)
             {
                 best_ms = ms;
-                best_k = k;
+                best = cand;
             }
         }
-        if (g.k != best_k)
-            plan_group(g, best_k);
+        plan_group(g, best.first, best.second);
     }
 }
 
@@ -540,6 +628,7 @@ void Batch::build()
     layout_entries();
     tune();
     layout_entries();
+    ensure_tensor_mats();
     fill_entries();
 
     // capture the run: a graph per group, then the results (after dropping
@@ -661,6 +750,8 @@ void Batch::info(qcs_b200_batch_info *out) const
         for (const Group &g : groups_)
         {
             out->passes += (uint32_t)g.passes.size();
+            for (const Pass &p : g.passes)
+                out->tensor_passes += p.tensor ? 1u : 0u;
             const double reg = std::ldexp((double)amp_bytes_, g.n) * g.members.size();
             if (!g.passes.empty())
                 bytes += reg * (2.0 * g.passes.size() - 1.0);

@@ -49,6 +49,11 @@ class Batch
     void expectation_z(double *out, uint64_t count) const;
     void get_statevector(uint32_t index, double *out, uint64_t count);
     void info(qcs_b200_batch_info *out) const;
+    // 0: register passes only; 1 (default): the tuner times 8 x 8 tensor
+    // passes per group beside the register passes; 2: tensor passes wherever
+    // a pass allows them
+    void set_tensor_mode(int mode);
+    int tensor_mode() const { return tensor_mode_; }
 
   private:
     struct Gate
@@ -72,6 +77,11 @@ class Batch
     {
         FPassParams prm;
         std::vector<FOpSource> src;
+        // 8 x 8 tensor pass: per-register stage matrices built on the GPU
+        // from each register's entries, then the pass (tensor_pass.cu)
+        bool tensor = false;
+        TPassParams tp{};
+        TBuildParams tb{};
     };
     struct Group
     {
@@ -88,7 +98,8 @@ class Batch
 
     void invalidate();
     void build();
-    void plan_group(Group &g, int k);
+    void plan_group(Group &g, int k, bool tensor = false);
+    void ensure_tensor_mats();
     void layout_entries();
     void fill_entries(int only_group = -1);
     void fill_group_range(const Group &g, size_t first, size_t last);
@@ -123,6 +134,11 @@ class Batch
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     uint32_t launches_per_run_ = 0;
     double last_ms_ = 0.0;
+    int tensor_mode_ = 1;
+    // stage matrices of the tensor pass being run (every group's passes run
+    // in stream order, each builder right before its pass)
+    void *tmats_dev_ = nullptr;
+    size_t tmats_bytes_ = 0;
 };
 
 } // namespace qcsb

@@ -854,6 +854,11 @@ extern "C" int qcs_b200_batch_get_statevector(qcs_b200_batch *batch, uint32_t in
     return guarded([&] { batch_of(batch).get_statevector(index, amplitudes, count); });
 }
 
+extern "C" int qcs_b200_batch_set_tensor_passes(qcs_b200_batch *batch, int mode)
+{
+    return guarded([&] { batch_of(batch).set_tensor_mode(mode); });
+}
+
 extern "C" int qcs_b200_batch_get_info(qcs_b200_batch *batch, qcs_b200_batch_info *info)
 {
     return guarded([&] {

@@ -97,6 +97,29 @@ struct PoolEntries
     uint32_t off;
     __device__ __forceinline__ V operator[](int i) const { return pool_entry<V>(p, off + i); }
 };
+// Entries of the stage-matrix builder (FP64): the pass parameters (one
+// register, blk null) or a register's block of a batch's entry buffer
+// (float2 entries for complex64 batches, double2 otherwise).
+template <typename V>
+struct BuildEntries
+{
+    const FPassParams &p;
+    const void *blk;
+    int flt;
+    uint32_t off;
+    __device__ __forceinline__ V operator[](int i) const
+    {
+        if (blk == nullptr)
+            return pool_entry<V>(p, off + i);
+        if (flt)
+        {
+            const float2 e = __ldg(static_cast<const float2 *>(blk) + off + i);
+            return V{e.x, e.y};
+        }
+        const double2 e = __ldg(static_cast<const double2 *>(blk) + off + i);
+        return V{e.x, e.y};
+    }
+};
 template <typename V>
 struct BufferEntries
 {

@@ -68,6 +68,11 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
     const int col = static_cast<int>(gid & ((1u << width) - 1u));
     if (mat >= tb.nmats)
         return;
+    // batched passes: register blockIdx.y, its entries and its matrices
+    const uint32_t breg = blockIdx.y;
+    const void *blk = tb.regs > 0 ? static_cast<const void *>(p.mats + static_cast<size_t>(breg) * p.mat_stride) : nullptr;
+    const BuildEntries<V> ent{p, blk, tb.batch_float, 0u};
+    const uint32_t omat = tb.regs > 0 ? breg * tb.nmats + mat : mat;   // matrix slot written
     int st = 0;
     while (st + 1 < tb.nstages && tb.stages[st + 1].woff <= mat)
         ++st;
@@ -145,13 +150,13 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
         if (op.kind == F_PRUN)
         {
             phase_inline<V>(a, op, p.ops + oi + 1, j0, cbase, chunk, static_cast<int>(tidx), T, p.tables,
-                            [&](int off) { return pool_entry<V>(p, off); });
+                            [&](int off) { return ent[off]; });
             oi += op.lcmask;
             continue;
         }
         if ((cbase & op.gcmask) != op.gcval)
             continue;
-        apply_op<V>(a, op, PoolEntries<V>{p, op.moff}, j0, cbase, ss);
+        apply_op<V>(a, op, BuildEntries<V>{p, blk, tb.batch_float, op.moff}, j0, cbase, ss);
     }
     if (tb.umma)
     {
@@ -204,14 +209,14 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
                         : "=r"(lo)
                         : "f"(static_cast<float>(parts[part] - __uint_as_float(hi))));
                     uint32_t *f = reinterpret_cast<uint32_t *>(tb.out) +
-                                  ((static_cast<size_t>(mat) * kTensor3Fragments + part) * 32 + lane) * 4;
+                                  ((static_cast<size_t>(omat) * kTensor3Fragments + part) * 32 + lane) * 4;
                     f[b] = hi;
                     f[2 + b] = lo;
                 }
                 else
                 {
                     Real *f = reinterpret_cast<Real *>(tb.out) +
-                              ((static_cast<size_t>(mat) * kTensor3Fragments + part) * 32 + lane) * 2;
+                              ((static_cast<size_t>(omat) * kTensor3Fragments + part) * 32 + lane) * 2;
                     f[b] = parts[part];
                 }
             }
@@ -268,7 +273,10 @@ int launch_stage_matrices(const FPassParams &prm, const TBuildParams &tb, cudaSt
 {
     const unsigned threads = 64;
     const unsigned blocks = static_cast<unsigned>((static_cast<uint64_t>(tb.nmats) * (1u << tb.width) + threads - 1) / threads);
-    stage_matrix_kernel<R><<<blocks, threads, 0, stream>>>(prm, tb);
+    if (tb.regs > 0 && (tb.width != 3 || tb.umma || tb.regs > 65535u))
+        throw std::runtime_error("internal: batched stage matrices need 8 x 8 stages and at most 65535 registers");
+    const dim3 grid(blocks, tb.regs > 0 ? tb.regs : 1u);
+    stage_matrix_kernel<R><<<grid, threads, 0, stream>>>(prm, tb);
     QCSB_CUDA(cudaGetLastError());
     return 1;
 }

@@ -82,6 +82,12 @@ struct TBuildParams
     int width;                   // slot bits of the stages: 4 (16 x 16) or 3 (8 x 8)
     int umma;                    // B operands of tcgen05 passes instead of mma.sync fragments
     double2 *out;                // nmats x kTensorFragments x 32 lanes x 16 bytes (umma: 2 x nmats slabs)
+    // batched passes (8 x 8 stages only): registers whose matrices are built
+    // (0: one register, entries in the pass parameters); register r reads
+    // its entries at prm.mats + r * prm.mat_stride (float2 entries when
+    // batch_float) and writes its nmats matrices after those of r - 1
+    uint32_t regs;
+    int batch_float;
     TStage stages[kFusedMaxStages];
 };
 // bytes of the matrix buffer per matrix, either format
@@ -98,6 +104,12 @@ struct TPassParams
     int umma;                    // complex64 16 x 16 stages on tcgen05 (tensor_pass_tc.cu)
     uint32_t nmats;              // matrices in mats (umma: the low-part slabs follow the high ones)
     int *err;                    // set to 1 when a tcgen05 pass gives up waiting (host-mapped), or null
+    // batched passes (8 x 8 stages only; reg_mats 0: one register): chunk c
+    // is chunk c mod 2^batch_cbits of register c >> batch_cbits, whose
+    // amplitudes start at register << n and whose matrices start at matrix
+    // register * reg_mats
+    uint32_t reg_mats;
+    int batch_cbits;
     uint64_t chunks;
     uint64_t qmasks[kMaxLocal];
     uint64_t qbit[kMaxLocal];

@@ -364,13 +364,17 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
 #pragma unroll
     for (int b = 0; b < kStageBits; ++b)
         hb[b] = p.qbit[kTensorLocal - kStageBits + b];
+    // batched passes: the register's amplitudes start at register << n (the
+    // bits above n of the base; matrix choices read bits below n only)
     auto chunk_base = [&](uint64_t c) -> uint64_t {
-        uint64_t x = c;
+        uint64_t x = p.reg_mats > 0 ? (c & ((1ull << p.batch_cbits) - 1)) : c;
         for (int i = 0; i < kTensorLocal; ++i)
         {
             const uint64_t lo = x & p.qmasks[i];
             x = lo | ((x ^ lo) << 1);
         }
+        if (p.reg_mats > 0)
+            x |= (c >> p.batch_cbits) << p.n;
         return x;
     };
     auto elem_offset = [&](int m) -> uint64_t {
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
 #pragma unroll
             for (int m = 0; m < kSlots; ++m)
             {
-                const bool one = cb == 0 && m == 0 && tid == 0;
+                const bool one = (cb & ((1ull << p.n) - 1)) == 0 && m == 0 && tid == 0;
                 dst[TT::swz(tid + m * kThreads)] = V{one ? Real(1) : Real(0), Real(0)};
             }
         }
@@ -403,6 +407,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
     Frag bf[kTensor3Fragments];
     int bf_st = -1;
     uint32_t bf_v = 0;
+    uint64_t bf_reg = 0;   // register whose matrices bf holds (batched passes)
     auto matrix_of = [&](int st, uint64_t cb, int mt) -> uint32_t {
         const TStage &S = p.stages[st];
         uint32_t vc = 0;
@@ -411,13 +416,16 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
         const uint32_t tile = static_cast<uint32_t>(mt | (warp << 2));
         return (tile & ((1u << S.nlc) - 1u)) | (vc << S.nlc);
     };
-    auto fetch = [&](int st, uint32_t v) {
-        const Frag *w = mats + (static_cast<size_t>(p.stages[st].woff + v) * kTensor3Fragments) * 32 + lane;
+    auto fetch = [&](int st, uint32_t v, uint64_t cb) {
+        const uint64_t reg = cb >> p.n;
+        const Frag *w =
+            mats + (static_cast<size_t>(reg * p.reg_mats + p.stages[st].woff + v) * kTensor3Fragments) * 32 + lane;
 #pragma unroll
         for (int f = 0; f < kTensor3Fragments; ++f)
             bf[f] = __ldg(w + f * 32);
         bf_st = st;
         bf_v = v;
+        bf_reg = reg;
     };
 
     uint64_t c = blockIdx.x;
@@ -426,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
     uint64_t cbase_next = chunk_base(c);
     issue_load(cbase_next, smem);
     if (p.nstages > 0)
-        fetch(0, matrix_of(0, cbase_next, 0));
+        fetch(0, matrix_of(0, cbase_next, 0), cbase_next);
     int cur = 0;
     for (; c < p.chunks; c += gridDim.x)
     {
@@ -467,8 +475,8 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
             {
                 const uint32_t tile = static_cast<uint32_t>(mt | (warp << 2));
                 const uint32_t v = matrix_of(st, cbase, mt);
-                if (bf_st != st || bf_v != v)
-                    fetch(st, v);
+                if (bf_st != st || bf_v != v || bf_reg != (cbase >> p.n))
+                    fetch(st, v, cbase);
                 const uint32_t base = lane_pos ^ ((tile & 1) ? gbit[4] : 0u) ^ ((tile & 2) ? gbit[5] : 0u) ^
                                       ((tile & 4) ? gbit[6] : 0u) ^ ((tile & 8) ? gbit[7] : 0u);
                 auto pos = [&](int h, int m) { return base ^ (h ? hpos : 0u) ^ (m ? sbit[2] : 0u); };
@@ -487,9 +495,9 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
                     sb[pos(e >> 1, e & 1)] = V{t1[e] - t2[e], t3[e] - (t1[e] + t2[e])};
             }
             if (st + 1 < p.nstages)
-                fetch(st + 1, matrix_of(st + 1, cbase, 0));
+                fetch(st + 1, matrix_of(st + 1, cbase, 0), cbase);
             else if (next < p.chunks)
-                fetch(0, matrix_of(0, cbase_next, 0));
+                fetch(0, matrix_of(0, cbase_next, 0), cbase_next);
             __syncthreads();
         }
 
@@ -713,6 +721,8 @@ template <typename R>
 int launch_tensor_pass(const TPassParams &tp, cudaStream_t stream)
 {
     typedef typename Tensor<R>::V V;
+    if (tp.reg_mats > 0 && tp.width != 3)
+        throw std::runtime_error("internal: batched tensor passes run 8 x 8 stages only");
     const size_t smem = kTensor4Buffers * sizeof(V) * kChunk;
     const size_t smem3 = kTensor3Buffers * sizeof(V) * kChunk;
     static bool configured[64] = {};

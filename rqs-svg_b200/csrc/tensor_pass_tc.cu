@@ -419,6 +419,8 @@ __global__ void __launch_bounds__(kThreads, 4) tc_pass_kernel(const __grid_const
 
 int launch_tc_pass(const TPassParams &tp, cudaStream_t stream)
 {
+    if (tp.reg_mats > 0)
+        throw std::runtime_error("internal: tcgen05 passes run one register");
     static bool configured[64] = {};
     int dev = 0, sms = 0, per_sm = 0;
     QCSB_CUDA(cudaGetDevice(&dev));

@@ -125,6 +125,8 @@ class BatchInfo(ctypes.Structure):
         ("parameters", ctypes.c_uint64),
         ("pass_bytes", ctypes.c_double),
         ("last_run_ms", ctypes.c_double),
+        ("tensor_passes", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -230,6 +232,7 @@ class Library:
             "qcs_b200_batch_expectation_z": [_P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
             "qcs_b200_batch_get_statevector": [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64],
             "qcs_b200_batch_get_info": [_P, ctypes.POINTER(BatchInfo)],
+            "qcs_b200_batch_set_tensor_passes": [_P, ctypes.c_int],
             "qcs_b200_plan_summary_get": [ctypes.c_int, ctypes.POINTER(BatchGate), ctypes.c_uint64,
                                           ctypes.POINTER(PlanSummary)],
         }
@@ -617,6 +620,11 @@ class Batch:
 
     def run(self):
         self.lib.call("qcs_b200_batch_run", self.h)
+
+    def set_tensor_passes(self, mode: int):
+        """0: register passes only; 1: tuned per group (default); 2: 8 x 8
+        tensor passes wherever a pass allows them."""
+        self.lib.call("qcs_b200_batch_set_tensor_passes", self.h, mode)
 
     def expectation_z(self):
         """<Z_q> per circuit: a list of arrays (one value per qubit)."""

@@ -41,10 +41,25 @@ def _mixed_circuits():
     return circs
 
 
+# batch tensor modes: 0 register passes only, 1 tuned per group (default),
+# 2 8 x 8 tensor passes wherever a pass allows them (groups of >= 11 qubits)
+TENSOR_MODES = [0, 1, 2]
+
+
+def _check_tensor_mode(info, mode, widest):
+    if mode == 0 or widest < 11:
+        assert info["tensor_passes"] == 0
+    elif mode == 2:
+        assert info["tensor_passes"] > 0
+    assert info["tensor_passes"] <= info["passes"]
+
+
+@pytest.mark.parametrize("tensor", TENSOR_MODES)
 @pytest.mark.parametrize("precision", [128, 64])
-def test_batch_matches_oracle(gpu_lib, oracle_lib, precision):
+def test_batch_matches_oracle(gpu_lib, oracle_lib, precision, tensor):
     circs = _mixed_circuits()
     with qcs_b200.Batch(gpu_lib, precision) as b:
+        b.set_tensor_passes(tensor)
         for n, circ in circs:
             b.add_circuit(n, circ)
         b.run()
@@ -53,6 +68,7 @@ def test_batch_matches_oracle(gpu_lib, oracle_lib, precision):
         assert info["circuits"] == len(circs)
         assert info["groups"] == len(circs) - 3   # three circuits reuse a plan
         assert info["launches_per_run"] >= info["passes"] > 0
+        _check_tensor_mode(info, tensor, max(n for n, _ in circs))
         for i, (n, circ) in enumerate(circs):
             ref = _oracle_state(oracle_lib, n, circ)
             got = b.statevector(i)
@@ -65,8 +81,9 @@ def test_batch_matches_oracle(gpu_lib, oracle_lib, precision):
                 assert np.max(np.abs(zs[i] - _z_from_state(ref, n))) <= 1e-5, i
 
 
+@pytest.mark.parametrize("tensor", [0, 2])
 @pytest.mark.parametrize("precision", [128, 64])
-def test_batch_phase_runs_and_sign_runs(gpu_lib, oracle_lib, precision):
+def test_batch_phase_runs_and_sign_runs(gpu_lib, oracle_lib, precision, tensor):
     """Batched passes with phase runs (QFT controlled phases: explicit terms,
     since entries differ per register), runs of -1 phases (CZ, CCZ) with
     controls on stage, thread and chunk qubits, and pairs / groups of
@@ -80,9 +97,11 @@ def test_batch_phase_runs_and_sign_runs(gpu_lib, oracle_lib, precision):
             c += C.random_circuit(n, 12, seed=400 + 10 * seed + blk, max_controls=2, gates=diag)
         circs.append((n, c))
     with qcs_b200.Batch(gpu_lib, precision) as b:
+        b.set_tensor_passes(tensor)
         for n, circ in circs:
             b.add_circuit(n, circ)
         b.run()
+        _check_tensor_mode(b.info(), tensor, 14)
         for i, (n, circ) in enumerate(circs):
             ref = _oracle_state(oracle_lib, n, circ)
             got = b.statevector(i)
@@ -93,9 +112,11 @@ def test_batch_phase_runs_and_sign_runs(gpu_lib, oracle_lib, precision):
                 assert fid >= 1 - 1e-6, i
 
 
-def test_batch_parameter_updates(gpu_lib, oracle_lib):
+@pytest.mark.parametrize("tensor", [0, 2])
+def test_batch_parameter_updates(gpu_lib, oracle_lib, tensor):
     shapes = [(9, 2), (12, 3), (9, 2)]
     with qcs_b200.Batch(gpu_lib, 128) as b:
+        b.set_tensor_passes(tensor)
         for k, (n, d) in enumerate(shapes):
             b.add_circuit(n, C.hea_circuit(n, d, seed=k))
         nparams = b.info()["parameters"]
@@ -139,6 +160,8 @@ def test_batch_rejects_bad_input(gpu_lib):
             b.expectation_z()
         with pytest.raises(qcs_b200.QCSError, match="parameters"):
             b.set_parameters([0.5])
+        with pytest.raises(qcs_b200.QCSError, match="tensor mode 3"):
+            b.set_tensor_passes(3)
         b.run()
         z = b.expectation_z()[0]
         assert abs(z[0]) < 1e-15 and np.all(np.abs(z[1:] - 1) < 1e-15)
@@ -182,19 +205,22 @@ def test_batch_failed_build_releases_memory(gpu_lib):
     assert free_before - free_after < (64 << 20), (free_before, free_after)
 
 
+@pytest.mark.parametrize("tensor", TENSOR_MODES)
 @pytest.mark.parametrize("precision", [128, 64])
-def test_batch_multi_chunk_registers(gpu_lib, oracle_lib, precision):
+def test_batch_multi_chunk_registers(gpu_lib, oracle_lib, precision, tensor):
     """The batch workload's widest registers (15-20 qubits, depth 8: 16 to
     512 chunks per register in the batched pass), including two circuits of
     one structure, against the oracle: states, and <Z_q> of every qubit."""
     widths = [15, 16, 17, 18, 19, 20, 17]
     circs = [(w, C.hea_circuit(w, 8, seed=500 + i)) for i, w in enumerate(widths)]
     with qcs_b200.Batch(gpu_lib, precision) as b:
+        b.set_tensor_passes(tensor)
         for n, circ in circs:
             b.add_circuit(n, circ)
         b.run()
         zs = b.expectation_z()
         assert b.info()["groups"] == len(circs) - 1
+        _check_tensor_mode(b.info(), tensor, max(widths))
         for i, (n, circ) in enumerate(circs):
             ref = _oracle_state(oracle_lib, n, circ)
             got = b.statevector(i)
