@@ -158,6 +158,18 @@ def traffic_per_launch(n, kernel="fused_pass_kernel"):
     return None
 
 
+def batch_traffic_per_amplitude():
+    """dram read+write bytes per amplitude and pass of the batched 8x8 tensor
+    pass (complex64), from profiles/tensor3_pass_kernel_batch_traffic.txt, or None."""
+    try:
+        for line in (REPO / "profiles" / "tensor3_pass_kernel_batch_traffic.txt").read_text().splitlines():
+            if line.startswith("traffic_bytes_per_amplitude_pass:"):
+                return float(line.split(":")[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
 def dominant_pass_kernel(stats):
     """The kernel that runs most fused passes: the register pass, or the
     tensor pass of 8x8 stages, of 16x16 stages on mma.sync, or on tcgen05."""
@@ -635,6 +647,15 @@ def main_batch(args, dist):
     peak, peak_kind = hbm_peak()
     achieved = info["pass_bytes"] / sec / 1e9
     nparams = info["parameters"]
+    # the kernel that runs most passes: the batched 8x8 tensor pass or the batched register pass
+    tensor_major = info["tensor_passes"] * 2 >= info["passes"]
+    batch_kernel = "tensor3_pass_kernel (batched, 8x8 stages)" if tensor_major else "fused_pass_kernel (batched)"
+    batch_traffic = None
+    if tensor_major:
+        per_amp = batch_traffic_per_amplitude()
+        if per_amp is not None:
+            # the measured fraction of the algorithmic bytes (complex64: 16 per amplitude and pass)
+            batch_traffic = info["pass_bytes"] * per_amp / 16.0
     alg = sum(C.algorithmic_bytes(c, w, precision // 8) for w, c in zip(widths, circs))
     cpu, accuracy = None, None
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
@@ -660,11 +681,13 @@ def main_batch(args, dist):
         "e2e": {"value": e2e_total / args.steps / WORLD, "unit": "s", "h2d_bytes_per_step": nparams * 8,
                 "d2h_bytes_per_step": sum(widths) * 8},
         "gpu_launches": info["launches_per_run"],
-        "roofline": {"bound": "hbm", "kernel": "fused_pass_kernel (batched)", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": batch_kernel, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": f"{peak_kind} (copy, MEASURED_PEAKS hbm_gbs)" if peak_kind == "measured" else "fallback",
-                     "traffic": None, "note": "pass bytes over the whole run's device time (graph: entries in, "
-                                              "passes, <Z>, results out)"},
+                     "traffic": batch_traffic,
+                     "note": "pass bytes over the whole run's device time (graph: entries in, stage matrices, "
+                             "passes, <Z>, results out); traffic = DRAM bytes per run, the pass bytes scaled by "
+                             "the measured bytes per amplitude of profiles/tensor3_pass_kernel_batch_traffic.txt"},
         "batch": {"groups": info["groups"], "passes": info["passes"], "tensor_passes": info["tensor_passes"],
                   "pass_bytes": info["pass_bytes"],
                   "setup_s": setup_s, "step_s": dev},
