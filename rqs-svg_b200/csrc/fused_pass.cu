@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
         for (int nu = 0; nu < 8; ++nu)
         {
             const V y = a[reg((nu >> 1) + 4 * (nu & 1))];
-            const double parts[3] = {y.x, y.y, y.x + y.y};
+            const double parts[3] = {y.x, y.y - y.x, -(y.x + y.y)};
             const int lane = nu * 4 + t;
 #pragma unroll
             for (int part = 0; part < 3; ++part)
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
             for (int g = 0; g < 8; ++g)
             {
                 const V y = a[reg(8 * i + (g >> 1) + 4 * (g & 1))];
-                const double parts[3] = {y.x, y.y, y.x + y.y};
+                const double parts[3] = {y.x, y.y - y.x, -(y.x + y.y)};
                 const int lane = g * 4 + t;
 #pragma unroll
                 for (int part = 0; part < 3; ++part)
@@ -261,8 +261,8 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
             const V y = a[reg(8 * i + (g >> 1) + 4 * (g & 1))];
             const int lane = g * 4 + t;
             out[((0 * 4 + j * 2 + i) * 32 + lane) * 2 + b] = y.x;
-            out[((1 * 4 + j * 2 + i) * 32 + lane) * 2 + b] = y.y;
-            out[((2 * 4 + j * 2 + i) * 32 + lane) * 2 + b] = y.x + y.y;
+            out[((1 * 4 + j * 2 + i) * 32 + lane) * 2 + b] = y.y - y.x;
+            out[((2 * 4 + j * 2 + i) * 32 + lane) * 2 + b] = -(y.x + y.y);
         }
 }
 

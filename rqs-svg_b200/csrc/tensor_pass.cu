@@ -14,11 +14,14 @@
 // FP64 from the pass's ops before the pass (stage_matrix_kernel).
 //
 // Product layout. A warp takes 16 groups (rows r) at a time: y_r = M x_r for
-// all 16 rows, with M = Mr + i Mi, in three real products (Gauss):
-// T1 = Mr Re(x), T2 = Mi Im(x), T3 = (Mr + Mi)(Re x + Im x), then
-// Re y = T1 - T2 and Im y = T3 - T1 - T2: twelve m16n8k8 products per 16
-// rows (K = 16 input slots in two k-steps, N = 16 output slots in two
-// n-tiles) instead of the sixteen of the four-product form. Lane (g, t) of
+// all 16 rows, with M = Mr + i Mi, in three real products (a three-
+// multiplication form of the complex product): K1 = Mr (Re x + Im x), then
+// Re y = K1 + B2 Im x and Im y = K1 + B1 Re x with B1 = Mi - Mr and
+// B2 = -(Mr + Mi) (the builder stores B0 = Mr, B1 and B2), the last two
+// accumulated onto a copy of K1 by the tensor cores, so no addition follows
+// the products: twelve m16n8k8 products per 16 rows (K = 16 input slots in
+// two k-steps, N = 16 output slots in two n-tiles) instead of the sixteen of
+// the four-product form. Lane (g, t) of
 // the warp (g = lane / 4, t = lane % 4) holds rows g and g + 8 at input
 // slots t, t + 4, t + 8, t + 12 for the A fragments; output column
 // nu = 8i + 2t + e of n-tile i stands for output slot 8i + t + 4e, so the
@@ -27,7 +30,7 @@
 // without barriers between the warp's tiles.
 //
 // complex128: 48 FP64 multiply-adds per amplitude and stage on the tensor
-// pipe plus 4 additions (the register path: 8 multiply-adds per complex 2x2
+// pipe plus one addition (Re x + Im x) (the register path: 8 multiply-adds per complex 2x2
 // gate), at the FP64 tensor rate, which on B200 equals the FMA rate, but
 // with one instruction per 1024 multiply-adds instead of 32.
 //
@@ -299,18 +302,22 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor_ctas_per_sm<Real>
 #pragma unroll
                 for (int i = 0; i < 2; ++i)
                 {
-                    Real t1[4] = {0, 0, 0, 0}, t2[4] = {0, 0, 0, 0}, t3[4] = {0, 0, 0, 0};
+                    // K1 = B0 (Re x + Im x); Re y = K1 + B2 Im x; Im y = K1 + B1 Re x
+                    Real k1[4] = {0, 0, 0, 0};
+#pragma unroll
+                    for (int j = 0; j < 2; ++j)
+                        TT::mma(k1, as[j], __ldg(w + (0 * 4 + j * 2 + i) * 32));
+                    Real yr[4] = {k1[0], k1[1], k1[2], k1[3]}, yi[4] = {k1[0], k1[1], k1[2], k1[3]};
 #pragma unroll
                     for (int j = 0; j < 2; ++j)
                     {
-                        TT::mma(t1, ar[j], __ldg(w + (0 * 4 + j * 2 + i) * 32));
-                        TT::mma(t2, ai[j], __ldg(w + (1 * 4 + j * 2 + i) * 32));
-                        TT::mma(t3, as[j], __ldg(w + (2 * 4 + j * 2 + i) * 32));
+                        TT::mma(yr, ai[j], __ldg(w + (2 * 4 + j * 2 + i) * 32));
+                        TT::mma(yi, ar[j], __ldg(w + (1 * 4 + j * 2 + i) * 32));
                     }
                     // e = 0: row g, slot t + 8i; 1: row g, slot t + 8i + 4; 2, 3: row g + 8
 #pragma unroll
                     for (int e = 0; e < 4; ++e)
-                        sb[pos(e >> 1, 2 * i + (e & 1))] = V{t1[e] - t2[e], t3[e] - (t1[e] + t2[e])};
+                        sb[pos(e >> 1, 2 * i + (e & 1))] = V{yr[e], yi[e]};
                 }
             }
             __syncthreads();
@@ -330,7 +337,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor_ctas_per_sm<Real>
 // rows (8-amplitude groups) at a time: lane (g, t) holds rows g and g + 8 at
 // input slots t and t + 4 (one k-step), and output column nu = 2t + e of the
 // single n-tile stands for output slot t + 4e, so the lane stores to the
-// positions it loaded. Three m16n8k8 products per 16 rows (Gauss, as above):
+// positions it loaded. Three m16n8k8 products per 16 rows (as above):
 // 24 multiply-adds per amplitude and stage, half those of a 16 x 16 stage
 // for three quarters of its qubits. 256 rows per chunk: 16 tiles, four per
 // warp; group bits 4..7 pick the tile.
@@ -470,12 +477,20 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
             const uint32_t lane_pos = ((g & 1) ? gbit[0] : 0u) ^ ((g & 2) ? gbit[1] : 0u) ^
                                       ((g & 4) ? gbit[2] : 0u) ^ ((t & 1) ? sbit[0] : 0u) ^ ((t & 2) ? sbit[1] : 0u);
             const uint32_t hpos = gbit[3];
+            // the stage's matrix of tile mt: local condition bits from the
+            // tile, chunk condition bits from the chunk (once per stage)
+            const TStage &S = p.stages[st];
+            uint32_t vc = 0;
+            for (int i = 0; i < S.ngc; ++i)
+                vc |= static_cast<uint32_t>((cbase >> S.gq[i]) & 1) << i;
+            const uint32_t vlo = (1u << S.nlc) - 1u, vhi = vc << S.nlc;
+            const uint64_t creg = cbase >> p.n;
 #pragma unroll
             for (int mt = 0; mt < 4; ++mt)
             {
                 const uint32_t tile = static_cast<uint32_t>(mt | (warp << 2));
-                const uint32_t v = matrix_of(st, cbase, mt);
-                if (bf_st != st || bf_v != v || bf_reg != (cbase >> p.n))
+                const uint32_t v = (tile & vlo) | vhi;
+                if (bf_st != st || bf_v != v || bf_reg != creg)
                     fetch(st, v, cbase);
                 const uint32_t base = lane_pos ^ ((tile & 1) ? gbit[4] : 0u) ^ ((tile & 2) ? gbit[5] : 0u) ^
                                       ((tile & 4) ? gbit[6] : 0u) ^ ((tile & 8) ? gbit[7] : 0u);
@@ -485,14 +500,16 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
                 const typename TT::AFrag ai = TT::afrag(x00.y, x10.y, x01.y, x11.y);
                 const typename TT::AFrag as =
                     TT::afrag(x00.x + x00.y, x10.x + x10.y, x01.x + x01.y, x11.x + x11.y);
-                Real t1[4] = {0, 0, 0, 0}, t2[4] = {0, 0, 0, 0}, t3[4] = {0, 0, 0, 0};
-                TT::mma(t1, ar, bf[0]);
-                TT::mma(t2, ai, bf[1]);
-                TT::mma(t3, as, bf[2]);
+                // K1 = B0 (Re x + Im x); Re y = K1 + B2 Im x; Im y = K1 + B1 Re x
+                Real k1[4] = {0, 0, 0, 0};
+                TT::mma(k1, as, bf[0]);
+                Real yr[4] = {k1[0], k1[1], k1[2], k1[3]}, yi[4] = {k1[0], k1[1], k1[2], k1[3]};
+                TT::mma(yr, ai, bf[2]);
+                TT::mma(yi, ar, bf[1]);
                 // e = 0: row g, slot t; 1: row g, slot t + 4; 2, 3: row g + 8
 #pragma unroll
                 for (int e = 0; e < 4; ++e)
-                    sb[pos(e >> 1, e & 1)] = V{t1[e] - t2[e], t3[e] - (t1[e] + t2[e])};
+                    sb[pos(e >> 1, e & 1)] = V{yr[e], yi[e]};
             }
             if (st + 1 < p.nstages)
                 fetch(st + 1, matrix_of(st + 1, cbase, 0), cbase);
@@ -708,13 +725,15 @@ double tensor_pass_cost(const TPassParams &tp, int amp_bytes)
     // an 8 x 8 stage: half the tensor-core work of a 16 x 16 one and the
     // same shared-memory round trip; measured on the 30-qubit layered and
     // matching circuits: 0.63 of a 16 x 16 stage for complex128, 0.93 for
-    // complex64 (whose stages are not bound by the tensor pipe)
+    // complex64 (whose stages are not bound by the tensor pipe). complex128
+    // stages lost 10% of their time when the additions after the products
+    // went into the tensor cores' accumulation (the factors below)
     if (tp.width == 3)
-        return (amp_bytes == 8 ? 28.0 : 52.0) * tp.nstages;
+        return (amp_bytes == 8 ? 28.0 : 47.0) * tp.nstages;
     // tcgen05 16 x 16 stages (complex64): measured 1% below mma.sync ones
     if (tp.umma)
         return 29.0 * tp.nstages;
-    return (amp_bytes == 8 ? 30.0 : 82.0) * tp.nstages;
+    return (amp_bytes == 8 ? 30.0 : 74.0) * tp.nstages;
 }
 
 template <typename R>
