@@ -1514,10 +1514,10 @@ void choose_execution(const std::vector<GateOp> &q, const PlannedPass &pp, int n
                       size_t before, int engine)
 {
     out = PassChoice();
-    // automatic mode: registers below kTensorMinQubits fit in L2 and their
-    // passes are bound by launch latency, where a tensor pass's extra launch
-    // (the matrix build) and second planning cost more than they save
-    if (tensor_mode == 1 && n < kTensorMinQubits)
+    // automatic mode: below tensor_min_qubits a register pass's chunks fit
+    // one wave of CTAs, and a tensor pass's extra launch (the matrix build)
+    // costs more than its stages save
+    if (tensor_mode == 1 && n < tensor_min_qubits(amp_bytes))
         tensor_mode = 0;
     double cost4 = 0.0;
     for (size_t i = before; i < params.size(); ++i)
@@ -1724,7 +1724,7 @@ std::vector<Segment> plan_learned(const std::vector<GateOp> &q, const std::vecto
     std::vector<Segment> out;
     *predicted_greedy = *predicted_learned = 0.0;
     const double amps_ns = std::ldexp(1.0, n);
-    const bool tensor_ok = tensor_mode != 0 && !(tensor_mode == 1 && n < kTensorMinQubits);
+    const bool tensor_ok = tensor_mode != 0 && !(tensor_mode == 1 && n < tensor_min_qubits(amp_bytes));
     size_t gi = 0;
     while (gi < greedy.size())
     {

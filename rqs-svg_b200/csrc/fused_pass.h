@@ -33,7 +33,15 @@ struct StageCond
 // the GPU from the pass's ops (stage_matrix_kernel) and applied to every
 // 16-amplitude group of the stage by warp-level MMAs.
 constexpr int kTensorLocal = 11;       // local qubits of a tensor pass (2^11-amplitude chunks)
-constexpr int kTensorMinQubits = 24;   // automatic mode: smaller registers stay on the register path
+// Automatic mode: smaller registers stay on the register path. Measured on
+// B200 (layered, CZ-layered and matching-CX circuits, complex128, and HEA
+// complex64, device time per flush): tensor passes are 20-36% slower at
+// 16-19 qubits, where the register pass's chunks fit one wave of CTAs and
+// a tensor pass adds the matrix build; 5-7% faster at 20 qubits (16% slower
+// for complex64 HEA), 15-52% faster at 21-23.
+constexpr int kTensorMinQubits = 20;      // complex128
+constexpr int kTensorMinQubitsC64 = 21;   // complex64
+inline int tensor_min_qubits(int amp_bytes) { return amp_bytes == 8 ? kTensorMinQubitsC64 : kTensorMinQubits; }
 constexpr int kTensorTileBits = 3;     // group bits that pick a warp's tiles: local condition bits go there
 constexpr int kTensorMaxCond = 8;      // condition bits of a stage: at most 2^8 matrices
 constexpr int kTensorMaxMats = 4096;   // matrices of one pass

@@ -48,6 +48,17 @@ int env_fusion_mode()
     return m;
 }
 
+// QCS_TENSOR_PASSES: the tensor-pass mode of new simulators (0-3; unset or
+// out of range: 1, automatic)
+int env_tensor_mode()
+{
+    const char *e = std::getenv("QCS_TENSOR_PASSES");
+    if (e == nullptr || e[0] == '\0')
+        return 1;
+    const int m = std::atoi(e);
+    return (m >= 0 && m <= 3) ? m : 1;
+}
+
 } // namespace
 
 Simulator::Simulator()
@@ -59,6 +70,7 @@ Simulator::Simulator()
     std::random_device rd;
     set_seed(rd());
     fusion_mode_ = env_fusion_mode();
+    opt_tensor_ = env_tensor_mode();
 }
 
 Simulator::~Simulator()
