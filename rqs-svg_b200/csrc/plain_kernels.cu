@@ -311,6 +311,8 @@ struct ProbParams
     double2 *partials;
     double2 *result;      // final (P0, P1); may be mapped host memory
     unsigned *ticket;     // zero between calls
+    volatile unsigned *done;   // host-mapped: set to seq once result is written (or null)
+    unsigned seq;
 };
 
 // Fixed-order sum of count double2 partials by one block of kThreads threads
@@ -390,6 +392,12 @@ __global__ void __launch_bounds__(kThreads) measure_probs_kernel(const __grid_co
     {
         *p.result = total;
         *p.ticket = 0;
+        if (p.done != nullptr)
+        {
+            // the result reaches host memory before the flag does
+            __threadfence_system();
+            *p.done = p.seq;
+        }
     }
 }
 
@@ -716,7 +724,8 @@ int launch_set_amplitude(typename Cx<R>::T *state, uint64_t index, double re, do
 
 template <typename R>
 int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t cmask, uint64_t cval,
-                         double2 *partials, double2 *result, unsigned *ticket, cudaStream_t stream)
+                         double2 *partials, double2 *result, unsigned *ticket, unsigned *done, unsigned seq,
+                         cudaStream_t stream)
 {
     ProbParams<R> p;
     std::memset(&p, 0, sizeof(p));
@@ -732,6 +741,8 @@ int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t 
     p.partials = partials;
     p.result = result;
     p.ticket = ticket;
+    p.done = done;
+    p.seq = seq;
     // A fixed grid (independent of n) keeps the partial count constant.
     measure_probs_kernel<R><<<kReduceBlocks, kThreads, 0, stream>>>(p);
     QCSB_CUDA(cudaGetLastError());
@@ -838,7 +849,7 @@ int launch_narrow(const double2 *in, uint64_t count, typename Cx<R>::T *out, cud
     template int launch_set_amplitude<R>(Cx<R>::T *, uint64_t, double, double, cudaStream_t);                      \
     template int launch_rescale<R>(Cx<R>::T *, int, double, const double *, cudaStream_t);                          \
     template int launch_measure_probs<R>(const Cx<R>::T *, int, int, uint64_t, uint64_t, double2 *, double2 *,      \
-                                         unsigned *, cudaStream_t);                                                 \
+                                         unsigned *, unsigned *, unsigned, cudaStream_t);                           \
     template int launch_collapse<R>(Cx<R>::T *, int, int, int, cudaStream_t);                                       \
     template int launch_collapse_mask<R>(Cx<R>::T *, int, uint64_t, uint64_t, cudaStream_t);                        \
     template int launch_zsums<R>(const Cx<R>::T *, int, double *, double *, cudaStream_t);                          \

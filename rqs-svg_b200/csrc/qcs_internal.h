@@ -122,11 +122,14 @@ int launch_rescale(typename Cx<R>::T *state, int n, double target, const double 
 // (index & cmask) == cval, in one launch. partials must hold kReduceBlocks
 // double2; result receives one double2 (device memory, or pinned host memory
 // the device can write); ticket is a device counter that must be zero before
-// the call and is zero again after it.
+// the call and is zero again after it. done (pinned host memory, or null)
+// receives seq after result has been written, so that the host can wait
+// for the result without synchronising the stream.
 constexpr int kReduceBlocks = 592;   // 4 x 148 SMs
 template <typename R>
 int launch_measure_probs(const typename Cx<R>::T *state, int n, int t, uint64_t cmask, uint64_t cval,
-                         double2 *partials, double2 *result, unsigned *ticket, cudaStream_t stream);
+                         double2 *partials, double2 *result, unsigned *ticket, unsigned *done, unsigned seq,
+                         cudaStream_t stream);
 
 // Zero every amplitude whose bit t differs from keep_value.
 template <typename R>

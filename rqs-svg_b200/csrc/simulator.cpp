@@ -15,6 +15,8 @@
 #include "simulator.h"
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -34,6 +36,8 @@ namespace
 
 constexpr uint64_t kStagingAmps = 1ull << 22;   // 64 MiB per staging buffer
 constexpr size_t kScratchReserve = 256ull << 20;
+constexpr size_t kMeasureFlagOffset = 16;   // in the measurement's pinned buffer, after the (P0, P1) result
+constexpr size_t kMeasureHostBytes = 64;
 
 bool contains(const std::vector<int> &v, int x) { return std::find(v.begin(), v.end(), x) != v.end(); }
 
@@ -161,6 +165,11 @@ void Simulator::allocate_memory()
     QCSB_CUDA(cudaMalloc(&zsum_result_, sizeof(double) * (kMaxQubits + 1)));
     host_pinned_bytes_ = 1 << 16;
     QCSB_CUDA(cudaMallocHost(&host_pinned_, host_pinned_bytes_));
+    // the measurement's result and completion flag: written only by the
+    // measurement kernel
+    QCSB_CUDA(cudaMallocHost(&meas_host_, kMeasureHostBytes));
+    *reinterpret_cast<unsigned *>(static_cast<char *>(meas_host_) + kMeasureFlagOffset) = 0;
+    measure_seq_ = 0;
     fused_ = new FusedExecutor(stream_);
     fused_->set_options(opt_max_ops_, opt_local_bits_);
     fused_->set_tensor_mode(opt_tensor_);
@@ -237,6 +246,9 @@ void Simulator::dispose()
     sampler_bytes_ = 0;
     if (host_pinned_)
         cudaFreeHost(host_pinned_);
+    if (meas_host_)
+        cudaFreeHost(meas_host_);
+    meas_host_ = nullptr;
     if (staging_host_)
         cudaFreeHost(staging_host_);
     state_ = nullptr;
@@ -500,10 +512,24 @@ int Simulator::measure(int q)
         cval |= 1ull << perm_l2p_[m];
     }
     const int t = perm_l2p_[q];
-    // (P0, P1) lands directly in pinned host memory
-    double2 *h = static_cast<double2 *>(host_pinned_);
-    stats.kernel_launches += QCSB_ON_STATE(launch_measure_probs, n_, t, cmask, cval, red_partials_, h, red_ticket_, stream_);
-    QCSB_CUDA(cudaStreamSynchronize(stream_));
+    // (P0, P1) lands directly in pinned host memory, followed by a sequence
+    // number the host spins on (a stream synchronisation costs a few
+    // microseconds more per measurement); past 500 us of spinning it
+    // synchronises the stream instead, which also reports any error
+    double2 *h = static_cast<double2 *>(meas_host_);
+    unsigned *done = reinterpret_cast<unsigned *>(static_cast<char *>(meas_host_) + kMeasureFlagOffset);
+    const unsigned seq = ++measure_seq_;
+    stats.kernel_launches += QCSB_ON_STATE(launch_measure_probs, n_, t, cmask, cval, red_partials_, h, red_ticket_,
+                                           done, seq, stream_);
+    const volatile unsigned *flag = done;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned i = 0; *flag != seq; ++i)
+        if ((i & 255u) == 255u && std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(500))
+        {
+            QCSB_CUDA(cudaStreamSynchronize(stream_));
+            break;
+        }
+    std::atomic_thread_fence(std::memory_order_acquire);
     fused_->check_device_error();
     const double p0 = h->x, p1 = h->y;
     const double sum = p0 + p1;

@@ -178,6 +178,8 @@ class Simulator
     double *zsum_result_ = nullptr;
     void *host_pinned_ = nullptr;
     size_t host_pinned_bytes_ = 0;
+    void *meas_host_ = nullptr;   // pinned: (P0, P1) and the completion flag of a measurement
+    unsigned measure_seq_ = 0;    // sequence number of the last measurement's completion flag
     double2 *staging_dev_ = nullptr;
     double2 *staging_host_ = nullptr;
     uint64_t staging_count_ = 0;
