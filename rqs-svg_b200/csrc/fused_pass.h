@@ -42,7 +42,10 @@ constexpr int kTensorLocal = 11;       // local qubits of a tensor pass (2^11-am
 constexpr int kTensorMinQubits = 20;      // complex128
 constexpr int kTensorMinQubitsC64 = 21;   // complex64
 inline int tensor_min_qubits(int amp_bytes) { return amp_bytes == 8 ? kTensorMinQubitsC64 : kTensorMinQubits; }
-constexpr int kTensorTileBits = 3;     // group bits that pick a warp's tiles: local condition bits go there
+// Group bits that number a chunk's tiles (tile = warp + 4 x the warp's own
+// tile index): local condition bits go to the lowest ones, the warp bits,
+// so that with at most two of them every tile of a warp uses one matrix.
+constexpr int kTensorTileBits = 3;
 constexpr int kTensorMaxCond = 8;      // condition bits of a stage: at most 2^8 matrices
 constexpr int kTensorMaxMats = 4096;   // matrices of one pass
 // Per matrix: the B fragments of the m16n8k8 products, 12 fragments (real
@@ -52,7 +55,8 @@ constexpr int kTensorMaxMats = 4096;   // matrices of one pass
 constexpr int kTensorFragments = 12;
 // 8 x 8 stages (three slot bits): one k-step and one n-tile, 3 fragments
 // (1.5 KiB) per matrix; 256 rows per chunk in 16 tiles, four per warp, so up
-// to four local condition bits pick a tile's matrix.
+// to four local condition bits pick a tile's matrix (the first two from the
+// warp, the others from the warp's tile).
 constexpr int kTensor3Fragments = 3;
 constexpr int kTensor3TileBits = 4;
 

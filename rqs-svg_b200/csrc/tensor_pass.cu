@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor_ctas_per_sm<Real>
         uint32_t vc = 0;
         for (int i = 0; i < S.ngc; ++i)
             vc |= static_cast<uint32_t>((cb >> S.gq[i]) & 1) << i;
-        const uint32_t tile = static_cast<uint32_t>(mt | (warp << 1));
+        const uint32_t tile = static_cast<uint32_t>(warp | (mt << 2));
         return (tile & ((1u << S.nlc) - 1u)) | (vc << S.nlc);
     };
 
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor_ctas_per_sm<Real>
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt)
             {
-                const uint32_t tile = static_cast<uint32_t>(mt | (warp << 1));
+                const uint32_t tile = static_cast<uint32_t>(warp | (mt << 2));
                 const uint32_t v = matrix_of(st, cbase, mt);
                 const Frag *w = mats + (static_cast<size_t>(S.woff + v) * kTensorFragments) * 32 + lane;
                 const uint32_t base = lane_pos ^ ((tile & 1) ? gbit[4] : 0u) ^ ((tile & 2) ? gbit[5] : 0u) ^
@@ -340,7 +340,10 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor_ctas_per_sm<Real>
 // positions it loaded. Three m16n8k8 products per 16 rows (as above):
 // 24 multiply-adds per amplitude and stage, half those of a 16 x 16 stage
 // for three quarters of its qubits. 256 rows per chunk: 16 tiles, four per
-// warp; group bits 4..7 pick the tile.
+// warp; group bits 4..7 pick the tile, warp + 4 x the warp's tile index (the
+// stage's local condition bits are the lowest group bits, so with at most
+// two of them a warp runs all its tiles with one matrix, fetched before the
+// stage begins).
 // CTAs per SM of the single-buffered 8 x 8 pass: six for complex128 (80
 // registers; 6 x 32 KiB of chunk), eight for complex64 (64 registers); each
 // step from four measured faster (30-qubit layered and matching complex128:
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
         uint32_t vc = 0;
         for (int i = 0; i < S.ngc; ++i)
             vc |= static_cast<uint32_t>((cb >> S.gq[i]) & 1) << i;
-        const uint32_t tile = static_cast<uint32_t>(mt | (warp << 2));
+        const uint32_t tile = static_cast<uint32_t>(warp | (mt << 2));
         return (tile & ((1u << S.nlc) - 1u)) | (vc << S.nlc);
     };
     auto fetch = [&](int st, uint32_t v, uint64_t cb) {
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(kThreads, NBUF == 1 ? tensor3_ctas_per_sm<Real
 #pragma unroll
             for (int mt = 0; mt < 4; ++mt)
             {
-                const uint32_t tile = static_cast<uint32_t>(mt | (warp << 2));
+                const uint32_t tile = static_cast<uint32_t>(warp | (mt << 2));
                 const uint32_t v = (tile & vlo) | vhi;
                 if (bf_st != st || bf_v != v || bf_reg != creg)
                     fetch(st, v, cbase);
