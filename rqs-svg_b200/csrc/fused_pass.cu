@@ -68,8 +68,8 @@ __global__ void __launch_bounds__(64) stage_matrix_kernel(const __grid_constant_
     const int col = static_cast<int>(gid & ((1u << width) - 1u));
     if (mat >= tb.nmats)
         return;
-    // batched passes: register blockIdx.y, its entries and its matrices
-    const uint32_t breg = blockIdx.y;
+    // batched passes: register reg0 + blockIdx.y, its entries and its matrices
+    const uint32_t breg = tb.reg0 + blockIdx.y;
     const void *blk = tb.regs > 0 ? static_cast<const void *>(p.mats + static_cast<size_t>(breg) * p.mat_stride) : nullptr;
     const BuildEntries<V> ent{p, blk, tb.batch_float, 0u};
     const uint32_t omat = tb.regs > 0 ? breg * tb.nmats + mat : mat;   // matrix slot written
@@ -273,12 +273,26 @@ int launch_stage_matrices(const FPassParams &prm, const TBuildParams &tb, cudaSt
 {
     const unsigned threads = 64;
     const unsigned blocks = static_cast<unsigned>((static_cast<uint64_t>(tb.nmats) * (1u << tb.width) + threads - 1) / threads);
-    if (tb.regs > 0 && (tb.width != 3 || tb.umma || tb.regs > 65535u))
-        throw std::runtime_error("internal: batched stage matrices need 8 x 8 stages and at most 65535 registers");
-    const dim3 grid(blocks, tb.regs > 0 ? tb.regs : 1u);
-    stage_matrix_kernel<R><<<grid, threads, 0, stream>>>(prm, tb);
-    QCSB_CUDA(cudaGetLastError());
-    return 1;
+    if (tb.regs == 0)
+    {
+        stage_matrix_kernel<R><<<blocks, threads, 0, stream>>>(prm, tb);
+        QCSB_CUDA(cudaGetLastError());
+        return 1;
+    }
+    if (tb.width != 3 || tb.umma)
+        throw std::runtime_error("internal: batched stage matrices need 8 x 8 stages");
+    // registers in slices of at most 65535 (the grid's y limit)
+    int launches = 0;
+    TBuildParams slice = tb;
+    for (uint32_t r0 = 0; r0 < tb.regs; r0 += 65535u)
+    {
+        slice.reg0 = r0;
+        const dim3 grid(blocks, std::min<uint32_t>(tb.regs - r0, 65535u));
+        stage_matrix_kernel<R><<<grid, threads, 0, stream>>>(prm, slice);
+        QCSB_CUDA(cudaGetLastError());
+        ++launches;
+    }
+    return launches;
 }
 template int launch_stage_matrices<double>(const FPassParams &, const TBuildParams &, cudaStream_t);
 

@@ -100,6 +100,7 @@ struct TBuildParams
     // batch_float) and writes its nmats matrices after those of r - 1
     uint32_t regs;
     int batch_float;
+    uint32_t reg0;               // first register of this launch (grid.y covers at most 65535)
     TStage stages[kFusedMaxStages];
 };
 // bytes of the matrix buffer per matrix, either format
