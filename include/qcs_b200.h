@@ -106,6 +106,19 @@ int qcs_simulator_sample(qcs_simulator *sim, uint32_t num_shots, uint64_t *bitst
 int qcs_simulator_get_amplitudes(qcs_simulator *sim, const uint64_t *indices, uint64_t count, double *amplitudes);
 
 /*
+ * The register on the device, in logical order, for zero-copy use by other
+ * GPU code: queued gates run first; if uncontrolled SWAPs (which only
+ * relabel qubits in the fused modes) or a mapping left physical qubits out
+ * of logical order, the amplitudes are moved in place so that physical qubit
+ * q holds logical qubit q (physical SWAPs through fused passes, at most
+ * n - 1 of them packed a few per pass); then the stream is synchronised.
+ * *state receives the device pointer: 2^n amplitudes, (re, im) interleaved,
+ * double (amplitude_bits 128) or float (64). Valid until the next call that
+ * changes the simulator; writes through it are seen by later calls.
+ */
+int qcs_simulator_get_device_state(qcs_simulator *sim, void **state, int *amplitude_bits);
+
+/*
  * Compare two registers of the same size on the same device, either
  * precision: <a|b> = sum over logical indices i of conj(a_i) b_i, max_i
  * |a_i - b_i|, and the squared norms <a|a>, <b|b> (FP64 accumulation, one

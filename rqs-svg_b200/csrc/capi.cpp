@@ -754,6 +754,17 @@ extern "C" int qcs_simulator_get_amplitudes(qcs_simulator *sim, const uint64_t *
     return guarded([&] { core(sim).get_amplitudes(indices, count, amplitudes); });
 }
 
+extern "C" int qcs_simulator_get_device_state(qcs_simulator *sim, void **state, int *amplitude_bits)
+{
+    return guarded([&] {
+        if (state == nullptr || amplitude_bits == nullptr)
+            throw std::runtime_error("result pointer must not be NULL");
+        void *p = core(sim).device_state_in_logical_order();
+        *state = p;
+        *amplitude_bits = core(sim).precision();
+    });
+}
+
 extern "C" int qcs_simulator_compare(qcs_simulator *a, qcs_simulator *b, double *overlap_re, double *overlap_im,
                                      double *max_abs_diff, double *norm_a, double *norm_b)
 {

@@ -558,6 +558,42 @@ int Simulator::measure(int q)
     return result;
 }
 
+void *Simulator::device_state_in_logical_order()
+{
+    require_allocated("get_device_state");
+    // Cycle by cycle: logical q, held at physical p, swaps places with
+    // whatever physical q holds; every swap puts at least one qubit home, so
+    // at most n - 1 swaps, which the fused planner packs into passes (a
+    // pass exchanges any of its local qubits in registers and shared memory)
+    const GateMatrix swap = gate_matrix("swap", nullptr, 0);
+    for (int q = 0; q < n_; ++q)
+    {
+        const int p = perm_l2p_[q];
+        if (p == q)
+            continue;
+        const int r = perm_p2l_[q];   // the logical qubit physical q holds
+        const int tq[kMaxTargets] = {q, p, 0, 0};
+        const GateOp op = make_gate_op(swap, tq, 0, 0);
+        if (fusion_mode_ == QCS_FUSION_PLAIN)
+        {
+            const int k = QCSB_ON_STATE(launch_gate_plain, n_, op, stream_);
+            stats.kernel_launches += k;
+            stats.plain_gate_kernels += k;
+        }
+        else
+        {
+            pending_.push_back(op);
+            ++pending_gates_;
+        }
+        perm_l2p_[q] = q;
+        perm_p2l_[q] = q;
+        perm_l2p_[r] = p;
+        perm_p2l_[p] = r;
+    }
+    synchronize();
+    return state_;
+}
+
 void Simulator::reset_qubit(int q)
 {
     // reference qcs_simulator_reset_cxx, src/qcs.cu:3077-3081

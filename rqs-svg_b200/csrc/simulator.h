@@ -120,6 +120,11 @@ class Simulator
 
     void flush();
     void synchronize();
+    // Physically move the register's amplitudes so that physical qubit q
+    // holds logical qubit q (physical SWAPs through the fused passes: the
+    // in-HBM qubit permutation), then return the device pointer of the
+    // register in logical order, with the stream synchronised.
+    void *device_state_in_logical_order();
 
     void set_planner_options(int max_ops, int local_bits);
     void set_tensor_mode(int mode);

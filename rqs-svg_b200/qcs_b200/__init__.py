@@ -223,6 +223,7 @@ class Library:
             "qcs_simulator_get_amplitudes": [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint64,
                                              ctypes.POINTER(ctypes.c_double)],
             "qcs_simulator_compare": [_P, _P] + [ctypes.POINTER(ctypes.c_double)] * 5,
+            "qcs_simulator_get_device_state": [_P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int)],
             "qcs_b200_batch_create": [ctypes.POINTER(_P), ctypes.c_int],
             "qcs_b200_batch_destroy": [_P],
             "qcs_b200_batch_add_circuit": [_P, ctypes.c_int, ctypes.POINTER(BatchGate), ctypes.c_uint32,
@@ -405,6 +406,14 @@ class Simulator:
         self.lib.call("qcs_simulator_get_amplitudes", self.h, idx.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
                       idx.size, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         return out.view(np.complex128)
+
+    def device_state(self):
+        """(device pointer, amplitude bits) of the register in logical order
+        (the library first moves the amplitudes so that physical qubit q
+        holds logical qubit q)."""
+        ptr, bits = ctypes.c_void_p(), ctypes.c_int()
+        self.lib.call("qcs_simulator_get_device_state", self.h, ctypes.byref(ptr), ctypes.byref(bits))
+        return ptr.value, bits.value
 
     def compare(self, other: "Simulator") -> dict:
         """<self|other>, max |self_i - other_i|, both squared norms and the
