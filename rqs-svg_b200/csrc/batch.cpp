@@ -69,6 +69,8 @@ GateOp op_like(const GateOp &shape, const GateMatrix &g)
     return op;
 }
 
+constexpr size_t kBatchTensorMatsBytes = size_t(2) << 30;   // stage matrices of one batched tensor pass
+
 bool tune_enabled()
 {
     const char *e = std::getenv("QCS_BATCH_TUNE");
@@ -237,7 +239,11 @@ void Batch::plan_group(Group &g, int k, bool tensor)
                 p.prm = params3[i];
                 p.src = std::move(srcs3[i]);
                 p.tensor = make_tensor_params(p.prm, conds3[i], amp_bytes_, p.tp, p.tb, 3);
-                ok = p.tensor;
+                // every register's matrices of a pass live on the device at
+                // once: beyond kBatchTensorMatsBytes the pass stays on the
+                // register path
+                ok = p.tensor && static_cast<double>(p.tb.nmats) * kTensor3Fragments * 32 * 16 * g.members.size() <=
+                                     static_cast<double>(kBatchTensorMatsBytes);
             }
             if (ok)
             {

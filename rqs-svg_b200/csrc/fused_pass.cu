@@ -2412,7 +2412,11 @@ int FusedExecutor::run(void *state, int n, int amp_bytes, const std::vector<Gate
     }
     if (timed_flush)
         QCSB_CUDA(cudaEventRecord(judge_b_, stream_));
-    if (!timer.enabled && !timed_flush)
+    // plans whose parameter blocks would take much host memory (a flush of
+    // thousands of passes) are not kept
+    const size_t plan_bytes = plan->params.size() * sizeof(FPassParams) + plan->tparams.size() * sizeof(TPassParams) +
+                              plan->tbuild.size() * sizeof(TBuildParams) + plan->tables.size() * sizeof(double2);
+    if (!timer.enabled && !timed_flush && plan_bytes <= kKeptPlanBytes)
     {
         plan->queued = queued;
         plan->hash = hash;

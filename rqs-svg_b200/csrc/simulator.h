@@ -276,6 +276,7 @@ class FusedExecutor
                          int max_ops, int tag);
     int replay(FlushPlan &plan, void *state, qcs_b200_stats &stats, KernelTimer &timer);
     static constexpr size_t kKeptPlans = 8;
+    static constexpr size_t kKeptPlanBytes = size_t(64) << 20;   // host memory of one kept plan's launches
     std::vector<std::unique_ptr<FlushPlan>> plans_;
     size_t plans_next_ = 0;   // the slot the next kept plan replaces once all are used
 
