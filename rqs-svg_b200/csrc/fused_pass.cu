@@ -2158,23 +2158,36 @@ int FusedExecutor::launch_plan_step(FlushPlan &plan, long st, void *state, const
     {
         TPassParams &tp = plan.tparams[t];
         TBuildParams &tb = plan.tbuild[t];
-        if (tb.nmats > mats_cap_)
+        double2 *mats = nullptr;
+        bool build = true;
+        if (plan.mats != nullptr)
         {
-            // the old buffer may still be read by queued passes
-            QCSB_CUDA(cudaStreamSynchronize(stream_));
-            cudaFree(mats_dev_);
-            mats_dev_ = nullptr;
-            mats_cap_ = 0;
-            const size_t cap = std::max<size_t>(tb.nmats, 256);
-            QCSB_CUDA(cudaMalloc(&mats_dev_, cap * kTensorMatrixBytes));
-            mats_cap_ = cap;
+            // the plan's own matrices: built on its first replay, reused after
+            mats = reinterpret_cast<double2 *>(static_cast<char *>(plan.mats) + plan.mat_off[t]);
+            build = !plan.mats_built;
+        }
+        else
+        {
+            if (tb.nmats > mats_cap_)
+            {
+                // the old buffer may still be read by queued passes
+                QCSB_CUDA(cudaStreamSynchronize(stream_));
+                cudaFree(mats_dev_);
+                mats_dev_ = nullptr;
+                mats_cap_ = 0;
+                const size_t cap = std::max<size_t>(tb.nmats, 256);
+                QCSB_CUDA(cudaMalloc(&mats_dev_, cap * kTensorMatrixBytes));
+                mats_cap_ = cap;
+            }
+            mats = mats_dev_;
         }
         prm.state = state;
-        tb.out = mats_dev_;
-        tp.mats = mats_dev_;
+        tb.out = mats;
+        tp.mats = mats;
         tp.state = state;
         tp.err = err_dev_;
-        launches += launch_stage_matrices<double>(prm, tb, stream_);
+        if (build)
+            launches += launch_stage_matrices<double>(prm, tb, stream_);
         if (tp.umma)
             launches += launch_tc_pass(tp, stream_);
         else
@@ -2194,12 +2207,40 @@ int FusedExecutor::launch_plan_step(FlushPlan &plan, long st, void *state, const
     return launches;
 }
 
+// Bytes of one matrix of a tensor pass in its format: 8 x 8 mma.sync
+// fragments, 16 x 16 mma.sync fragments, or tcgen05 slabs (high and low).
+static size_t tensor_matrix_bytes(const TPassParams &tp)
+{
+    if (tp.umma)
+        return 2 * static_cast<size_t>(kUmmaSlab);
+    return static_cast<size_t>(tp.width == 3 ? kTensor3Fragments : kTensorFragments) * 32 * 16;
+}
+
 int FusedExecutor::replay(FlushPlan &plan, void *state, qcs_b200_stats &stats, KernelTimer &timer)
 {
+    if (plan.mats == nullptr && !plan.tparams.empty())
+    {
+        // first replay: give the plan its own matrices (256-byte aligned per
+        // pass) if they fit the budget; the builds below fill them
+        size_t total = 0;
+        plan.mat_off.assign(plan.tparams.size(), 0);
+        for (size_t t = 0; t < plan.tparams.size(); ++t)
+        {
+            plan.mat_off[t] = total;
+            total += (plan.tparams[t].nmats * tensor_matrix_bytes(plan.tparams[t]) + 255) & ~size_t(255);
+        }
+        if (total <= kKeptMatsBytes && cudaMalloc(&plan.mats, total) != cudaSuccess)
+        {
+            plan.mats = nullptr;
+            (void)cudaGetLastError();   // out of memory: keep building into the shared buffer
+        }
+    }
     const double2 *tables_dev = upload_tables(plan.tables);
     int launches = 0;
     for (long st : plan.steps)
         launches += launch_plan_step(plan, st, state, tables_dev, stats, timer, nullptr);
+    if (plan.mats != nullptr)
+        plan.mats_built = true;
     ++stats.replayed_flushes;
     return launches;
 }

@@ -267,7 +267,23 @@ class FusedExecutor
         std::vector<TBuildParams> tbuild;
         std::vector<long> steps;      // launch order: >= 0 a pass, < 0 plain op -1 - step
         std::vector<double2> tables;  // phase-run tables of the passes
+        // The tensor passes' stage matrices, kept on the device from the
+        // plan's first replay on (every tensor pass at its own offset), so
+        // that later replays launch no matrix builds. Freed with the plan
+        // (cudaFree waits for the kernels that may still read it).
+        void *mats = nullptr;
+        std::vector<size_t> mat_off;  // bytes, per tensor pass
+        bool mats_built = false;
+        FlushPlan() = default;
+        FlushPlan(const FlushPlan &) = delete;
+        FlushPlan &operator=(const FlushPlan &) = delete;
+        ~FlushPlan()
+        {
+            if (mats != nullptr)
+                cudaFree(mats);
+        }
     };
+    static constexpr size_t kKeptMatsBytes = size_t(256) << 20;   // device memory of one kept plan's matrices
     void settle_judge();
     const double2 *upload_tables(const std::vector<double2> &tables);
     int launch_plan_step(FlushPlan &plan, long st, void *state, const double2 *tables_dev, qcs_b200_stats &stats,

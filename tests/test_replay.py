@@ -46,8 +46,21 @@ def test_replayed_flush_equals_planned(gpu_lib, oracle_lib, case):
         sim.run(circ)
         second = sim.statevector()
         s2 = sim.stats()
+        # the plan's own stage matrices, built on its first replay, serve
+        # the later ones: no matrix builds from the second replay on
+        sim.set_state("zero")
+        sim.run(circ)
+        third = sim.statevector()
+        s3 = sim.stats()
     assert s1["replayed_flushes"] == 0
-    assert s2["replayed_flushes"] == 1
+    assert s2["replayed_flushes"] == 1 and s3["replayed_flushes"] == 2
+    launches2 = s2["kernel_launches"] - s1["kernel_launches"]
+    launches3 = s3["kernel_launches"] - s2["kernel_launches"]
+    if s1["tensor_passes"] > 0:
+        assert launches3 == launches2 - s1["tensor_passes"]
+    else:
+        assert launches3 == launches2
+    assert third.tobytes() == first.tobytes()
     # the same launches: the same passes of each kind, bit-identical results
     for key in ("fused_passes", "tensor_passes", "tensor8_passes", "tcgen05_passes", "plain_gate_kernels"):
         assert s2[key] == 2 * s1[key], key
