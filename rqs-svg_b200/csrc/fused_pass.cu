@@ -2229,10 +2229,16 @@ int FusedExecutor::replay(FlushPlan &plan, void *state, qcs_b200_stats &stats, K
             plan.mat_off[t] = total;
             total += (plan.tparams[t].nmats * tensor_matrix_bytes(plan.tparams[t]) + 255) & ~size_t(255);
         }
-        if (total <= kKeptMatsBytes && cudaMalloc(&plan.mats, total) != cudaSuccess)
+        // kept matrices are a cache: they are made only while 256 MiB stay
+        // free beside them, so that they never take the memory the
+        // register's own scratch (sampler, staging) would need later
+        size_t free_b = 0, total_b = 0;
+        const bool room = total <= kKeptMatsBytes && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+                          free_b >= total + kKeptMatsFreeReserve;
+        if (!room || cudaMalloc(&plan.mats, total) != cudaSuccess)
         {
             plan.mats = nullptr;
-            (void)cudaGetLastError();   // out of memory: keep building into the shared buffer
+            (void)cudaGetLastError();   // no room: keep building into the shared buffer
         }
     }
     const double2 *tables_dev = upload_tables(plan.tables);

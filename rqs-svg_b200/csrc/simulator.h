@@ -284,6 +284,7 @@ class FusedExecutor
         }
     };
     static constexpr size_t kKeptMatsBytes = size_t(256) << 20;   // device memory of one kept plan's matrices
+    static constexpr size_t kKeptMatsFreeReserve = size_t(256) << 20;   // left free beside kept matrices
     void settle_judge();
     const double2 *upload_tables(const std::vector<double2> &tables);
     int launch_plan_step(FlushPlan &plan, long st, void *state, const double2 *tables_dev, qcs_b200_stats &stats,
