@@ -1984,7 +1984,14 @@ FusedExecutor::FusedExecutor(cudaStream_t stream) : stream_(stream)
 {
     QCSB_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&err_host_), sizeof(int), cudaHostAllocMapped));
     *err_host_ = 0;
-    QCSB_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&err_dev_), err_host_, 0));
+    const cudaError_t e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&err_dev_), err_host_, 0);
+    if (e != cudaSuccess)
+    {
+        // a throwing constructor runs no destructor: free the flag here
+        cudaFreeHost(err_host_);
+        err_host_ = nullptr;
+        throw std::runtime_error(strformat("cudaHostGetDevicePointer: %s", cudaGetErrorString(e)));
+    }
 }
 
 void FusedExecutor::check_device_error()

@@ -150,32 +150,91 @@ void Simulator::allocate_memory()
     if (n > max_n)
         throw std::runtime_error(strformat("num_qubits(%d) > max_num_qubits_local_device(%d) + log_num_procs(0)", n, max_n));
     QCSB_CUDA(cudaGetDevice(&device_));
-    QCSB_CUDA(cudaMalloc(&state_, (size_t)amp_bytes_ << n));
-    n_ = n;
-    perm_p2l_.assign(n, 0);
-    perm_l2p_.assign(n, 0);
-    ref_l2p_.assign(n, 0);
-    for (int q = 0; q < n; ++q)
-        perm_p2l_[q] = perm_l2p_[q] = ref_l2p_[q] = q;
-    reinitialize_mapping();
-    QCSB_CUDA(cudaMalloc(&red_partials_, sizeof(double2) * kReduceBlocks));
-    QCSB_CUDA(cudaMalloc(&red_ticket_, sizeof(unsigned)));
-    QCSB_CUDA(cudaMemset(red_ticket_, 0, sizeof(unsigned)));
-    QCSB_CUDA(cudaMalloc(&zsum_partials_, sizeof(double) * 512 * (kMaxQubits + 1)));
-    QCSB_CUDA(cudaMalloc(&zsum_result_, sizeof(double) * (kMaxQubits + 1)));
-    host_pinned_bytes_ = 1 << 16;
-    QCSB_CUDA(cudaMallocHost(&host_pinned_, host_pinned_bytes_));
-    // the measurement's result and completion flag: written only by the
-    // measurement kernel
-    QCSB_CUDA(cudaMallocHost(&meas_host_, kMeasureHostBytes));
-    *reinterpret_cast<unsigned *>(static_cast<char *>(meas_host_) + kMeasureFlagOffset) = 0;
-    measure_seq_ = 0;
-    fused_ = new FusedExecutor(stream_);
-    fused_->set_options(opt_max_ops_, opt_local_bits_);
-    fused_->set_tensor_mode(opt_tensor_);
-    fused_->set_tensor_engine(opt_engine_);
-    fused_->set_cost_model(model_);
-    set_zero_state();
+    // A failure part way (device or pinned memory exhausted) releases what
+    // this call allocated and leaves the simulator unallocated: a later
+    // allocate_memory may retry, and every other call reports that
+    // allocate_memory must come first, so no kernel ever sees a missing
+    // buffer. QCS_FAIL_ALLOC_AFTER=k makes allocation k (counted from 0) of
+    // this call fail as if memory were exhausted, the host-side test hook
+    // of this path.
+    const char *fail_env = std::getenv("QCS_FAIL_ALLOC_AFTER");
+    const int fail_at = (fail_env != nullptr && fail_env[0] != '\0') ? std::atoi(fail_env) : -1;
+    int allocation = 0;
+    auto injected = [&](const char *what) {
+        if (allocation++ == fail_at)
+            throw std::runtime_error(strformat("allocate_memory: %s: injected failure of allocation %d (QCS_FAIL_ALLOC_AFTER)",
+                                               what, fail_at));
+    };
+    try
+    {
+        injected("cudaMalloc of the state");
+        QCSB_CUDA(cudaMalloc(&state_, (size_t)amp_bytes_ << n));
+        n_ = n;
+        perm_p2l_.assign(n, 0);
+        perm_l2p_.assign(n, 0);
+        ref_l2p_.assign(n, 0);
+        for (int q = 0; q < n; ++q)
+            perm_p2l_[q] = perm_l2p_[q] = ref_l2p_[q] = q;
+        reinitialize_mapping();
+        injected("cudaMalloc of the reduction partials");
+        QCSB_CUDA(cudaMalloc(&red_partials_, sizeof(double2) * kReduceBlocks));
+        injected("cudaMalloc of the reduction ticket");
+        QCSB_CUDA(cudaMalloc(&red_ticket_, sizeof(unsigned)));
+        QCSB_CUDA(cudaMemset(red_ticket_, 0, sizeof(unsigned)));
+        injected("cudaMalloc of the <Z> partials");
+        QCSB_CUDA(cudaMalloc(&zsum_partials_, sizeof(double) * 512 * (kMaxQubits + 1)));
+        injected("cudaMalloc of the <Z> sums");
+        QCSB_CUDA(cudaMalloc(&zsum_result_, sizeof(double) * (kMaxQubits + 1)));
+        injected("cudaMallocHost of the host buffer");
+        QCSB_CUDA(cudaMallocHost(&host_pinned_, 1 << 16));
+        host_pinned_bytes_ = 1 << 16;
+        // the measurement's result and completion flag: written only by the
+        // measurement kernel
+        injected("cudaMallocHost of the measurement result");
+        QCSB_CUDA(cudaMallocHost(&meas_host_, kMeasureHostBytes));
+        *reinterpret_cast<unsigned *>(static_cast<char *>(meas_host_) + kMeasureFlagOffset) = 0;
+        measure_seq_ = 0;
+        injected("cudaHostAlloc of the pass error flag");
+        fused_ = new FusedExecutor(stream_);
+        fused_->set_options(opt_max_ops_, opt_local_bits_);
+        fused_->set_tensor_mode(opt_tensor_);
+        fused_->set_tensor_engine(opt_engine_);
+        fused_->set_cost_model(model_);
+        set_zero_state();
+    }
+    catch (...)
+    {
+        release_allocation();
+        throw;
+    }
+}
+
+void Simulator::release_allocation()
+{
+    if (stream_)
+        cudaStreamSynchronize(stream_);
+    delete fused_;
+    fused_ = nullptr;
+    cudaFree(state_);
+    cudaFree(red_partials_);
+    cudaFree(red_ticket_);
+    cudaFree(zsum_partials_);
+    cudaFree(zsum_result_);
+    if (host_pinned_)
+        cudaFreeHost(host_pinned_);
+    if (meas_host_)
+        cudaFreeHost(meas_host_);
+    state_ = nullptr;
+    red_partials_ = nullptr;
+    red_ticket_ = nullptr;
+    zsum_partials_ = zsum_result_ = nullptr;
+    host_pinned_ = nullptr;
+    host_pinned_bytes_ = 0;
+    meas_host_ = nullptr;
+    n_ = 0;
+    // the failure was reported by the exception; an exhausted allocation
+    // must not surface again as the error of a later launch check
+    (void)cudaGetLastError();
 }
 
 void Simulator::set_planner_options(int max_ops, int local_bits)

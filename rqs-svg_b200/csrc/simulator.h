@@ -150,6 +150,8 @@ class Simulator
         pending_gates_ = 0;
     }
     void restore_reference_layout();
+    // frees what allocate_memory allocated (after a failure part way)
+    void release_allocation();
 
     bool disposed_ = false;
     int device_ = 0;
