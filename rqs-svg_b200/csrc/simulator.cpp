@@ -743,9 +743,22 @@ void Simulator::ensure_staging()
 {
     if (staging_dev_ != nullptr)
         return;
-    staging_count_ = std::max<uint64_t>(2, std::min<uint64_t>(kStagingAmps, 1ull << n_));
-    QCSB_CUDA(cudaMalloc(&staging_dev_, sizeof(double2) * staging_count_));
-    QCSB_CUDA(cudaMallocHost(&staging_host_, sizeof(double2) * staging_count_));
+    // both buffers or neither: a failed pinned allocation frees the device
+    // one, so that a later call allocates again instead of copying through
+    // a missing host buffer
+    const uint64_t count = std::max<uint64_t>(2, std::min<uint64_t>(kStagingAmps, 1ull << n_));
+    double2 *dev = nullptr, *host = nullptr;
+    QCSB_CUDA(cudaMalloc(&dev, sizeof(double2) * count));
+    const cudaError_t err = cudaMallocHost(&host, sizeof(double2) * count);
+    if (err != cudaSuccess)
+    {
+        cudaFree(dev);
+        (void)cudaGetLastError();
+        throw std::runtime_error(strformat("cudaMallocHost of the staging buffer: %s", cudaGetErrorString(err)));
+    }
+    staging_dev_ = dev;
+    staging_host_ = host;
+    staging_count_ = count;
 }
 
 // Move the whole register between device (physical order) and host (logical
